@@ -1,0 +1,488 @@
+"""Benchmark of the mover + P2G hot path on the GEM cycle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 128x64x64 cells, 4 species x 65,536,000 particles (125 ppc on a
+5x5x5 jittered sub-lattice), NiterMover = 3, E ~ U(-1e-3, 1e-3) plus the
+Harris-sheet B; seeded synthetic inputs generated on the device. One step is
+one cycle of the hot section of the reference driver
+(src/sputniPIC_CPU.cpp:232-256): mover_PC for every species, zero the
+moments, interpP2G + applyBCids for every species.
+
+Keys of the JSON line:
+  value       particles pushed+deposited per second with all inputs already
+              in HBM (device-timed with CUDA events, max over ranks)
+  e2e         the same metric through the reference-facing C-ABI drop-in
+              (spb_mover_PC / spb_interpP2G on the reference structs) with
+              pinned HOST arrays: every step uploads the particles, fields and
+              moments and downloads the results, inside the timed region
+  roofline    the dominant kernel's algorithmic bytes per launch / its mean
+              CUDA-event duration, against MEASURED_PEAKS.json's HBM copy
+              bandwidth
+  cpu_baseline  the reference CPU code (oracle/_ref, else the restated port)
+              timed on this host's cores on a bounded sample of the workload
+The particle arrays (7.3 GB) are far larger than the 126 MB L2, so no L2
+flush is needed between steps.
+
+``--impl reference`` times the reference's own CPU mover_PC + interpP2G +
+applyBCids (the CPU driver's hot section) on a bounded sample per step with
+all host threads; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from sputnipic_b200 import workload as W  # noqa: E402
+
+METRIC = "mover_p2g_particles_per_s"
+UNIT = "particles/s"
+# the reference GPU build, same GEM config, 5.208 s and 4.942 s
+# per mover+interp cycle of 262,144,000 particles (README.md:76,93)
+PUBLISHED_PPS = 262_144_000 / ((5.208 + 4.942) / 2)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        if not self.lines:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --- CPU reference arm ------------------------------------------------------------
+def cpu_sample(wl, slabs: int):
+    """Fields of the whole grid and the particles of the first ``slabs``
+    x-slabs of cells of every species (host generator)."""
+    fields = W.gem_fields(wl)
+    hi = slabs * wl.nyc * wl.nzc
+    parts = [W.gem_particles(wl, s, 0, hi) for s in range(len(wl.species))]
+    for p in parts:
+        p.pop("cell")
+    return fields, parts
+
+
+def time_cpu(wl, slabs: int, steps: int, warmup: int, min_seconds: float = 0.0):
+    """Times the CPU driver's hot section on a sample; returns per-step times,
+    the sample size and the oracle kind/threads."""
+    import oracle
+    kind = "reference" if oracle.reference_available(32) else "restated"
+    orc = oracle.CpuOracle(kind, 32)
+    fields, parts = cpu_sample(wl, slabs)
+    setup = oracle.setup_from(wl)
+    n = sum(len(p["x"]) for p in parts)
+    mom = [np.zeros(wl.nodes, np.float32) for _ in range(10 * len(parts))]
+    times = []
+    t_start = time.perf_counter()
+    i = 0
+    while i < warmup + steps or (time.perf_counter() - t_start < min_seconds and i < 200):
+        tm, ti = orc.cycle(setup, fields, parts, mom)
+        if i >= warmup:
+            times.append(tm + ti)
+        i += 1
+    return times, n, ("reference" if kind == "reference" else "port"), orc.threads
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    wl = W.gem()
+    slabs = args.cpu_slabs
+    times, n, kind, cores = time_cpu(wl, slabs, args.steps, args.warmup)
+    t = sum(times)
+    pps = n * len(times) / t
+    sample = (f"first {slabs} of 128 x-slabs of cells of the GEM workload: {n} particles "
+              f"({n // len(wl.species)} per species), full 128x64x64 grid fields")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": pps, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / len(times) * (wl.total_particles / n),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": pps / PUBLISHED_PPS,
+        "dtype": "fp32", "data": "synthetic (seeded GEM Harris sheet)",
+        "config": {"workload": wl.name, "particles": wl.total_particles, "niter": wl.niter,
+                   "sample_particles": n, "form": "reference CPU (mover_PC + interpP2G + applyBCids)"},
+        "cpu_baseline": {"value": pps, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": pps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --- our arm ------------------------------------------------------------------------
+def algorithmic_bytes(kind: str, n: int, nodes: int, ns: int = 1) -> int:
+    """Compulsory HBM bytes of one launch (per-kernel table of the design notes)."""
+    if kind == "mover":       # plain: read x..w, write x..w; packed fields once
+        return 48 * n + 24 * nodes
+    if kind == "p2g":         # plain: read x..w, q; read+write the ten FP32 moments
+        return 28 * n + 80 * nodes
+    if kind == "cycle":       # precision: read cell, offsets, u..w, q (32 B); write 28 B;
+        return 60 * n + 24 * nodes + 80 * nodes * ns   # fields once; FP64 moments written
+    if kind == "sort":        # counting sort: read cell; read + write 32 B per particle
+        return 68 * n
+    raise ValueError(kind)
+
+
+def load_traffic():
+    """DRAM bytes per particle of each kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def device_timed(torch, dist, stream, steps, fn):
+    """Runs fn() `steps` times between CUDA events; max over ranks (ms)."""
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        fn()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def measure_plain(args, torch, wl, fields, parts, dist, stream):
+    """Plain form (reference precision types) on device-resident arrays: the
+    CPU driver's sequence mover_PC x ns, zero moments, interpP2G + applyBCids."""
+    from sputnipic_b200 import _lib
+    from sputnipic_b200.device import GridContext, push_params
+    ns = len(parts)
+    counts = [p["x"].numel() for p in parts]
+    ctx = GridContext(wl)
+    ctx.set_fields(fields)
+    pushes = [push_params(wl, s) for s in range(ns)]
+    mom = torch.zeros(ns, 10, wl.nodes, device="cuda")
+    ev = {"mover": [], "p2g": []}
+
+    def timed(kind, n, fn, record):
+        if record:
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        fn()
+        if record:
+            b.record(stream)
+            ev[kind].append((a, b, n))
+
+    def step(record=False):
+        for s in range(ns):
+            timed("mover", counts[s], lambda: ctx.mover(parts[s], pushes[s]), record)
+        mom.zero_()
+        for s in range(ns):
+            timed("p2g", counts[s], lambda: ctx.p2g(parts[s], mom[s]), record)
+            ctx.apply_bc_ids(mom[s], wl.periodic)
+        if dist is not None:
+            dist.all_reduce(mom)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    rc = ctx.check()
+    if rc:
+        raise RuntimeError(f"plain warm-up status {rc}: {_lib.last_error()}")
+    steps = max(2, args.steps // 2)
+    ms = device_timed(torch, dist, stream, steps, lambda: step(True))
+    kern = {}
+    for k, lst in ev.items():
+        durs = [a.elapsed_time(b) for a, b, _ in lst]
+        n_mean = statistics.mean(c for _, _, c in lst)
+        alg = algorithmic_bytes(k, int(n_mean), wl.nodes)
+        kern[k] = {"ms_mean": statistics.mean(durs), "share": sum(durs) / ms,
+                   "achieved_gbs": alg / (statistics.mean(durs) / 1e3) / 1e9}
+    ctx.close()
+    del mom
+    return {"value": sum(counts) * steps / (ms / 1e3), "ms_per_step": ms / steps,
+            "steps": steps, "kernels": kern}
+
+
+def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
+    """Precision form: one fused mover + deposit kernel per cycle for all
+    species, counting sort every `resort` cycles (amortised in the steps)."""
+    from sputnipic_b200 import _lib
+    from sputnipic_b200.sim import Simulation
+    ns = len(parts)
+    n = sum(p["x"].numel() for p in parts)
+    sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort)
+    sim.set_fields(fields)
+    for s, p in enumerate(parts):
+        sim.load_species(s, p)
+    for _ in range(args.warmup):
+        sim.cycle(1)
+    rc = sim.check()
+    if rc:
+        raise RuntimeError(f"precision warm-up status {rc}: {_lib.last_error()}")
+    lib = _lib.load()
+    sim.set_timing(True)
+    sim.timing()
+    l0 = lib.spb_launch_count()
+    local_rank = torch.cuda.current_device()
+    with Clocks(local_rank) as clk:
+        ms = device_timed(torch, dist, stream, args.steps, lambda: sim.cycle(1))
+    launches = lib.spb_launch_count() - l0
+    cyc_ms, ncyc, sort_ms, nsort = sim.timing()
+    sim.set_timing(False)
+    rc = sim.check()
+    if rc:
+        raise RuntimeError(f"precision status {rc}: {_lib.last_error()}")
+    peak, peak_kind = peaks()
+    alg = algorithmic_bytes("cycle", n, wl.nodes, ns)
+    kms = cyc_ms / max(ncyc, 1)
+    achieved = alg / (kms / 1e3) / 1e9
+    traffic = load_traffic().get("precision_cycle")
+    roofline = {
+        "kernel": "k_cycle (fused mover + deposit, all species)", "bound": "hbm",
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": (traffic["dram_bytes_per_particle"] * n if traffic else None),
+        "algorithmic_bytes": alg, "kernel_ms_mean": kms,
+        "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+        "share_of_step": cyc_ms / ms,
+        "sort": {"ms_mean": sort_ms / max(nsort, 1), "launches": nsort,
+                 "share_of_step": sort_ms / ms,
+                 "achieved_gbs": (algorithmic_bytes("sort", n // ns, 0) /
+                                  ((sort_ms / max(nsort, 1)) / 1e3) / 1e9) if nsort else None},
+    }
+    sim.close()
+    return {"value": n * world * args.steps / (ms / 1e3), "ms": ms, "roofline": roofline,
+            "clocks": clk.summary(), "launches": launches}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from sputnipic_b200 import _lib
+    from sputnipic_b200.device import gen_fields, gen_particles
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    _lib.load()
+    wl = W.gem(seed=rank)
+    if args.nspecies != 4 or args.ppc != 125:
+        wl = wl.with_(lattice=5 if args.ppc == 125 else 0,
+                      species=W.gem_species((args.ppc,) * 4)[:args.nspecies])
+    ns = len(wl.species)
+    stream = torch.cuda.current_stream()
+    fields = gen_fields(wl)
+    parts = [gen_particles(wl, s) for s in range(ns)]
+    ntot = sum(p["x"].numel() for p in parts)
+    host = None
+    if not args.no_e2e:
+        host = [{k: p[k].cpu().pin_memory() for k in "xyzuvwq"} for p in parts]
+        host_f = [f.cpu().pin_memory() for f in fields]
+
+    plain = None
+    if not args.no_plain:
+        plain = measure_plain(args, torch, wl, fields, [dict(p) for p in parts], dist, stream)
+        # the plain run moved the particles: regenerate the initial state
+        parts = [gen_particles(wl, s) for s in range(ns)]
+    prec = measure_precision(args, torch, wl, fields, parts, dist, stream, world)
+    del parts
+    torch.cuda.empty_cache()
+
+    e2e = None
+    if host is not None:
+        e2e = run_e2e(args, wl, host, host_f, world, dist)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        times, n, kind, cores = time_cpu(wl, args.cpu_slabs, 3, 1, min_seconds=10.0)
+        cpu = {"value": n / statistics.median(times), "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"first {args.cpu_slabs} of 128 x-slabs of cells ({n} particles, "
+                         f"full 128x64x64 grid fields); median of {len(times)} cycles of "
+                         "mover_PC + interpP2G + applyBCids"}
+
+    if rank == 0:
+        value = prec["value"]
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": prec["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / PUBLISHED_PPS, "dtype": "fp32 push, fp64 moments",
+            "data": "synthetic (seeded GEM Harris sheet, generated on the device)",
+            "config": {"workload": f"{wl.name}: {ns} species x {ntot // ns:,} particles, "
+                                   f"{wl.species[0].ppc:g} ppc, NiterMover {wl.niter}, "
+                                   "one mover + 10-moment deposit cycle",
+                       "form": "precision (int32 cell + fp32 offset, fp32 push, "
+                               "fp32 smem partials -> fp64 moments)",
+                       "tile": list(args.tile), "resort_every": args.resort,
+                       "particles_per_gpu": ntot, "grid_cells": [wl.nxc, wl.nyc, wl.nzc],
+                       "parallelism": f"particle decomposition x{world}" if world > 1 else "1 GPU",
+                       "l2": "particle arrays (8.4 GB) exceed the 126 MB L2; no flush needed"},
+            "roofline": prec["roofline"], "clocks": prec["clocks"],
+            "gpu_launches": prec["launches"],
+            "plain": None if plain is None else {
+                "value": plain["value"], "unit": UNIT, "ms_per_step": plain["ms_per_step"],
+                "kernels": plain["kernels"], "speedup_of_precision_form": value / plain["value"]},
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, wl, host_parts, host_f, world, dist):
+    """Drop-in path with host arrays: COPY residency, pinned host memory."""
+    import torch
+    from sputnipic_b200 import dropin
+    ns = len(wl.species)
+    param = dropin.make_parameters(wl)
+    grd = dropin.setGrid(param)
+    field = dropin.field_allocate(grd, [f.numpy() for f in host_f])
+    # the struct adopts the pinned buffers (no copy for contiguous float32)
+    P, keep = [], []
+    for s in range(ns):
+        arrs = {k: host_parts[s][k].numpy() for k in "xyzuvwq"}
+        P.append(dropin.particle_allocate(param, s, arrays=arrs))
+    ids = []
+    for s in range(ns):
+        i = dropin.interp_dens_species_allocate(grd, s)
+        for name in list(i._arrays):
+            t = torch.zeros(i._arrays[name].size, dtype=torch.float32).pin_memory()
+            keep.append(t)
+            i._arrays[name] = t.numpy()
+            setattr(i, name + "_flat", t.numpy().ctypes.data)
+        ids.append(i)
+    nodes = wl.nodes
+    n = [p.nop for p in P]
+    h2d = sum(52 * c for c in n) + ns * (24 * nodes + 40 * nodes)
+    d2h = sum(24 * c for c in n) + ns * 40 * nodes
+
+    def step():
+        for s in range(ns):
+            if dropin.mover_PC(P[s], field, grd, param) != 0:
+                raise RuntimeError(dropin.last_error())
+        for s in range(ns):
+            dropin.setZeroSpeciesDensities(ids[s])
+            dropin.interpP2G(P[s], ids[s], grd, raise_on_error=True)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    steps = max(2, min(args.steps, 5))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    t = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    dropin.release_all()
+    return {"value": sum(n) * world * steps / t, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps, "ms_per_step": 1e3 * t / steps,
+            "path": "spb_mover_PC + spb_interpP2G on reference structs, COPY residency, "
+                    "pinned host arrays; timed on the host clock"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-slabs", type=int, default=4)
+    ap.add_argument("--tile", type=int, nargs=3, default=[8, 4, 4])
+    ap.add_argument("--nspecies", type=int, default=4,
+                    help="smaller profiling cases only; the benchmark uses all 4")
+    ap.add_argument("--ppc", type=float, default=125,
+                    help="smaller profiling cases only; the benchmark uses 125")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--resort", type=int, default=4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+        try:
+            run_ours(args, rank, world, local_rank)
+        finally:
+            dist.destroy_process_group()
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,300 @@
+/*
+ * libsputnipic_b200: B200 (sm_100a) particle mover and particle-to-grid (P2G)
+ * moment deposition for sputniPIC, behind the reference's own entry points.
+ *
+ * Boundary. The reference exposes the hot path as C-style free functions over
+ * plain structs (include/Mover.h:11-26):
+ *
+ *   int  mover_PC(struct particles*, struct EMfield*, struct grid*, struct parameters*);
+ *   int  mover_PC_V(struct particles*, struct EMfield*, struct grid*, struct parameters*);
+ *   void interpP2G(struct particles*, struct interpDensSpecies*, struct grid*);
+ *   int  mover_interp(struct particles*, struct EMfield*, struct interpDensSpecies*,
+ *                     struct grid*, struct parameters*);
+ *
+ * The library exports those four symbols with C++ linkage (the reference is
+ * compiled as C++), so the unchanged driver links against this library in
+ * place of src/Mover.cpp, and an extern "C" twin of each (spb_*) for FFI.
+ * Struct layouts: include/sputnipic_ref_layout.h (or the reference's own
+ * headers). Every other entry point below uses plain pointers and sizes.
+ *
+ * Errors. The reference exits the process on a CUDA error
+ * (include/gpu/cuda_helper.h:14-21). Here every call returns a status
+ * (0 = SPB_OK); interpP2G, which returns void, leaves its status in
+ * spb_last_error(). Nothing in the library exits, aborts or traps.
+ *
+ * Threading. The reference driver calls interpP2G from an OpenMP team over
+ * species (src/sputniPIC_CPU.cpp:250-256). All entry points are thread-safe;
+ * calls on different species run on their own CUDA streams.
+ */
+#ifndef SPUTNIPIC_B200_H
+#define SPUTNIPIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct particles;
+struct EMfield;
+struct grid;
+struct interpDensSpecies;
+struct parameters;
+
+/* ---------------------------------------------------------------------------
+ * Status codes
+ * ------------------------------------------------------------------------- */
+enum spb_status {
+  SPB_OK = 0,
+  SPB_ERR_CUDA = 1,          /* a CUDA runtime call failed */
+  SPB_ERR_INVALID = 2,       /* bad argument (null pointer, size, layout) */
+  SPB_ERR_OUT_OF_GRID = 3,   /* a particle's cell index left the node array;
+                                the reference reads out of bounds there */
+  SPB_ERR_NO_DEVICE = 4,     /* no CUDA device */
+  SPB_ERR_ALLOC = 5,         /* device or pinned allocation failed */
+  SPB_ERR_UNSUPPORTED = 6,   /* configuration outside what the kernels cover */
+  SPB_ERR_TIMEOUT = 7,       /* a bounded device wait gave up */
+  SPB_ERR_CAPACITY = 8       /* a request exceeds a fixed capacity */
+};
+
+/* Status of the calling thread's most recent failing call (sticky until
+ * spb_clear_error), with a one-line message. */
+int spb_last_error(void);
+const char *spb_last_error_message(void);
+void spb_clear_error(void);
+const char *spb_error_string(int status);
+
+/* Library version string and the sm architecture it was built for. */
+const char *spb_version(void);
+
+/* Number of kernels this library has launched in this process. */
+long spb_launch_count(void);
+
+/* JSON object: "struct.member": offset for every member of the boundary
+ * structs as this library lays them out (see sputnipic_ref_layout.h). */
+const char *spb_abi_layout_json(void);
+
+/* Select the CUDA device used by the drop-in entry points (default 0). */
+int spb_set_device(int device);
+
+/* ---------------------------------------------------------------------------
+ * Drop-in entry points, extern "C" twins of the reference functions.
+ * Replace: include/Mover.h:11 (mover_PC), :16 (mover_PC_V), :20 (interpP2G),
+ * :24 (mover_interp); bodies src/Mover.cpp:4-162, :166-382, :385-572, :575-862.
+ *
+ * Semantics match the reference's CPU functions: mover_PC updates
+ * part->x..w in place (NiterMover predictor-corrector iterations, one pass,
+ * particle BC from param->PERIODICX/Y/Z); interpP2G ADDS the ten moments of
+ * every particle into ids->rhon..pzz (the caller zeroes them and applies
+ * applyBCids afterwards); mover_interp does both per particle.
+ * Arithmetic: float with the reference's double promotions, no FMA
+ * contraction, so particle outputs are bit-identical to the reference CPU
+ * code. Moments are FP32 sums in a different order (within tolerance).
+ * ------------------------------------------------------------------------- */
+int spb_mover_PC(struct particles *part, struct EMfield *field, struct grid *grd,
+                 struct parameters *param);
+int spb_mover_PC_V(struct particles *part, struct EMfield *field,
+                   struct grid *grd, struct parameters *param);
+void spb_interpP2G(struct particles *part, struct interpDensSpecies *ids,
+                   struct grid *grd);
+int spb_mover_interp(struct particles *part, struct EMfield *field,
+                     struct interpDensSpecies *ids, struct grid *grd,
+                     struct parameters *param);
+
+/* Host coherence of the drop-in. COPY (default): particles are uploaded and
+ * downloaded on every call, so the host arrays are always current. DEVICE:
+ * particles stay in HBM between calls; the host arrays are refreshed only by
+ * spb_sync_particles_to_host (call it before particle_sort or particle IO),
+ * and spb_invalidate_particles must follow any host-side change. */
+enum spb_residency { SPB_RESIDENCY_COPY = 0, SPB_RESIDENCY_DEVICE = 1 };
+int spb_set_residency(int mode);
+int spb_sync_particles_to_host(struct particles *part);
+int spb_invalidate_particles(struct particles *part);
+/* Free every device mirror and stream the drop-in holds. */
+int spb_release_all(void);
+
+/* ---------------------------------------------------------------------------
+ * Device-pointer API of the plain form (reference precision types, arrays in
+ * HBM). A grid context holds the grid geometry, the node coordinates and
+ * the packed E/B fields on one device.
+ * Replaces the reference GPU build's per-batch staging path
+ * (src/gpu/Particles_gpu.cu:221-287, batch_update_particles) and its kernel
+ * move_and_interpolate (src/gpu/Particles_gpu.cu:291-577).
+ * `stream` is a cudaStream_t (NULL = legacy default stream).
+ * ------------------------------------------------------------------------- */
+typedef struct spb_grid_ctx spb_grid_ctx;
+
+/* Time-step parameters of one species' push. */
+typedef struct spb_push {
+  double dt;          /* param->dt */
+  double c;           /* param->c */
+  float qom;          /* part->qom */
+  int niter;          /* part->NiterMover (>= 1) */
+  int n_sub_cycles;   /* part->n_sub_cycles (>= 1; divides dt only) */
+  int periodic[3];    /* param->PERIODICX/Y/Z */
+} spb_push;
+
+/* Build a context from a host `struct grid` (setGrid output). The node
+ * coordinate arrays must be separable (XN depends on i only, and so on),
+ * which setGrid guarantees (src/Grid.cpp:53-61). */
+int spb_grid_create(const struct grid *grd, spb_grid_ctx **out);
+/* Same, from scalars: active cells and lengths, as setGrid computes them. */
+int spb_grid_create_uniform(int nxc, int nyc, int nzc, double Lx, double Ly,
+                            double Lz, spb_grid_ctx **out);
+void spb_grid_destroy(spb_grid_ctx *ctx);
+/* Number of nodes nxn*nyn*nzn. */
+long spb_grid_nodes(const spb_grid_ctx *ctx);
+/* Upload and pack the six node fields (Ex, Ey, Ez, Bxn, Byn, Bzn; each
+ * nodes floats). `on_device` != 0: the pointers are device pointers. */
+int spb_grid_set_fields(spb_grid_ctx *ctx, const float *const fields[6],
+                        int on_device, void *stream);
+/* mover_PC over n particles in device memory. */
+int spb_grid_mover(spb_grid_ctx *ctx, const spb_push *push, float *x, float *y,
+                   float *z, float *u, float *v, float *w, long n, void *stream);
+/* interpP2G over n particles: ADDS into mom[0..9] (device, nodes floats each,
+ * order rhon, Jx, Jy, Jz, pxx, pxy, pxz, pyy, pyz, pzz). */
+int spb_grid_p2g(spb_grid_ctx *ctx, const float *x, const float *y,
+                 const float *z, const float *u, const float *v, const float *w,
+                 const float *q, long n, float *const mom[10], void *stream);
+/* mover_interp: move then deposit, one kernel. */
+int spb_grid_mover_interp(spb_grid_ctx *ctx, const spb_push *push, float *x,
+                          float *y, float *z, float *u, float *v, float *w,
+                          const float *q, long n, float *const mom[10],
+                          void *stream);
+/* applyBCids (src/BC.cpp:362-615) on device moments, for callers that keep
+ * the moments in HBM. periodic = param->PERIODICX/Y/Z. */
+int spb_grid_apply_bc_ids(spb_grid_ctx *ctx, const int periodic[3],
+                          float *const mom[10], void *stream);
+/* Synchronise `stream` and report SPB_ERR_OUT_OF_GRID if any kernel of this
+ * context saw a cell index outside the node array since the last check
+ * (such particles are clamped to the edge cell instead of reading out of
+ * bounds). Clears the flag. */
+int spb_grid_check(spb_grid_ctx *ctx, void *stream);
+/* Kernel launches issued by this context since creation. */
+long spb_grid_launches(const spb_grid_ctx *ctx);
+
+/* ---------------------------------------------------------------------------
+ * Precision form (device-resident simulation). Replaces, for callers that
+ * keep particles in HBM across cycles, the per-cycle section of the CPU
+ * driver that calls mover_PC and interpP2G for every species
+ * (src/sputniPIC_CPU.cpp:232-256; src/Mover.cpp:4-162 and :385-572).
+ *
+ * Particles are stored as an int32 cell index (packed cz | cy<<11 | cx<<21)
+ * plus FP32 in-cell offsets, FP32 velocities and charge, cell-sorted in
+ * tile-major order by an on-device counting sort. One fused kernel per cycle
+ * runs the NiterMover predictor-corrector push (FP32, E/B gathered from a
+ * TMA-staged tile of nodes) and deposits the ten moments as FP32
+ * shared-memory partials flushed into FP64 global moments.
+ * Moments are the raw interpP2G sums (zeroed at the start of every cycle, no
+ * applyBCids), FP64, [10][nxn*nyn*nzn] per species in the reference order.
+ * ------------------------------------------------------------------------- */
+typedef struct spb_sim spb_sim;
+
+#define SPB_SIM_MAX_SPECIES 8
+
+typedef struct spb_sim_desc {
+  int nxc, nyc, nzc;        /* active cells; multiples of the tile shape */
+  double Lx, Ly, Lz;
+  double dt, c;             /* param->dt, param->c */
+  int niter;                /* NiterMover */
+  int periodic[3];          /* param->PERIODICX/Y/Z */
+  int ns;                   /* species, 1..8 */
+  double qom[SPB_SIM_MAX_SPECIES];
+  long capacity[SPB_SIM_MAX_SPECIES]; /* optional: particles to reserve for */
+  int tile[3];              /* cells per tile (0,0,0: default 8x4x4) */
+  int resort_every;         /* cycles between counting sorts (>= 1) */
+  int ctas;                 /* persistent CTAs (0: one per SM) */
+} spb_sim_desc;
+
+/* Whether a tile shape has an instantiated kernel. */
+int spb_sim_tile_supported(int tx, int ty, int tz);
+int spb_sim_create(const spb_sim_desc *desc, spb_sim **out);
+void spb_sim_destroy(spb_sim *sim);
+long spb_sim_nodes(const spb_sim *sim);
+long spb_sim_count(const spb_sim *sim, int species);
+/* Kernel launches issued by this simulation. */
+long spb_sim_launches(const spb_sim *sim);
+/* Six node fields (Ex, Ey, Ez, Bxn, Byn, Bzn), nodes floats each. */
+int spb_sim_set_fields(spb_sim *sim, const float *const fields[6], int on_device,
+                       void *stream);
+/* Load one species from reference-style float arrays (positions in domain
+ * units, inside [0, L]); converts to cell + offset and sorts. */
+int spb_sim_load_species(spb_sim *sim, int species, const float *x, const float *y,
+                         const float *z, const float *u, const float *v,
+                         const float *w, const float *q, long n, int on_device,
+                         void *stream);
+/* ncycles of mover + deposit for all species (the last cycle's moments
+ * remain). Resorts every desc.resort_every cycles. */
+int spb_sim_cycle(spb_sim *sim, int ncycles, void *stream);
+/* Counting sort of every species now. */
+int spb_sim_resort(spb_sim *sim, void *stream);
+/* FP64 moments of a species: 10*nodes doubles. */
+int spb_sim_moments(spb_sim *sim, int species, double *out, int on_device,
+                    void *stream);
+/* applyBCids (src/BC.cpp:362-615) on a species' FP64 moments, in place. */
+int spb_sim_apply_bc_ids(spb_sim *sim, int species, void *stream);
+/* Positions x = (cell + offset) * dx, velocities and (if q is not NULL)
+ * charges, as floats, in the simulation's current (sorted) order. */
+int spb_sim_particles(spb_sim *sim, int species, float *x, float *y, float *z,
+                      float *u, float *v, float *w, float *q, int on_device,
+                      void *stream);
+/* Synchronise; SPB_ERR_OUT_OF_GRID / SPB_ERR_TIMEOUT from the kernels. */
+int spb_sim_check(spb_sim *sim, void *stream);
+/* CUDA-event timing of the fused cycle kernel and of the sorts, recorded on
+ * the launching stream while enabled. spb_sim_timing synchronises, returns
+ * the summed milliseconds and launch counts since the last query, and
+ * clears them. */
+int spb_sim_set_timing(spb_sim *sim, int on);
+int spb_sim_timing(spb_sim *sim, double *cycle_ms, int *ncycle, double *sort_ms,
+                   int *nsort);
+
+/* ---------------------------------------------------------------------------
+ * Seeded synthetic GEM (Harris current sheet) inputs, generated on the device.
+ * No counterpart in the reference's hot path: the reference builds its inputs
+ * on the host with initGEM (src/IC.cpp:7-188). Same hash and formulas as
+ * sputnipic_b200/workload.py.
+ * ------------------------------------------------------------------------- */
+typedef struct spb_gem_desc {
+  int nxc, nyc, nzc;        /* active cells */
+  double Lx, Ly, Lz;
+  double B0, delta, pert;   /* Harris sheet amplitude, width, flux perturbation */
+  double E_amp;             /* E ~ U(-E_amp, E_amp) per node and axis */
+  int lattice;              /* 0: uniform in the cell; m: m^3 jittered sub-lattice */
+  unsigned long long seed;
+} spb_gem_desc;
+
+typedef struct spb_gem_species {
+  double qom, rho0, vth, w0, ppc;
+  int sheet;                /* 1: sech^2 current sheet density, 0: uniform */
+} spb_gem_species;
+
+/* Particles of one species in the whole grid: floor(cells * ppc). */
+long spb_gem_species_count(const spb_gem_desc *d, const spb_gem_species *sp);
+/* Fields on all nodes: six device arrays of nxn*nyn*nzn floats. */
+int spb_gen_gem_fields(const spb_gem_desc *d, float *const fields[6], void *stream);
+/* Particles [first, first+count) of species `species` (cells in x-major
+ * order) into device arrays; `cell` (optional) receives the active-cell
+ * index of each particle. */
+int spb_gen_gem_particles(const spb_gem_desc *d, const spb_gem_species *sp,
+                          int species, long first, long count, float *x, float *y,
+                          float *z, float *u, float *v, float *w, float *q,
+                          int *cell, void *stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+
+/* C++-linkage drop-ins with the reference's exact signatures, so objects
+ * compiled against the reference's include/Mover.h link to this library. */
+int mover_PC(struct particles *part, struct EMfield *field, struct grid *grd,
+             struct parameters *param);
+int mover_PC_V(struct particles *part, struct EMfield *field, struct grid *grd,
+               struct parameters *param);
+void interpP2G(struct particles *part, struct interpDensSpecies *ids,
+               struct grid *grd);
+int mover_interp(struct particles *part, struct EMfield *field,
+                 struct interpDensSpecies *ids, struct grid *grd,
+                 struct parameters *param);
+#endif
+
+#endif /* SPUTNIPIC_B200_H */

@@ -1,0 +1,426 @@
+/*
+ * CPU oracle: a plain-C restatement of sputniPIC's particle mover and
+ * particle-to-grid deposition, written from the reference's behaviour.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA library. Only tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg may load it.
+ *
+ * Parity pin: tests/test_oracle_golden.py checks this restatement against
+ * fixtures produced by the reference's own sources (tests/golden/, made by
+ * tests/golden/make_golden.py through oracle/_ref). In the float build the
+ * particle outputs must be bit-identical to the reference; moments too, since
+ * both accumulate serially in the same particle order.
+ *
+ * Build: -DORACLE_FP64 gives the FP64 oracle (every FP type double), as if the
+ * reference's include/PrecisionTypes.h:6-10 typedefs were double. Compiled
+ * with -ffp-contract=off, as the baseline x86-64 reference build has no FMA.
+ *
+ * Arithmetic follows the C promotion rules of the reference expressions:
+ * where the reference mixes a float with a double member or literal the
+ * operation happens in double and is rounded on assignment.
+ */
+#include "oracle_api.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifdef ORACLE_FP64
+typedef double fpp; /* FPpart   */
+typedef double fpf; /* FPfield  */
+typedef double fpi; /* FPinterp */
+#else
+typedef float fpp;
+typedef float fpf;
+typedef float fpi;
+#endif
+
+/* Grid geometry, as setGrid computes it (src/Grid.cpp:5-62). The node
+ * coordinate arrays XN/YN/ZN only depend on their own axis index, so the
+ * oracle keeps one 1D array per axis. */
+typedef struct og_grid {
+  int nxc, nyc, nzc; /* guard cells included */
+  int nxn, nyn, nzn;
+  double dx, dy, dz;
+  fpf invdx, invdy, invdz, invVOL;
+  double xStart, yStart, zStart;
+  double Lx, Ly, Lz;
+  fpf *xn, *yn, *zn;
+} og_grid;
+
+static int og_make_grid(const orc_setup *s, og_grid *g) {
+  /* src/Grid.cpp:9-15: two guard cells, one extra node */
+  g->nxc = s->nxc + 2;
+  g->nyc = s->nyc + 2;
+  g->nzc = s->nzc + 2;
+  g->nxn = g->nxc + 1;
+  g->nyn = g->nyc + 1;
+  g->nzn = g->nzc + 1;
+  /* src/Grid.cpp:19-27: spacing in double; inverses rounded to FPfield */
+  g->dx = s->Lx / s->nxc;
+  g->dy = s->Ly / s->nyc;
+  g->dz = s->Lz / s->nzc;
+  g->invVOL = (fpf)((fpf)1.0 / (g->dx * g->dy * g->dz));
+  g->invdx = (fpf)((fpf)1.0 / g->dx);
+  g->invdy = (fpf)((fpf)1.0 / g->dy);
+  g->invdz = (fpf)((fpf)1.0 / g->dz);
+  /* src/Grid.cpp:30-41 */
+  g->xStart = 0.0;
+  g->yStart = 0.0;
+  g->zStart = 0.0;
+  g->Lx = s->Lx;
+  g->Ly = s->Ly;
+  g->Lz = s->Lz;
+  g->xn = (fpf *)malloc(sizeof(fpf) * g->nxn);
+  g->yn = (fpf *)malloc(sizeof(fpf) * g->nyn);
+  g->zn = (fpf *)malloc(sizeof(fpf) * g->nzn);
+  if (!g->xn || !g->yn || !g->zn) return -1;
+  /* src/Grid.cpp:53-61: node i sits at (i-1)*dx */
+  for (int i = 0; i < g->nxn; i++) g->xn[i] = (fpf)(g->xStart + (i - 1) * g->dx);
+  for (int j = 0; j < g->nyn; j++) g->yn[j] = (fpf)(g->yStart + (j - 1) * g->dy);
+  for (int k = 0; k < g->nzn; k++) g->zn[k] = (fpf)(g->zStart + (k - 1) * g->dz);
+  return 0;
+}
+
+static void og_free_grid(og_grid *g) {
+  free(g->xn);
+  free(g->yn);
+  free(g->zn);
+}
+
+static inline long og_node(const og_grid *g, int i, int j, int k) {
+  return ((long)i * g->nyn + j) * g->nzn + k;
+}
+
+/* Time-step constants of mover_PC (src/Mover.cpp:11-12). dt_sub_cycling is
+ * the float dt divided in double by n_sub_cycles, then rounded. */
+typedef struct og_push {
+  fpp dt_sub_cycling, dto2, qomdt2;
+} og_push;
+
+static og_push og_push_consts(const orc_setup *s, double qom_in) {
+  og_push p;
+  fpp qom = (fpp)qom_in; /* part->qom = (FPpart)param->qom[is], src/Particles.cpp:25 */
+  p.dt_sub_cycling = (fpp)((double)(fpp)s->dt / ((double)s->n_sub_cycles));
+  p.dto2 = (fpp)(.5 * p.dt_sub_cycling);
+  p.qomdt2 = (fpp)((fpp)(qom * p.dto2) / s->c);
+  return p;
+}
+
+/* One particle of mover_PC, src/Mover.cpp:33-157. The order of every sum
+ * and product is the reference's. */
+static void og_move_one(const og_grid *g, const orc_setup *s, const og_push *pc,
+                        const fpf *const *F, fpp *x, fpp *y, fpp *z, fpp *u,
+                        fpp *v, fpp *w, int bc_v) {
+  const fpp qomdt2 = pc->qomdt2;
+  fpp xptilde = *x, yptilde = *y, zptilde = *z;
+  fpp uptilde = 0, vptilde = 0, wptilde = 0;
+  for (int it = 0; it < s->niter; it++) {
+    /* cell index: truncation of a double product (:39-41) */
+    int ix = 2 + (int)(((double)*x - g->xStart) * (double)g->invdx);
+    int iy = 2 + (int)(((double)*y - g->yStart) * (double)g->invdy);
+    int iz = 2 + (int)(((double)*z - g->zStart) * (double)g->invdz);
+    fpf xi[2], eta[2], zeta[2], wgt[2][2][2];
+    xi[0] = *x - g->xn[ix - 1];
+    eta[0] = *y - g->yn[iy - 1];
+    zeta[0] = *z - g->zn[iz - 1];
+    xi[1] = g->xn[ix] - *x;
+    eta[1] = g->yn[iy] - *y;
+    zeta[1] = g->zn[iz] - *z;
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 2; c++) wgt[a][b][c] = xi[a] * eta[b] * zeta[c] * g->invVOL;
+    fpf El[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 2; c++) {
+          long n = og_node(g, ix - a, iy - b, iz - c);
+          for (int f = 0; f < 6; f++) El[f] += wgt[a][b][c] * F[f][n];
+        }
+    const fpf Exl = El[0], Eyl = El[1], Ezl = El[2];
+    const fpf Bxl = El[3], Byl = El[4], Bzl = El[5];
+    /* implicit velocity solve (:70-83); denom is computed in double */
+    fpp omdtsq = qomdt2 * qomdt2 * (Bxl * Bxl + Byl * Byl + Bzl * Bzl);
+    fpp denom = (fpp)(1.0 / (1.0 + (double)omdtsq));
+    fpp ut = *u + qomdt2 * Exl;
+    fpp vt = *v + qomdt2 * Eyl;
+    fpp wt = *w + qomdt2 * Ezl;
+    fpp udotb = ut * Bxl + vt * Byl + wt * Bzl;
+    uptilde = (ut + qomdt2 * (vt * Bzl - wt * Byl + qomdt2 * udotb * Bxl)) * denom;
+    vptilde = (vt + qomdt2 * (wt * Bxl - ut * Bzl + qomdt2 * udotb * Byl)) * denom;
+    wptilde = (wt + qomdt2 * (ut * Byl - vt * Bxl + qomdt2 * udotb * Bzl)) * denom;
+    /* half-step position (:85-87) */
+    *x = xptilde + uptilde * pc->dto2;
+    *y = yptilde + vptilde * pc->dto2;
+    *z = zptilde + wptilde * pc->dto2;
+  }
+  /* final velocity in double, position in FPpart (:91-96) */
+  *u = (fpp)(2.0 * (double)uptilde - (double)*u);
+  *v = (fpp)(2.0 * (double)vptilde - (double)*v);
+  *w = (fpp)(2.0 * (double)wptilde - (double)*w);
+  *x = xptilde + uptilde * pc->dt_sub_cycling;
+  *y = yptilde + vptilde * pc->dt_sub_cycling;
+  *z = zptilde + wptilde * pc->dt_sub_cycling;
+
+  /* particle BC per axis (:103-157): an "above L" test, then a separate
+   * "below 0" test; the field periodicity flags choose periodic or mirror */
+  fpp *pos[3] = {x, y, z};
+  fpp *vel[3] = {u, v, w};
+  const double L[3] = {g->Lx, g->Ly, g->Lz};
+  if (bc_v) {
+    /* mover_PC_V (src/Mover.cpp:296-379): per axis, periodic shifts; else the
+     * position is mirrored first, then the velocity is flipped only where
+     * the mirrored position is still outside [0, L] */
+    for (int d = 0; d < 3; d++) {
+      if (s->periodic[d]) {
+        if ((double)*pos[d] > L[d]) *pos[d] = (fpp)((double)*pos[d] - L[d]);
+        if (*pos[d] < 0) *pos[d] = (fpp)((double)*pos[d] + L[d]);
+      } else {
+        if ((double)*pos[d] > L[d]) *pos[d] = (fpp)(2 * L[d] - (double)*pos[d]);
+        if (*pos[d] < 0) *pos[d] = -*pos[d];
+        if ((double)*pos[d] > L[d]) *vel[d] = -*vel[d];
+        if (*pos[d] < 0) *vel[d] = -*vel[d];
+      }
+    }
+    return;
+  }
+  for (int d = 0; d < 3; d++) {
+    if ((double)*pos[d] > L[d]) {
+      if (s->periodic[d]) {
+        *pos[d] = (fpp)((double)*pos[d] - L[d]);
+      } else {
+        *vel[d] = -*vel[d];
+        *pos[d] = (fpp)(2 * L[d] - (double)*pos[d]);
+      }
+    }
+    if (*pos[d] < 0) {
+      if (s->periodic[d]) {
+        *pos[d] = (fpp)((double)*pos[d] + L[d]);
+      } else {
+        *vel[d] = -*vel[d];
+        *pos[d] = -*pos[d];
+      }
+    }
+  }
+}
+
+/* Deposit of one particle, interpP2G's loop body (src/Mover.cpp:399-570). */
+static void og_deposit_one(const og_grid *g, fpp x, fpp y, fpp z, fpp u, fpp v,
+                           fpp w, fpi q, fpi *const *mom) {
+  /* cell index: floor of a double product (:399-401) */
+  int ix = 2 + (int)floor(((double)x - g->xStart) * (double)g->invdx);
+  int iy = 2 + (int)floor(((double)y - g->yStart) * (double)g->invdy);
+  int iz = 2 + (int)floor(((double)z - g->zStart) * (double)g->invdz);
+  fpp xi[2], eta[2], zeta[2], wgt[2][2][2];
+  xi[0] = x - g->xn[ix - 1];
+  eta[0] = y - g->yn[iy - 1];
+  zeta[0] = z - g->zn[iz - 1];
+  xi[1] = g->xn[ix] - x;
+  eta[1] = g->yn[iy] - y;
+  zeta[1] = g->zn[iz] - z;
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++)
+      for (int c = 0; c < 2; c++) wgt[a][b][c] = q * xi[a] * eta[b] * zeta[c] * g->invVOL;
+  /* moment factors: 1, u, v, w, uu, uv, uw, vv, vw, ww (:469-570) */
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++)
+      for (int c = 0; c < 2; c++) {
+        const long n = og_node(g, ix - a, iy - b, iz - c);
+        const fpp wv = wgt[a][b][c];
+        mom[0][n] += wv * g->invVOL;
+        mom[1][n] += (fpp)(u * wv) * g->invVOL;
+        mom[2][n] += (fpp)(v * wv) * g->invVOL;
+        mom[3][n] += (fpp)(w * wv) * g->invVOL;
+        mom[4][n] += (fpp)(u * u * wv) * g->invVOL;
+        mom[5][n] += (fpp)(u * v * wv) * g->invVOL;
+        mom[6][n] += (fpp)(u * w * wv) * g->invVOL;
+        mom[7][n] += (fpp)(v * v * wv) * g->invVOL;
+        mom[8][n] += (fpp)(v * w * wv) * g->invVOL;
+        mom[9][n] += (fpp)(w * w * wv) * g->invVOL;
+      }
+}
+
+/* The reference adds the ten moments one moment at a time over the eight
+ * nodes (src/Mover.cpp:466-570). Each node receives exactly one add per
+ * moment per particle, so the per-node summation order of
+ * og_deposit_one (node-major) equals the reference's (moment-major). */
+
+static int og_mover(const orc_setup *s, const void *const fld[6], void *x, void *y,
+                    void *z, void *u, void *v, void *w, long nop, double qom, int bc_v) {
+  og_grid g;
+  if (og_make_grid(s, &g)) return -1;
+  og_push pc = og_push_consts(s, qom);
+  const fpf *F[6];
+  for (int f = 0; f < 6; f++) F[f] = (const fpf *)fld[f];
+  fpp *X = (fpp *)x, *Y = (fpp *)y, *Z = (fpp *)z;
+  fpp *U = (fpp *)u, *V = (fpp *)v, *W = (fpp *)w;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < nop; i++)
+    og_move_one(&g, s, &pc, F, &X[i], &Y[i], &Z[i], &U[i], &V[i], &W[i], bc_v);
+  og_free_grid(&g);
+  return 0;
+}
+
+int orc_mover_pc(const orc_setup *s, const void *const fld[6], void *x, void *y,
+                 void *z, void *u, void *v, void *w, long nop, double qom) {
+  return og_mover(s, fld, x, y, z, u, v, w, nop, qom, 0);
+}
+
+int orc_mover_pc_v(const orc_setup *s, const void *const fld[6], void *x, void *y,
+                   void *z, void *u, void *v, void *w, long nop, double qom) {
+  return og_mover(s, fld, x, y, z, u, v, w, nop, qom, 1);
+}
+
+void orc_interp_p2g(const orc_setup *s, const void *x, const void *y,
+                    const void *z, const void *u, const void *v, const void *w,
+                    const void *q, long nop, void *const mom[10]) {
+  og_grid g;
+  if (og_make_grid(s, &g)) return;
+  const fpp *X = (const fpp *)x, *Y = (const fpp *)y, *Z = (const fpp *)z;
+  const fpp *U = (const fpp *)u, *V = (const fpp *)v, *W = (const fpp *)w;
+  const fpi *Q = (const fpi *)q;
+  fpi *M[10];
+  for (int m = 0; m < 10; m++) M[m] = (fpi *)mom[m];
+  for (long i = 0; i < nop; i++) og_deposit_one(&g, X[i], Y[i], Z[i], U[i], V[i], W[i], Q[i], M);
+  og_free_grid(&g);
+}
+
+/* applyBCids (src/BC.cpp:362-615): periodic axes fold the last active node
+ * onto the first (node1 += node[n-2]; node[n-2] = node1) in the order X, Y,
+ * Z; then non-periodic axes double both boundary planes, again X, Y, Z. */
+static void og_apply_bc(const og_grid *g, const orc_setup *s, fpi *const *mom) {
+  const int nxn = g->nxn, nyn = g->nyn, nzn = g->nzn;
+  for (int m = 0; m < 10; m++) {
+    fpi *a = mom[m];
+#define N3(i, j, k) a[((long)(i) * nyn + (j)) * nzn + (k)]
+    if (s->periodic[0])
+      for (int j = 1; j < nyn - 1; j++)
+        for (int k = 1; k < nzn - 1; k++) {
+          N3(1, j, k) += N3(nxn - 2, j, k);
+          N3(nxn - 2, j, k) = N3(1, j, k);
+        }
+    if (s->periodic[1])
+      for (int i = 1; i < nxn - 1; i++)
+        for (int k = 1; k < nzn - 1; k++) {
+          N3(i, 1, k) += N3(i, nyn - 2, k);
+          N3(i, nyn - 2, k) = N3(i, 1, k);
+        }
+    if (s->periodic[2])
+      for (int i = 1; i < nxn - 1; i++)
+        for (int j = 1; j < nyn - 1; j++) {
+          N3(i, j, 1) += N3(i, j, nzn - 2);
+          N3(i, j, nzn - 2) = N3(i, j, 1);
+        }
+    if (!s->periodic[0])
+      for (int j = 1; j < nyn - 1; j++)
+        for (int k = 1; k < nzn - 1; k++) {
+          N3(1, j, k) *= 2;
+          N3(nxn - 2, j, k) *= 2;
+        }
+    if (!s->periodic[1])
+      for (int i = 1; i < nxn - 1; i++)
+        for (int k = 1; k < nzn - 1; k++) {
+          N3(i, 1, k) *= 2;
+          N3(i, nyn - 2, k) *= 2;
+        }
+    if (!s->periodic[2])
+      for (int i = 1; i < nxn - 1; i++)
+        for (int j = 1; j < nyn - 1; j++) {
+          N3(i, j, 1) *= 2;
+          N3(i, j, nzn - 2) *= 2;
+        }
+#undef N3
+  }
+}
+
+void orc_apply_bc_ids(const orc_setup *s, void *const mom[10]) {
+  og_grid g;
+  if (og_make_grid(s, &g)) return;
+  fpi *M[10];
+  for (int m = 0; m < 10; m++) M[m] = (fpi *)mom[m];
+  og_apply_bc(&g, s, M);
+  og_free_grid(&g);
+}
+
+int orc_mover_interp(const orc_setup *s, const void *const fld[6], void *x,
+                     void *y, void *z, void *u, void *v, void *w, const void *q,
+                     long nop, double qom, void *const mom[10]) {
+  og_grid g;
+  if (og_make_grid(s, &g)) return -1;
+  og_push pc = og_push_consts(s, qom);
+  const fpf *F[6];
+  for (int f = 0; f < 6; f++) F[f] = (const fpf *)fld[f];
+  fpp *X = (fpp *)x, *Y = (fpp *)y, *Z = (fpp *)z;
+  fpp *U = (fpp *)u, *V = (fpp *)v, *W = (fpp *)w;
+  const fpi *Q = (const fpi *)q;
+  fpi *M[10];
+  for (int m = 0; m < 10; m++) M[m] = (fpi *)mom[m];
+  for (long i = 0; i < nop; i++) {
+    og_move_one(&g, s, &pc, F, &X[i], &Y[i], &Z[i], &U[i], &V[i], &W[i], 0);
+    og_deposit_one(&g, X[i], Y[i], Z[i], U[i], V[i], W[i], Q[i], M);
+  }
+  og_free_grid(&g);
+  return 0;
+}
+
+#ifdef _OPENMP
+static double og_now(void) { return omp_get_wtime(); }
+#else
+#include <time.h>
+static double og_now(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+#endif
+
+int orc_cycle(const orc_setup *s, const void *const fld[6], int ns,
+              void *const *x, void *const *y, void *const *z, void *const *u,
+              void *const *v, void *const *w, void *const *q, const long *nop,
+              const double *qom, void *const *mom, double *t_mover,
+              double *t_interp) {
+  og_grid g;
+  if (og_make_grid(s, &g)) return -1;
+  const fpf *F[6];
+  for (int f = 0; f < 6; f++) F[f] = (const fpf *)fld[f];
+  const long nodes = (long)g.nxn * g.nyn * g.nzn;
+  double t0 = og_now();
+  for (int is = 0; is < ns; is++) {
+    og_push pc = og_push_consts(s, qom[is]);
+    fpp *X = (fpp *)x[is], *Y = (fpp *)y[is], *Z = (fpp *)z[is];
+    fpp *U = (fpp *)u[is], *V = (fpp *)v[is], *W = (fpp *)w[is];
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < nop[is]; i++)
+      og_move_one(&g, s, &pc, F, &X[i], &Y[i], &Z[i], &U[i], &V[i], &W[i], 0);
+  }
+  double t1 = og_now();
+  for (int a = 0; a < ns * 10; a++) memset(mom[a], 0, sizeof(fpi) * nodes);
+#pragma omp parallel for schedule(static, 1)
+  for (int is = 0; is < ns; is++) {
+    fpi *M[10];
+    for (int m = 0; m < 10; m++) M[m] = (fpi *)mom[is * 10 + m];
+    const fpp *X = (const fpp *)x[is], *Y = (const fpp *)y[is], *Z = (const fpp *)z[is];
+    const fpp *U = (const fpp *)u[is], *V = (const fpp *)v[is], *W = (const fpp *)w[is];
+    const fpi *Q = (const fpi *)q[is];
+    for (long i = 0; i < nop[is]; i++) og_deposit_one(&g, X[i], Y[i], Z[i], U[i], V[i], W[i], Q[i], M);
+    og_apply_bc(&g, s, M);
+  }
+  double t2 = og_now();
+  if (t_mover) *t_mover = t1 - t0;
+  if (t_interp) *t_interp = t2 - t1;
+  og_free_grid(&g);
+  return 0;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+int orc_fp_bytes(void) { return (int)sizeof(fpp); }

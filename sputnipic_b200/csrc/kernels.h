@@ -1,0 +1,27 @@
+// Launchers of the kernels, one declaration per kernel family.
+#pragma once
+
+#include "common.h"
+
+namespace spb {
+
+// plain_kernels.cu
+int launch_pack_fields(const float *const f[6], float4 *eb4, float2 *eb2, long nodes,
+                       cudaStream_t s);
+int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F, float *x,
+                       float *y, float *z, float *u, float *v, float *w, long n, int *err,
+                       cudaStream_t s, int bc_variant = 0);
+int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
+                     const float *u, const float *v, const float *w, const float *q, long n,
+                     float *const mom[10], int *err, cudaStream_t s);
+int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFields &F,
+                              float *x, float *y, float *z, float *u, float *v, float *w,
+                              const float *q, long n, float *const mom[10], int *err,
+                              cudaStream_t s);
+int launch_apply_bc_ids(int nxn, int nyn, int nzn, const int periodic[3],
+                        float *const mom[10], cudaStream_t s, long *launches);
+
+// The reference's time-step constants (src/Mover.cpp:11-12) for one species.
+PushDev make_push(const spb_push &p);
+
+}  // namespace spb

@@ -1,0 +1,481 @@
+// Plain-form kernels: the reference's mover_PC / interpP2G / mover_interp /
+// applyBCids on device-resident SoA particles with the reference's precision
+// types (float particles, fields and moments).
+//
+// Bit-exactness. The mover reproduces src/Mover.cpp:31-157 operation by
+// operation: float arithmetic in the reference's evaluation order, the double
+// promotions where the reference mixes float with double (cell index,
+// denominator, final velocity, boundary tests), truncating (mover) and
+// flooring (P2G) double-to-int conversions. This file is compiled with
+// -fmad=false so no multiply-add pair is contracted into an FMA, matching a
+// baseline x86-64 build of the reference. Particle outputs are therefore
+// bit-identical to the reference CPU code; moments differ only by the order
+// of the FP32 additions.
+//
+// Launch shape. One thread per particle, 256 threads per block: the particle
+// SoA streams through once (coalesced 4-byte loads per array per warp), the
+// 8-node gathers hit the packed fields, which stay L2-resident (14 MB at
+// 128x64x64 cells).
+#include "grid_ctx.h"
+
+namespace spb {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int TPB = 256;
+
+struct Moments10 {
+  float *m[10];
+};
+
+// The double product (x - start) * inv, limited to [-8, n + 8] so that the
+// int conversion below never overflows (NaN maps to -8). Exact for every
+// position inside the grid, where the limit does not bite.
+__device__ __forceinline__ double cell_coord(float p, double start, float inv, int n) {
+  const double d = ((double)p - start) * (double)inv;
+  return fmin(fmax(d, -8.0), (double)n + 8.0);
+}
+
+// Reference cell index of the mover: 2 + int((x - xStart) * invdx), the
+// product in double, truncated toward zero (src/Mover.cpp:39-41).
+__device__ __forceinline__ int cell_trunc(float p, double start, float inv, int n) {
+  return 2 + __double2int_rz(cell_coord(p, start, inv, n));
+}
+
+// Reference cell index of the deposit: 2 + int(floor(...)) (src/Mover.cpp:399-401).
+__device__ __forceinline__ int cell_floor(float p, double start, float inv, int n) {
+  return 2 + __double2int_rd(cell_coord(p, start, inv, n));
+}
+
+// Keeps the node pair (i-1, i) inside [0, n-1]. The reference reads out of
+// bounds for such particles; here they are flagged and clamped.
+__device__ __forceinline__ int clamp_cell(int i, int n, int &bad) {
+  if (i < 1) { bad = 1; return 1; }
+  if (i > n - 1) { bad = 1; return n - 1; }
+  return i;
+}
+
+// Particle boundary condition on one axis (src/Mover.cpp:103-157): an
+// "above L" test in double, then a separate "below 0" test in float.
+__device__ __forceinline__ void bc_axis(float &pos, float &vel, double L, int periodic) {
+  if ((double)pos > L) {
+    if (periodic) {
+      pos = (float)((double)pos - L);
+    } else {
+      vel = -vel;
+      pos = (float)(2.0 * L - (double)pos);
+    }
+  }
+  if (pos < 0.0f) {
+    if (periodic) {
+      pos = (float)((double)pos + L);
+    } else {
+      vel = -vel;
+      pos = -pos;
+    }
+  }
+}
+
+// Particle boundary condition of mover_PC_V (src/Mover.cpp:296-379): the
+// periodic branch is mover_PC's; the reflecting branch first mirrors the
+// position, then flips the velocity only if the MIRRORED position is still
+// outside [0, L].
+__device__ __forceinline__ void bc_axis_v(float &pos, float &vel, double L, int periodic) {
+  if (periodic) {
+    if ((double)pos > L) pos = (float)((double)pos - L);
+    if (pos < 0.0f) pos = (float)((double)pos + L);
+  } else {
+    if ((double)pos > L) pos = (float)(2.0 * L - (double)pos);
+    if (pos < 0.0f) pos = -pos;
+    if ((double)pos > L) vel = -vel;
+    if (pos < 0.0f) vel = -vel;
+  }
+}
+
+// One particle of mover_PC (src/Mover.cpp:33-157); BCV = 1 gives mover_PC_V's
+// boundary handling instead.
+template <int BCV>
+__device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
+                                         const PackedFields &F, float &x, float &y,
+                                         float &z, float &u, float &v, float &w,
+                                         int &bad) {
+  const float xpt = x, ypt = y, zpt = z;
+  const float qomdt2 = p.qomdt2;
+  float upt = 0.0f, vpt = 0.0f, wpt = 0.0f;
+  float xc = x, yc = y, zc = z;
+  const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
+  for (int it = 0; it < p.niter; ++it) {
+    const int ix = clamp_cell(cell_trunc(xc, g.xStart, g.invdx, g.nxn), g.nxn, bad);
+    const int iy = clamp_cell(cell_trunc(yc, g.yStart, g.invdy, g.nyn), g.nyn, bad);
+    const int iz = clamp_cell(cell_trunc(zc, g.zStart, g.invdz, g.nzn), g.nzn, bad);
+    const float xi[2] = {xc - __ldg(g.xn + ix - 1), __ldg(g.xn + ix) - xc};
+    const float eta[2] = {yc - __ldg(g.yn + iy - 1), __ldg(g.yn + iy) - yc};
+    const float zeta[2] = {zc - __ldg(g.zn + iz - 1), __ldg(g.zn + iz) - zc};
+    float Ex = 0.0f, Ey = 0.0f, Ez = 0.0f, Bx = 0.0f, By = 0.0f, Bz = 0.0f;
+    const long base = ix * sx + iy * sy + iz;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const float wgt = xi[a] * eta[b] * zeta[c] * g.invVOL;
+          const long n = base - a * sx - b * sy - c;
+          const float4 f4 = __ldg(F.eb4 + n);
+          const float2 f2 = __ldg(F.eb2 + n);
+          Ex += wgt * f4.x;
+          Ey += wgt * f4.y;
+          Ez += wgt * f4.z;
+          Bx += wgt * f4.w;
+          By += wgt * f2.x;
+          Bz += wgt * f2.y;
+        }
+    const float omdtsq = qomdt2 * qomdt2 * (Bx * Bx + By * By + Bz * Bz);
+    const float denom = (float)(1.0 / (1.0 + (double)omdtsq));
+    const float ut = u + qomdt2 * Ex;
+    const float vt = v + qomdt2 * Ey;
+    const float wt = w + qomdt2 * Ez;
+    const float udotb = ut * Bx + vt * By + wt * Bz;
+    upt = (ut + qomdt2 * (vt * Bz - wt * By + qomdt2 * udotb * Bx)) * denom;
+    vpt = (vt + qomdt2 * (wt * Bx - ut * Bz + qomdt2 * udotb * By)) * denom;
+    wpt = (wt + qomdt2 * (ut * By - vt * Bx + qomdt2 * udotb * Bz)) * denom;
+    xc = xpt + upt * p.dto2;
+    yc = ypt + vpt * p.dto2;
+    zc = zpt + wpt * p.dto2;
+  }
+  u = (float)(2.0 * (double)upt - (double)u);
+  v = (float)(2.0 * (double)vpt - (double)v);
+  w = (float)(2.0 * (double)wpt - (double)w);
+  x = xpt + upt * p.dt_sub;
+  y = ypt + vpt * p.dt_sub;
+  z = zpt + wpt * p.dt_sub;
+  if (BCV == 0) {
+    bc_axis(x, u, g.Lx, p.periodic[0]);
+    bc_axis(y, v, g.Ly, p.periodic[1]);
+    bc_axis(z, w, g.Lz, p.periodic[2]);
+  } else {
+    bc_axis_v(x, u, g.Lx, p.periodic[0]);
+    bc_axis_v(y, v, g.Ly, p.periodic[1]);
+    bc_axis_v(z, w, g.Lz, p.periodic[2]);
+  }
+}
+
+// The 80 summands of one particle (src/Mover.cpp:399-570), value index
+// node*10 + moment with node = a*4 + b*2 + c for the node (ix-a, iy-b, iz-c).
+// Returns the linear index of node (ix, iy, iz).
+__device__ __forceinline__ long deposit_terms(const GeomDev &g, float x, float y,
+                                              float z, float u, float v, float w,
+                                              float q, float (&t)[80], int &bad) {
+  const int ix = clamp_cell(cell_floor(x, g.xStart, g.invdx, g.nxn), g.nxn, bad);
+  const int iy = clamp_cell(cell_floor(y, g.yStart, g.invdy, g.nyn), g.nyn, bad);
+  const int iz = clamp_cell(cell_floor(z, g.zStart, g.invdz, g.nzn), g.nzn, bad);
+  const float xi[2] = {x - __ldg(g.xn + ix - 1), __ldg(g.xn + ix) - x};
+  const float eta[2] = {y - __ldg(g.yn + iy - 1), __ldg(g.yn + iy) - y};
+  const float zeta[2] = {z - __ldg(g.zn + iz - 1), __ldg(g.zn + iz) - z};
+  const float uu = u * u, uv = u * v, uw = u * w, vv = v * v, vw = v * w, ww = w * w;
+  const float inv = g.invVOL;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const float wgt = q * xi[a] * eta[b] * zeta[c] * inv;
+        float *o = t + (a * 4 + b * 2 + c) * 10;
+        o[0] = wgt * inv;
+        o[1] = (u * wgt) * inv;
+        o[2] = (v * wgt) * inv;
+        o[3] = (w * wgt) * inv;
+        o[4] = (uu * wgt) * inv;
+        o[5] = (uv * wgt) * inv;
+        o[6] = (uw * wgt) * inv;
+        o[7] = (vv * wgt) * inv;
+        o[8] = (vw * wgt) * inv;
+        o[9] = (ww * wgt) * inv;
+      }
+  return ((long)ix * g.nyn + iy) * g.nzn + iz;
+}
+
+// Sums t[0..79] over the 32 lanes by recursive halving: at each xor-step
+// every lane keeps half of its values and receives the partner's partial sums
+// of that half (40+20+10+5+5 shuffles in all). Afterwards slot i (0..4) of
+// lane l holds the warp total of value index
+//   i + 5*b1 + 10*b2 + 20*b3 + 40*b4,  bK = bit K of l,
+// replicated in both lanes of each pair (l, l^1).
+__device__ __forceinline__ void warp_reduce80(float (&t)[80], int lane) {
+  {
+    const bool h = lane & 16;
+#pragma unroll
+    for (int i = 0; i < 40; ++i) {
+      const float send = h ? t[i] : t[i + 40];
+      const float keep = h ? t[i + 40] : t[i];
+      t[i] = keep + __shfl_xor_sync(FULL, send, 16);
+    }
+  }
+  {
+    const bool h = lane & 8;
+#pragma unroll
+    for (int i = 0; i < 20; ++i) {
+      const float send = h ? t[i] : t[i + 20];
+      const float keep = h ? t[i + 20] : t[i];
+      t[i] = keep + __shfl_xor_sync(FULL, send, 8);
+    }
+  }
+  {
+    const bool h = lane & 4;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      const float send = h ? t[i] : t[i + 10];
+      const float keep = h ? t[i + 10] : t[i];
+      t[i] = keep + __shfl_xor_sync(FULL, send, 4);
+    }
+  }
+  {
+    const bool h = lane & 2;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const float send = h ? t[i] : t[i + 5];
+      const float keep = h ? t[i + 5] : t[i];
+      t[i] = keep + __shfl_xor_sync(FULL, send, 2);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) t[i] += __shfl_xor_sync(FULL, t[i], 1);
+}
+
+// Adds one warp's deposits to the moments. Warps whose valid lanes all sit in
+// one cell (the common case for cell-sorted particles) reduce in registers
+// and issue 80 atomics for the warp; other warps issue 80 per lane.
+__device__ __forceinline__ void deposit_warp(const GeomDev &g, const Moments10 &M,
+                                             bool valid, long key, float (&t)[80]) {
+  const int lane = threadIdx.x & 31;
+  const long k = valid ? key : -1;
+  const unsigned peers = __match_any_sync(FULL, k);
+  const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
+  if (__all_sync(FULL, valid && peers == FULL)) {
+    warp_reduce80(t, lane);
+    const int hi = 5 * ((lane >> 1) & 1) + 10 * ((lane >> 2) & 1) + 20 * ((lane >> 3) & 1) +
+                   40 * ((lane >> 4) & 1);
+    const int lo = (lane & 1) ? 3 : 0, cnt = (lane & 1) ? 2 : 3;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (i >= lo && i < lo + cnt) {
+        const int idx = hi + i;
+        const int node = idx / 10, m = idx % 10;
+        const long n = key - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);
+        atomicAdd(M.m[m] + n, t[i]);
+      }
+    }
+  } else if (valid) {
+#pragma unroll
+    for (int node = 0; node < 8; ++node) {
+      const long n = key - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);
+#pragma unroll
+      for (int m = 0; m < 10; ++m) atomicAdd(M.m[m] + n, t[node * 10 + m]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TPB) k_pack_fields(const float *__restrict__ ex,
+                                                     const float *__restrict__ ey,
+                                                     const float *__restrict__ ez,
+                                                     const float *__restrict__ bx,
+                                                     const float *__restrict__ by,
+                                                     const float *__restrict__ bz,
+                                                     float4 *__restrict__ eb4,
+                                                     float2 *__restrict__ eb2, long nodes) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nodes;
+       i += (long)gridDim.x * blockDim.x) {
+    eb4[i] = make_float4(ex[i], ey[i], ez[i], bx[i]);
+    eb2[i] = make_float2(by[i], bz[i]);
+  }
+}
+
+template <int BCV>
+__global__ void __launch_bounds__(TPB) k_plain_mover(GeomDev g, PushDev p, PackedFields F,
+                                                     float *__restrict__ x, float *__restrict__ y,
+                                                     float *__restrict__ z, float *__restrict__ u,
+                                                     float *__restrict__ v, float *__restrict__ w,
+                                                     long n, int *__restrict__ err) {
+  const long i = blockIdx.x * (long)TPB + threadIdx.x;
+  if (i >= n) return;
+  float px = x[i], py = y[i], pz = z[i], pu = u[i], pv = v[i], pw = w[i];
+  int bad = 0;
+  move_one<BCV>(g, p, F, px, py, pz, pu, pv, pw, bad);
+  x[i] = px;
+  y[i] = py;
+  z[i] = pz;
+  u[i] = pu;
+  v[i] = pv;
+  w[i] = pw;
+  if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
+__global__ void __launch_bounds__(TPB) k_plain_p2g(GeomDev g, const float *__restrict__ x,
+                                                   const float *__restrict__ y,
+                                                   const float *__restrict__ z,
+                                                   const float *__restrict__ u,
+                                                   const float *__restrict__ v,
+                                                   const float *__restrict__ w,
+                                                   const float *__restrict__ q, long n,
+                                                   Moments10 M, int *__restrict__ err) {
+  const long i = blockIdx.x * (long)TPB + threadIdx.x;
+  const bool valid = i < n;
+  float t[80];
+  long key = 0;
+  int bad = 0;
+  if (valid) {
+    key = deposit_terms(g, x[i], y[i], z[i], u[i], v[i], w[i], q[i], t, bad);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 80; ++j) t[j] = 0.0f;
+  }
+  deposit_warp(g, M, valid, key, t);
+  if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
+__global__ void __launch_bounds__(TPB) k_plain_mover_interp(
+    GeomDev g, PushDev p, PackedFields F, float *__restrict__ x, float *__restrict__ y,
+    float *__restrict__ z, float *__restrict__ u, float *__restrict__ v,
+    float *__restrict__ w, const float *__restrict__ q, long n, Moments10 M,
+    int *__restrict__ err) {
+  const long i = blockIdx.x * (long)TPB + threadIdx.x;
+  const bool valid = i < n;
+  float t[80];
+  long key = 0;
+  int bad = 0;
+  if (valid) {
+    float px = x[i], py = y[i], pz = z[i], pu = u[i], pv = v[i], pw = w[i];
+    move_one<0>(g, p, F, px, py, pz, pu, pv, pw, bad);
+    x[i] = px;
+    y[i] = py;
+    z[i] = pz;
+    u[i] = pu;
+    v[i] = pv;
+    w[i] = pw;
+    key = deposit_terms(g, px, py, pz, pu, pv, pw, q[i], t, bad);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 80; ++j) t[j] = 0.0f;
+  }
+  deposit_warp(g, M, valid, key, t);
+  if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
+// applyBCids (src/BC.cpp:362-615), one launch per step so the axis order of
+// the reference holds: periodic folds X, Y, Z, then non-periodic doubling X,
+// Y, Z. Thread t handles one (row, col) pair of the boundary planes of all
+// ten moments.
+__global__ void __launch_bounds__(TPB) k_bc_fold(Moments10 M, int nxn, int nyn, int nzn,
+                                                 int axis, int periodic) {
+  int n1, n2;
+  if (axis == 0) {
+    n1 = nyn - 2;
+    n2 = nzn - 2;
+  } else if (axis == 1) {
+    n1 = nxn - 2;
+    n2 = nzn - 2;
+  } else {
+    n1 = nxn - 2;
+    n2 = nyn - 2;
+  }
+  const long t = blockIdx.x * (long)TPB + threadIdx.x;
+  if (t >= (long)n1 * n2) return;
+  const int r = 1 + (int)(t / n2), s = 1 + (int)(t % n2);
+  long lo, hi;
+  if (axis == 0) {
+    lo = ((long)1 * nyn + r) * nzn + s;
+    hi = ((long)(nxn - 2) * nyn + r) * nzn + s;
+  } else if (axis == 1) {
+    lo = ((long)r * nyn + 1) * nzn + s;
+    hi = ((long)r * nyn + (nyn - 2)) * nzn + s;
+  } else {
+    lo = ((long)r * nyn + s) * nzn + 1;
+    hi = ((long)r * nyn + s) * nzn + (nzn - 2);
+  }
+#pragma unroll
+  for (int m = 0; m < 10; ++m) {
+    float *a = M.m[m];
+    if (periodic) {
+      const float sum = a[lo] + a[hi];
+      a[lo] = sum;
+      a[hi] = sum;
+    } else {
+      a[lo] *= 2.0f;
+      a[hi] *= 2.0f;
+    }
+  }
+}
+
+inline unsigned blocks_for(long n) { return (unsigned)ceil_div(n, TPB); }
+
+}  // namespace
+
+int launch_pack_fields(const float *const f[6], float4 *eb4, float2 *eb2, long nodes,
+                       cudaStream_t s) {
+  const unsigned blocks = (unsigned)std::min<long>(ceil_div(nodes, TPB), 4096);
+  k_pack_fields<<<blocks, TPB, 0, s>>>(f[0], f[1], f[2], f[3], f[4], f[5], eb4, eb2, nodes);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
+int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F, float *x,
+                       float *y, float *z, float *u, float *v, float *w, long n, int *err,
+                       cudaStream_t s, int bc_variant) {
+  if (n <= 0) return SPB_OK;
+  if (bc_variant == 0)
+    k_plain_mover<0><<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, n, err);
+  else
+    k_plain_mover<1><<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, n, err);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
+int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
+                     const float *u, const float *v, const float *w, const float *q, long n,
+                     float *const mom[10], int *err, cudaStream_t s) {
+  if (n <= 0) return SPB_OK;
+  Moments10 M;
+  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  k_plain_p2g<<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, M, err);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
+int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFields &F,
+                              float *x, float *y, float *z, float *u, float *v, float *w,
+                              const float *q, long n, float *const mom[10], int *err,
+                              cudaStream_t s) {
+  if (n <= 0) return SPB_OK;
+  Moments10 M;
+  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  k_plain_mover_interp<<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n, M, err);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
+int launch_apply_bc_ids(int nxn, int nyn, int nzn, const int periodic[3],
+                        float *const mom[10], cudaStream_t s, long *launches) {
+  Moments10 M;
+  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  const long plane[3] = {(long)(nyn - 2) * (nzn - 2), (long)(nxn - 2) * (nzn - 2),
+                         (long)(nxn - 2) * (nyn - 2)};
+  // periodic folds in axis order, then the doubling of non-periodic axes
+  for (int pass = 0; pass < 2; ++pass)
+    for (int axis = 0; axis < 3; ++axis) {
+      const bool fold = periodic[axis] != 0;
+      if (fold != (pass == 0)) continue;
+      k_bc_fold<<<blocks_for(plane[axis]), TPB, 0, s>>>(M, nxn, nyn, nzn, axis, fold ? 1 : 0);
+      SPB_CUDA(cudaGetLastError());
+      g_launches++;
+      if (launches) ++*launches;
+    }
+  return SPB_OK;
+}
+
+}  // namespace spb

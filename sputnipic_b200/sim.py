@@ -1,0 +1,114 @@
+"""Precision form: a device-resident simulation of the mover + deposit
+(spb_sim_* of libsputnipic_b200.so) over torch CUDA tensors.
+
+Particles are kept in HBM as int32 cell + FP32 in-cell offsets, cell-sorted;
+one fused kernel per cycle pushes all species (FP32) and deposits the ten
+moments into FP64 global arrays. See include/sputnipic_b200.h.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+
+
+def _stream(stream):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Simulation:
+    def __init__(self, wl, tile=(8, 4, 4), resort_every=1, ctas=0, species=None):
+        self.lib = _lib.load()
+        self.wl = wl
+        species = list(range(len(wl.species))) if species is None else list(species)
+        d = _lib.SimDesc()
+        d.nxc, d.nyc, d.nzc = wl.nxc, wl.nyc, wl.nzc
+        d.Lx, d.Ly, d.Lz = wl.Lx, wl.Ly, wl.Lz
+        d.dt, d.c, d.niter = wl.dt, wl.c, wl.niter
+        for a in range(3):
+            d.periodic[a] = 1 if wl.periodic[a] else 0
+        d.ns = len(species)
+        for i, s in enumerate(species):
+            d.qom[i] = wl.species[s].qom
+        for a in range(3):
+            d.tile[a] = tile[a]
+        d.resort_every, d.ctas = resort_every, ctas
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.spb_sim_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+        self.desc = d
+        self.ns = d.ns
+        self.nodes = self.lib.spb_sim_nodes(h)
+
+    def close(self):
+        if self.h:
+            self.lib.spb_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return self.lib.spb_sim_launches(self.h)
+
+    def count(self, s: int) -> int:
+        return self.lib.spb_sim_count(self.h, s)
+
+    def set_fields(self, fields, stream=None):
+        """Six float32 tensors (CUDA or CPU) Ex, Ey, Ez, Bxn, Byn, Bzn."""
+        on_dev = int(fields[0].is_cuda)
+        arr = (ctypes.c_void_p * 6)(*[f.data_ptr() for f in fields])
+        _lib.check(self.lib.spb_sim_set_fields(self.h, arr, on_dev, _stream(stream)))
+
+    def load_species(self, s: int, part: dict, stream=None):
+        """part: float32 tensors x, y, z, u, v, w, q (CUDA or CPU)."""
+        on_dev = int(part["x"].is_cuda)
+        n = part["x"].numel()
+        _lib.check(self.lib.spb_sim_load_species(
+            self.h, s, *[part[k].data_ptr() for k in "xyzuvwq"], n, on_dev, _stream(stream)))
+
+    def cycle(self, ncycles: int = 1, stream=None):
+        _lib.check(self.lib.spb_sim_cycle(self.h, ncycles, _stream(stream)))
+
+    def resort(self, stream=None):
+        _lib.check(self.lib.spb_sim_resort(self.h, _stream(stream)))
+
+    def moments(self, s: int, bc: bool = False, stream=None):
+        """FP64 moments of species s as a (10, nodes) CUDA tensor (a copy).
+        bc=True applies applyBCids to the simulation's moments first."""
+        import torch
+        if bc:
+            _lib.check(self.lib.spb_sim_apply_bc_ids(self.h, s, _stream(stream)))
+        out = torch.empty(10, self.nodes, dtype=torch.float64, device="cuda")
+        _lib.check(self.lib.spb_sim_moments(self.h, s, out.data_ptr(), 1, _stream(stream)))
+        return out
+
+    def particles(self, s: int, stream=None) -> dict:
+        """Positions (domain units), velocities and charges of species s,
+        float32 CUDA tensors in the simulation's (sorted) order."""
+        import torch
+        n = self.count(s)
+        out = {k: torch.empty(n, dtype=torch.float32, device="cuda") for k in "xyzuvwq"}
+        _lib.check(self.lib.spb_sim_particles(self.h, s, *[out[k].data_ptr() for k in "xyzuvwq"],
+                                              1, _stream(stream)))
+        return out
+
+    def check(self, stream=None) -> int:
+        return self.lib.spb_sim_check(self.h, _stream(stream))
+
+    def set_timing(self, on: bool = True):
+        _lib.check(self.lib.spb_sim_set_timing(self.h, 1 if on else 0))
+
+    def timing(self):
+        """(cycle kernel ms, launches, sort ms, sorts) since the last call."""
+        c, nc, o, no = ctypes.c_double(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        _lib.check(self.lib.spb_sim_timing(self.h, ctypes.byref(c), ctypes.byref(nc),
+                                           ctypes.byref(o), ctypes.byref(no)))
+        return c.value, nc.value, o.value, no.value
