@@ -271,7 +271,12 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     from sputnipic_b200.sim import Simulation
     ns = len(parts)
     n = sum(p["x"].numel() for p in parts)
-    sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort)
+    tune = None
+    if args.autotune:
+        from sputnipic_b200.sim import autotune
+        tune = autotune(wl, fields, parts)
+        args.tile, args.variant, args.resort = list(tune["tile"]), tune["variant"], tune["resort_every"]
+    sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort, variant=args.variant)
     sim.set_fields(fields)
     for s, p in enumerate(parts):
         sim.load_species(s, p)
@@ -312,7 +317,7 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     }
     sim.close()
     return {"value": n * world * args.steps / (ms / 1e3), "ms": ms, "roofline": roofline,
-            "clocks": clk.summary(), "launches": launches}
+            "clocks": clk.summary(), "launches": launches, "autotune": tune}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -374,6 +379,8 @@ def run_ours(args, rank, world, local_rank):
                        "form": "precision (int32 cell + fp32 offset, fp32 push, "
                                "fp32 smem partials -> fp64 moments)",
                        "tile": list(args.tile), "resort_every": args.resort,
+                       "deposit_variant": args.variant,
+                       "autotune": prec["autotune"],
                        "particles_per_gpu": ntot, "grid_cells": [wl.nxc, wl.nyc, wl.nzc],
                        "parallelism": f"particle decomposition x{world}" if world > 1 else "1 GPU",
                        "l2": "particle arrays (8.4 GB) exceed the 126 MB L2; no flush needed"},
@@ -457,6 +464,9 @@ def main():
                     help="smaller profiling cases only; the benchmark uses 125")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--resort", type=int, default=4)
+    ap.add_argument("--variant", type=int, default=1)
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick tile, deposit variant and resort interval first")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

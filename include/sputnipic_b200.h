@@ -204,7 +204,9 @@ typedef struct spb_sim_desc {
   long capacity[SPB_SIM_MAX_SPECIES]; /* optional: particles to reserve for */
   int tile[3];              /* cells per tile (0,0,0: default 8x4x4) */
   int resort_every;         /* cycles between counting sorts (>= 1) */
-  int ctas;                 /* persistent CTAs (0: one per SM) */
+  int ctas;                 /* persistent CTAs (0: one or two per SM) */
+  int variant;              /* deposit: 0 per-lane register sums per cell,
+                               1 warp sums per 32 particles (more occupancy) */
 } spb_sim_desc;
 
 /* Whether a tile shape has an instantiated kernel. */

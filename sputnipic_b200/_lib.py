@@ -135,7 +135,8 @@ class SimDesc(ctypes.Structure):
                 ("Lx", c_double), ("Ly", c_double), ("Lz", c_double),
                 ("dt", c_double), ("c", c_double), ("niter", c_int), ("periodic", c_int * 3),
                 ("ns", c_int), ("qom", c_double * 8), ("capacity", c_long * 8),
-                ("tile", c_int * 3), ("resort_every", c_int), ("ctas", c_int)]
+                ("tile", c_int * 3), ("resort_every", c_int), ("ctas", c_int),
+                ("variant", c_int)]
 
 
 def ctypes_layout() -> dict:

@@ -244,17 +244,26 @@ __device__ __forceinline__ void warp_reduce80(float (&t)[80], int lane) {
   for (int i = 0; i < 5; ++i) t[i] += __shfl_xor_sync(FULL, t[i], 1);
 }
 
-// Adds one warp's deposits to the moments. Warps whose valid lanes all sit in
-// one cell (the common case for cell-sorted particles) reduce in registers
-// and issue 80 atomics for the warp; other warps issue 80 per lane.
+// Adds one warp's deposits to the moments. For each of up to four distinct
+// cells among the warp's particles (cell-sorted particles give one or two),
+// the warp sums the members' 80 terms in registers and issues 80 atomics;
+// particles of further cells (unsorted input) issue 80 atomics each.
 __device__ __forceinline__ void deposit_warp(const GeomDev &g, const Moments10 &M,
                                              bool valid, long key, float (&t)[80]) {
   const int lane = threadIdx.x & 31;
-  const long k = valid ? key : -1;
-  const unsigned peers = __match_any_sync(FULL, k);
   const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
-  if (__all_sync(FULL, valid && peers == FULL)) {
-    warp_reduce80(t, lane);
+  unsigned remaining = __ballot_sync(FULL, valid);
+  for (int round = 0; round < 4 && remaining; ++round) {
+    const int leader = __ffs(remaining) - 1;
+    const long k = __shfl_sync(FULL, key, leader);
+    const bool member = valid && key == k;
+    const unsigned members = __ballot_sync(FULL, member);
+    remaining &= ~members;
+    if (__popc(members) < 2 && round > 0) continue;   // lone particle: direct atomics below
+    float r[80];
+#pragma unroll
+    for (int j = 0; j < 80; ++j) r[j] = member ? t[j] : 0.0f;
+    warp_reduce80(r, lane);
     const int hi = 5 * ((lane >> 1) & 1) + 10 * ((lane >> 2) & 1) + 20 * ((lane >> 3) & 1) +
                    40 * ((lane >> 4) & 1);
     const int lo = (lane & 1) ? 3 : 0, cnt = (lane & 1) ? 2 : 3;
@@ -263,11 +272,13 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const Moments10 &
       if (i >= lo && i < lo + cnt) {
         const int idx = hi + i;
         const int node = idx / 10, m = idx % 10;
-        const long n = key - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);
-        atomicAdd(M.m[m] + n, t[i]);
+        const long n = k - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);
+        atomicAdd(M.m[m] + n, r[i]);
       }
     }
-  } else if (valid) {
+    if (member) valid = false;   // done
+  }
+  if (valid) {
 #pragma unroll
     for (int node = 0; node < 8; ++node) {
       const long n = key - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);

@@ -161,17 +161,18 @@ __device__ __forceinline__ void advance(int &c, float &o, float disp, int N) {
   }
 }
 
+// E and B as three packed pairs (Ex,Ey), (Ez,Bx), (By,Bz): the node record in
+// shared memory is (Ex,Ey,Ez,Bx | By,Bz,0,0), so every pair is a register
+// pair and one packed FP32x2 FMA updates two components.
 struct Field6 {
-  float ex, ey, ez, bx, by, bz;
+  float2 exy, ezbx, byz;
 };
 
 __device__ __forceinline__ void acc_node(Field6 &F, float w, float4 a, float2 b) {
-  F.ex = fmaf(w, a.x, F.ex);
-  F.ey = fmaf(w, a.y, F.ey);
-  F.ez = fmaf(w, a.z, F.ez);
-  F.bx = fmaf(w, a.w, F.bx);
-  F.by = fmaf(w, b.x, F.by);
-  F.bz = fmaf(w, b.y, F.bz);
+  const float2 w2 = make_float2(w, w);
+  F.exy = __ffma2_rn(w2, make_float2(a.x, a.y), F.exy);
+  F.ezbx = __ffma2_rn(w2, make_float2(a.z, a.w), F.ezbx);
+  F.byz = __ffma2_rn(w2, b, F.byz);
 }
 
 template <int TX, int TY, int TZ>
@@ -189,7 +190,7 @@ __device__ __forceinline__ Field6 gather(const CycleParams &P, const float *__re
                                          float fx, float fy, float fz) {
   using T = Tile<TX, TY, TZ>;
   const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
-  Field6 F = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  Field6 F = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   const int bx = gx + 1 - c0x, by = gy + 1 - c0y, bz = gz + 1 - c0z;
   if ((unsigned)bx <= (unsigned)(TX + 1) && (unsigned)by <= (unsigned)(TY + 1) &&
       (unsigned)bz <= (unsigned)(TZ + 1)) {
@@ -235,22 +236,27 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
                                      int &bad) {
   float dx = 0.f, dy = 0.f, dz = 0.f;   // predicted displacement in cells
   float up = 0.f, vp = 0.f, wp = 0.f;
+#pragma unroll 1
   for (int it = 0; it < P.niter; ++it) {
-    int gx, gy, gz;
-    float fx, fy, fz;
-    locate(ox + dx, cx, P.nxc, gx, fx, bad);
-    locate(oy + dy, cy, P.nyc, gy, fy, bad);
-    locate(oz + dz, cz, P.nzc, gz, fz, bad);
+    int gx = cx, gy = cy, gz = cz;
+    float fx = ox, fy = oy, fz = oz;
+    if (it > 0) {   // the first gather is at the start position: (c, o) as stored
+      locate(ox + dx, cx, P.nxc, gx, fx, bad);
+      locate(oy + dy, cy, P.nyc, gy, fy, bad);
+      locate(oz + dz, cz, P.nzc, gz, fz, bad);
+    }
     const Field6 F = gather<TX, TY, TZ>(P, sF, c0x, c0y, c0z, gx, gy, gz, fx, fy, fz);
-    const float omdtsq = qomdt2 * qomdt2 * (F.bx * F.bx + F.by * F.by + F.bz * F.bz);
+    const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
+    const float bx = F.ezbx.y, by = F.byz.x, bz = F.byz.y;
+    const float omdtsq = qomdt2 * qomdt2 * (bx * bx + by * by + bz * bz);
     const float denom = __frcp_rn(1.0f + omdtsq);
-    const float ut = fmaf(qomdt2, F.ex, u);
-    const float vt = fmaf(qomdt2, F.ey, v);
-    const float wt = fmaf(qomdt2, F.ez, w);
-    const float qud = qomdt2 * (ut * F.bx + vt * F.by + wt * F.bz);
-    up = fmaf(qomdt2, vt * F.bz - wt * F.by + qud * F.bx, ut) * denom;
-    vp = fmaf(qomdt2, wt * F.bx - ut * F.bz + qud * F.by, vt) * denom;
-    wp = fmaf(qomdt2, ut * F.by - vt * F.bx + qud * F.bz, wt) * denom;
+    const float ut = fmaf(qomdt2, ex, u);
+    const float vt = fmaf(qomdt2, ey, v);
+    const float wt = fmaf(qomdt2, ez, w);
+    const float qud = qomdt2 * (ut * bx + vt * by + wt * bz);
+    up = fmaf(qomdt2, vt * bz - wt * by + qud * bx, ut) * denom;
+    vp = fmaf(qomdt2, wt * bx - ut * bz + qud * by, vt) * denom;
+    wp = fmaf(qomdt2, ut * by - vt * bx + qud * bz, wt) * denom;
     dx = up * P.hdt[0];
     dy = vp * P.hdt[1];
     dz = wp * P.hdt[2];
@@ -272,51 +278,60 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   }
 }
 
-// 80 deposit terms of one particle: 8 node weights (q folded into x) x 10
-// moment factors 1, u, v, w, uu, uv, uw, vv, vw, ww. Index node*10 + m,
-// node = a*4 + b*2 + c, where a/b/c = 1 selects the upper node on that axis,
-// XOR-permuted by lane bits 4/3/2 (see warp_sum80).
-__device__ __forceinline__ void add_terms(float (&acc)[80], float q, float ox, float oy, float oz,
+// Deposit terms of one particle added to 40 packed accumulators:
+// acc[node*5 + k] += W_node * (mf[k], mf[k+5]) with the moment factors
+// mf = 1, u, v, w, uu | uv, uw, vv, vw, ww, i.e. the pairs (1,uv) (u,uw)
+// (v,vv) (w,vw) (uu,ww). node = a*4 + b*2 + c, a/b/c = 1 the upper node on
+// that axis, XOR-permuted by lane bits 4/3/2 (see warp_sum80). q is folded
+// into the x weights; q = 0 adds nothing.
+__device__ __forceinline__ void add_terms(float2 (&acc)[40], float q, float ox, float oy, float oz,
                                           float u, float v, float w, int lane) {
   const bool px = lane & 16, py = lane & 8, pz = lane & 4;
   const float lox = 1.0f - ox, loy = 1.0f - oy, loz = 1.0f - oz;
   const float wx0 = q * (px ? ox : lox), wx1 = q * (px ? lox : ox);
   const float wy0 = py ? oy : loy, wy1 = py ? loy : oy;
   const float wz0 = pz ? oz : loz, wz1 = pz ? loz : oz;
-  const float mf[10] = {1.0f, u, v, w, u * u, u * v, u * w, v * v, v * w, w * w};
+  const float2 mf[5] = {make_float2(1.0f, u * v), make_float2(u, u * w), make_float2(v, v * v),
+                        make_float2(w, v * w), make_float2(u * u, w * w)};
   const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
 #pragma unroll
   for (int ab = 0; ab < 4; ++ab) {
     const float W0 = wxy[ab] * wz0, W1 = wxy[ab] * wz1;
+    const float2 W02 = make_float2(W0, W0), W12 = make_float2(W1, W1);
 #pragma unroll
-    for (int m = 0; m < 10; ++m) {
-      acc[(ab * 2 + 0) * 10 + m] = fmaf(W0, mf[m], acc[(ab * 2 + 0) * 10 + m]);
-      acc[(ab * 2 + 1) * 10 + m] = fmaf(W1, mf[m], acc[(ab * 2 + 1) * 10 + m]);
+    for (int k = 0; k < 5; ++k) {
+      acc[(ab * 2 + 0) * 5 + k] = __ffma2_rn(W02, mf[k], acc[(ab * 2 + 0) * 5 + k]);
+      acc[(ab * 2 + 1) * 5 + k] = __ffma2_rn(W12, mf[k], acc[(ab * 2 + 1) * 5 + k]);
     }
   }
 }
 
-// Sums acc over the warp. Lanes hold their terms with the x/y/z node halves
-// swapped by lane bits 4/3/2, so the first three halving steps need no
-// selects: every lane keeps its lower half and receives its partner's upper
-// half. Afterwards lane l holds in acc[0..4] the totals of node
-// (a, b, c) = (bit4, bit3, bit2) of l, moments 5*bit1(l) .. 5*bit1(l)+4.
-__device__ __forceinline__ void warp_sum80(float (&acc)[80], int lane) {
+__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
+  return make_float2(__shfl_xor_sync(FULL, v.x, m), __shfl_xor_sync(FULL, v.y, m));
+}
+
+// Sums the packed accumulators over the warp. Lanes hold their terms with
+// the x/y/z node halves swapped by lane bits 4/3/2, so the first three
+// halving steps need no selects: every lane keeps its lower half and
+// receives its partner's upper half. Afterwards lane l holds in r[0..4] the
+// totals of node (a, b, c) = (bit4, bit3, bit2) of l, moments
+// 5*bit1(l) .. 5*bit1(l)+4 (reference order).
+__device__ __forceinline__ void warp_sum80(float2 (&acc)[40], float (&r)[5], int lane) {
 #pragma unroll
-  for (int i = 0; i < 40; ++i) acc[i] += __shfl_xor_sync(FULL, acc[i + 40], 16);
+  for (int i = 0; i < 20; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 20], 16));
 #pragma unroll
-  for (int i = 0; i < 20; ++i) acc[i] += __shfl_xor_sync(FULL, acc[i + 20], 8);
+  for (int i = 0; i < 10; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 10], 8));
 #pragma unroll
-  for (int i = 0; i < 10; ++i) acc[i] += __shfl_xor_sync(FULL, acc[i + 10], 4);
+  for (int i = 0; i < 5; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 5], 4));
   const bool h = lane & 2;
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const float send = h ? acc[i] : acc[i + 5];
-    const float keep = h ? acc[i + 5] : acc[i];
-    acc[i] = keep + __shfl_xor_sync(FULL, send, 2);
+  for (int k = 0; k < 5; ++k) {
+    const float send = h ? acc[k].x : acc[k].y;
+    const float keep = h ? acc[k].y : acc[k].x;
+    r[k] = keep + __shfl_xor_sync(FULL, send, 2);
   }
 #pragma unroll
-  for (int i = 0; i < 5; ++i) acc[i] += __shfl_xor_sync(FULL, acc[i], 1);
+  for (int k = 0; k < 5; ++k) r[k] += __shfl_xor_sync(FULL, r[k], 1);
 }
 
 struct MoverEntry {  // one queued deposit: final cell and state
@@ -369,42 +384,71 @@ __device__ __forceinline__ void deposit_scatter(const CycleParams &P, const Spec
   }
 }
 
+// Adds the warp totals of the segment cell's 8 nodes into the tile partials.
 template <int TX, int TY, int TZ>
-__global__ void __launch_bounds__(SIM_TPB, 1)
+__device__ __forceinline__ void flush_cell(float2 (&acc)[40], float *__restrict__ sAcc, int lx,
+                                           int ly, int lz, int lane) {
+  using T = Tile<TX, TY, TZ>;
+  float r[5];
+  warp_sum80(acc, r, lane);
+  const int a = (lane >> 4) & 1, bb = (lane >> 3) & 1, c = (lane >> 2) & 1;
+  const int mbase = 5 * ((lane >> 1) & 1);
+  const int n = ((lx + 1 + a) * T::BY + (ly + 1 + bb)) * T::BZ + (lz + 1 + c);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+    if (k >= lo && k < hi) atomicAdd(sAcc + (mbase + k) * T::BN + n, r[k]);
+}
+
+// ACC = true: each lane accumulates the terms of all its particles of a cell
+// in registers and the warp sums once per cell. ACC = false: the warp sums
+// after every 32 particles (fewer live registers, more occupancy).
+template <int TX, int TY, int TZ, bool ACC>
+__global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
     k_cycle(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P) {
   using T = Tile<TX, TY, TZ>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float *sF = reinterpret_cast<float *>(smem_raw);                  // BN * 8
-  float *sAcc = sF + 8 * T::BN;                                     // 10 * BN
+  float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x BN * 8
+  float *sAcc = sF0 + 2 * 8 * T::BN;                                // 10 * BN
   MoverEntry *sQ = reinterpret_cast<MoverEntry *>(sAcc + 10 * T::BN);  // NW * QCAP
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sQ + SIM_NW * QCAP);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sQ + SIM_NW * QCAP);   // 2 barriers
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   MoverEntry *myQ = sQ + warp * QCAP;
-  if (tid == 0) mbar_init(bar, 1);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+  }
   for (int i = tid; i < 10 * T::BN; i += SIM_TPB) sAcc[i] = 0.0f;
   __syncthreads();
 
   const int ntiles = P.ntx * P.nty * P.ntz;
   const long nodes = (long)P.nxn * P.nyn * P.nzn;
-  unsigned phase = 0;
-  int bad = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
-    const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
-    if (tid == 0) {
-      fence_proxy_async();
-      mbar_expect_tx(bar, (unsigned)(T::BN * 8 * sizeof(float)));
-      // box origin: node c0 on every axis (the lower node of halo cell c0-1)
-      tma_load_4d(sF, &fmap, 0, c0z, c0y, c0x, bar);
-    }
-    if (!mbar_wait_bounded(bar, phase)) {
+  const unsigned box_bytes = (unsigned)(T::BN * 8 * sizeof(float));
+  auto issue = [&](int t, int stage) {
+    const int z = t % P.ntz, y = (t / P.ntz) % P.nty, x = t / (P.ntz * P.nty);
+    fence_proxy_async();
+    mbar_expect_tx(bar + stage, box_bytes);
+    // box origin: node c0 on every axis (the lower node of halo cell c0-1)
+    tma_load_4d(sF0 + stage * 8 * T::BN, &fmap, 0, z * TZ, y * TY, x * TX, bar + stage);
+  };
+  if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  int bad = 0, it = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int stage = it & 1;
+    // prefetch the next tile's fields into the other stage (read by the
+    // previous tile, which every thread finished before the last barrier)
+    if (tid == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
+    if (!mbar_wait_bounded(bar + stage, (it >> 1) & 1)) {
       // the staged fields never arrived: report, wait once more, give up
       if (tid == 0) atomicOr(P.err, 2);
-      mbar_wait_bounded(bar, phase);
+      mbar_wait_bounded(bar + stage, (it >> 1) & 1);
+      mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
       return;
     }
-    phase ^= 1u;
+    const float *sF = sF0 + stage * 8 * T::BN;
+    const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
+    const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
 
     for (int s = 0; s < P.ns; ++s) {
       const SpeciesDev S = P.sp[s];
@@ -417,95 +461,64 @@ __global__ void __launch_bounds__(SIM_TPB, 1)
         if (b >= e) continue;
         const int lx = lc / (TY * TZ), ly = (lc / TZ) % TY, lz = lc % TZ;
         const uint32_t seg = pack_cell(c0x + lx, c0y + ly, c0z + lz);
-        float acc[80];
+        float2 acc[40];
+        if (ACC) {
 #pragma unroll
-        for (int i = 0; i < 80; ++i) acc[i] = 0.0f;
-        for (int cb = b & ~3; cb < e; cb += 128) {
-          const int i0 = cb + 4 * lane;
-          uint4 C = *reinterpret_cast<const uint4 *>(S.cell + i0);
-          float4 OX = *reinterpret_cast<const float4 *>(S.ox + i0);
-          float4 OY = *reinterpret_cast<const float4 *>(S.oy + i0);
-          float4 OZ = *reinterpret_cast<const float4 *>(S.oz + i0);
-          float4 U = *reinterpret_cast<const float4 *>(S.u + i0);
-          float4 V = *reinterpret_cast<const float4 *>(S.v + i0);
-          float4 W = *reinterpret_cast<const float4 *>(S.w + i0);
-          const float4 Q = *reinterpret_cast<const float4 *>(S.q + i0);
-          uint32_t *Cp = reinterpret_cast<uint32_t *>(&C);
-          float *pox = reinterpret_cast<float *>(&OX), *poy = reinterpret_cast<float *>(&OY);
-          float *poz = reinterpret_cast<float *>(&OZ), *pu = reinterpret_cast<float *>(&U);
-          float *pv = reinterpret_cast<float *>(&V), *pw = reinterpret_cast<float *>(&W);
-          const float *pq = reinterpret_cast<const float *>(&Q);
-          int nvalid = 0;
+          for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
+        }
+#pragma unroll 1
+        for (int base = b; base < e; base += 32) {
+          const int i = base + lane;
+          const bool valid = i < e;
+          uint32_t cell = 0;
+          float ox = 0.f, oy = 0.f, oz = 0.f, u = 0.f, v = 0.f, w = 0.f, q = 0.f;
+          if (valid) {
+            cell = S.cell[i];
+            ox = S.ox[i];
+            oy = S.oy[i];
+            oz = S.oz[i];
+            u = S.u[i];
+            v = S.v[i];
+            w = S.w[i];
+            q = S.q[i];
+            int cx = cell_x(cell), cy = cell_y(cell), cz = cell_z(cell);
+            push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, bad);
+            cell = pack_cell(cx, cy, cz);
+            S.cell[i] = cell;
+            S.ox[i] = ox;
+            S.oy[i] = oy;
+            S.oz[i] = oz;
+            S.u[i] = u;
+            S.v[i] = v;
+            S.w[i] = w;
+          }
+          const bool mover = valid && cell != seg;
+          // particles that stay in the segment cell: register terms
+          if (!ACC) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int i = i0 + j;
-            const bool valid = i >= b && i < e;
-            bool mover = false;
-            if (valid) {
-              ++nvalid;
-              int cx = cell_x(Cp[j]), cy = cell_y(Cp[j]), cz = cell_z(Cp[j]);
-              push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, qomdt2, cx, cy, cz, pox[j], poy[j],
-                               poz[j], pu[j], pv[j], pw[j], bad);
-              Cp[j] = pack_cell(cx, cy, cz);
-              if (Cp[j] == seg)
-                add_terms(acc, pq[j], pox[j], poy[j], poz[j], pu[j], pv[j], pw[j], lane);
-              else
-                mover = true;
+            for (int k = 0; k < 40; ++k) acc[k] = make_float2(0.f, 0.f);
+          }
+          add_terms(acc, (valid && !mover) ? q : 0.0f, ox, oy, oz, u, v, w, lane);
+          if (!ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane);
+          // particles that changed cell: per-warp queue, shared atomics
+          const unsigned mb = __ballot_sync(FULL, mover);
+          if (mb) {
+            if (mover) {
+              const int slot = qcount + __popc(mb & ((1u << lane) - 1u));
+              myQ[slot] = MoverEntry{cell, ox, oy, oz, q, u, v, w};
             }
-            // queue the movers of this slot (warp-converged)
-            const unsigned mb = __ballot_sync(FULL, mover);
-            if (mb) {
-              if (mover) {
-                const int slot = qcount + __popc(mb & ((1u << lane) - 1u));
-                myQ[slot] = MoverEntry{Cp[j], pox[j], poy[j], poz[j], pq[j], pu[j], pv[j], pw[j]};
-              }
-              qcount += __popc(mb);
+            qcount += __popc(mb);
+            __syncwarp();
+            if (qcount >= 32) {
+              deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane]);
               __syncwarp();
-              if (qcount >= 32) {
-                deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane]);
-                __syncwarp();
-                if (lane < qcount - 32) myQ[lane] = myQ[32 + lane];
-                qcount -= 32;
-                __syncwarp();
-              }
-            }
-          }
-          // write back: whole vectors for full lanes, single values at the edges
-          if (nvalid == 4) {
-            *reinterpret_cast<uint4 *>(S.cell + i0) = C;
-            *reinterpret_cast<float4 *>(S.ox + i0) = OX;
-            *reinterpret_cast<float4 *>(S.oy + i0) = OY;
-            *reinterpret_cast<float4 *>(S.oz + i0) = OZ;
-            *reinterpret_cast<float4 *>(S.u + i0) = U;
-            *reinterpret_cast<float4 *>(S.v + i0) = V;
-            *reinterpret_cast<float4 *>(S.w + i0) = W;
-          } else if (nvalid > 0) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const int i = i0 + j;
-              if (i >= b && i < e) {
-                S.cell[i] = Cp[j];
-                S.ox[i] = pox[j];
-                S.oy[i] = poy[j];
-                S.oz[i] = poz[j];
-                S.u[i] = pu[j];
-                S.v[i] = pv[j];
-                S.w[i] = pw[j];
-              }
+              if (lane < qcount - 32) myQ[lane] = myQ[32 + lane];
+              qcount -= 32;
+              __syncwarp();
             }
           }
         }
-        // the segment cell's 8 nodes: warp sum, then 80 shared atomics
-        warp_sum80(acc, lane);
-        {
-          const int a = (lane >> 4) & 1, bb = (lane >> 3) & 1, c = (lane >> 2) & 1;
-          const int mbase = 5 * ((lane >> 1) & 1);
-          const int n = ((lx + 1 + a) * T::BY + (ly + 1 + bb)) * T::BZ + (lz + 1 + c);
-          const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
-#pragma unroll
-          for (int i = 0; i < 5; ++i)
-            if (i >= lo && i < hi) atomicAdd(sAcc + (mbase + i) * T::BN + n, acc[i]);
-        }
+        if (ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane);
       }
       // remaining queued movers of this warp
       if (lane < qcount) deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane]);
@@ -866,8 +879,8 @@ int encode_field_map(spb_sim *s) {
 template <int TX, int TY, int TZ>
 size_t cycle_smem() {
   using T = Tile<TX, TY, TZ>;
-  return (size_t)T::BN * 8 * 4 + (size_t)T::BN * 10 * 4 + (size_t)SIM_NW * QCAP * sizeof(MoverEntry) +
-         16;
+  return 2 * (size_t)T::BN * 8 * 4 + (size_t)T::BN * 10 * 4 +
+         (size_t)SIM_NW * QCAP * sizeof(MoverEntry) + 16;
 }
 
 CycleParams make_params(spb_sim *s) {
@@ -910,24 +923,31 @@ CycleParams make_params(spb_sim *s) {
   return P;
 }
 
-template <int TX, int TY, int TZ>
-int launch_cycle(spb_sim *s, cudaStream_t st) {
+template <int TX, int TY, int TZ, bool ACC>
+int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   const size_t smem = cycle_smem<TX, TY, TZ>();
   static bool attr = false;
   if (!attr) {
-    SPB_CUDA(cudaFuncSetAttribute(k_cycle<TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    SPB_CUDA(cudaFuncSetAttribute(k_cycle<TX, TY, TZ, ACC>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
   const CycleParams P = make_params(s);
   const int ntiles = s->nt[0] * s->nt[1] * s->nt[2];
-  const int ctas = std::min(ntiles, s->grid_ctas > 0 ? s->grid_ctas : num_sms());
+  const int per_sm = ACC ? 1 : 2;
+  const int ctas = std::min(ntiles, s->grid_ctas > 0 ? s->grid_ctas : per_sm * num_sms());
   Timed tm(s, &s->ev_cycle, st);
-  k_cycle<TX, TY, TZ><<<ctas, SIM_TPB, smem, st>>>(s->fmap, P);
+  k_cycle<TX, TY, TZ, ACC><<<ctas, SIM_TPB, smem, st>>>(s->fmap, P);
   SPB_CUDA(cudaGetLastError());
   g_launches++;
   s->launches++;
   return SPB_OK;
+}
+
+template <int TX, int TY, int TZ>
+int launch_cycle(spb_sim *s, cudaStream_t st) {
+  return s->d.variant == 1 ? launch_cycle_v<TX, TY, TZ, false>(s, st)
+                           : launch_cycle_v<TX, TY, TZ, true>(s, st);
 }
 
 template <int TX, int TY, int TZ>
@@ -970,7 +990,7 @@ struct TileImpl {
 #define SPB_TILE(X, Y, Z) \
   TileImpl { {X, Y, Z}, launch_cycle<X, Y, Z>, launch_sort<X, Y, Z>, cycle_smem<X, Y, Z> }
 const TileImpl kTiles[] = {SPB_TILE(8, 4, 4), SPB_TILE(4, 4, 4), SPB_TILE(2, 2, 2),
-                           SPB_TILE(8, 8, 4), SPB_TILE(4, 4, 8), SPB_TILE(8, 4, 8)};
+                           SPB_TILE(8, 8, 4)};
 #undef SPB_TILE
 
 const TileImpl *find_tile(const int t[3]) {

@@ -20,7 +20,7 @@ def _stream(stream):
 
 
 class Simulation:
-    def __init__(self, wl, tile=(8, 4, 4), resort_every=1, ctas=0, species=None):
+    def __init__(self, wl, tile=(8, 4, 4), resort_every=1, ctas=0, species=None, variant=0):
         self.lib = _lib.load()
         self.wl = wl
         species = list(range(len(wl.species))) if species is None else list(species)
@@ -35,7 +35,7 @@ class Simulation:
             d.qom[i] = wl.species[s].qom
         for a in range(3):
             d.tile[a] = tile[a]
-        d.resort_every, d.ctas = resort_every, ctas
+        d.resort_every, d.ctas, d.variant = resort_every, ctas, variant
         h = ctypes.c_void_p()
         _lib.check(self.lib.spb_sim_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h
@@ -112,3 +112,57 @@ class Simulation:
         _lib.check(self.lib.spb_sim_timing(self.h, ctypes.byref(c), ctypes.byref(nc),
                                            ctypes.byref(o), ctypes.byref(no)))
         return c.value, nc.value, o.value, no.value
+
+
+def autotune(wl, fields, parts, tiles=((8, 4, 4), (4, 4, 4), (8, 8, 4)), variants=(0, 1),
+             resorts=(1, 2, 4, 8), cycles=2, stream=None):
+    """Picks the tile shape, deposit variant and resort interval with the
+    highest particles/s on the given workload (device tensors; left intact).
+
+    Tile and variant are timed on `cycles` cycles right after a sort (CUDA
+    events around the cycle kernel). The resort interval k is then chosen from
+    a model of the measured costs: per cycle, the kernel time grows with the
+    cycles since the last sort (particles drift out of their cells), while a
+    sort costs a fixed time every k cycles.
+    Returns a dict with the choice and the measurements."""
+    import torch
+    n = sum(p["x"].numel() for p in parts)
+    best, trials = None, []
+    for tile in tiles:
+        if any(N % t for N, t in zip((wl.nxc, wl.nyc, wl.nzc), tile)):
+            continue
+        for var in variants:
+            sim = Simulation(wl, tile=tile, resort_every=10**6, variant=var)
+            sim.set_fields(fields)
+            for s, p in enumerate(parts):
+                sim.load_species(s, p)
+            sim.cycle(1)                       # warm-up (first launch, attributes)
+            sim.resort()
+            sim.set_timing(True)
+            sim.timing()
+            sim.cycle(cycles)
+            ms, nc, _, _ = sim.timing()
+            sim.resort()
+            _, _, sort_ms, ns = sim.timing()
+            per = ms / max(nc, 1)
+            trials.append({"tile": list(tile), "variant": var, "cycle_ms": per,
+                           "sort_ms": sort_ms})
+            if best is None or per < best[0]:
+                best = (per, tile, var, sort_ms, sim)
+            else:
+                sim.close()
+    per0, tile, var, sort_ms, sim = best
+    # drift cost: time cycles 1..max(resorts) after a sort
+    sim.resort()
+    sim.timing()
+    drift = []
+    for _ in range(max(resorts)):
+        sim.cycle(1)
+        drift.append(sim.timing()[0])
+    sim.close()
+    torch.cuda.synchronize()
+    costs = {k: (sum(drift[:k]) + sort_ms) / k for k in resorts}
+    k = min(costs, key=costs.get)
+    return {"tile": tile, "variant": var, "resort_every": k, "trials": trials,
+            "drift_ms": drift, "sort_ms": sort_ms, "ms_per_cycle_model": costs,
+            "particles": n}

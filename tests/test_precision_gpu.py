@@ -30,9 +30,9 @@ def rel_l2(a, b):
 
 
 def run_sim(torch, wl, fields, parts, tile=(8, 4, 4), resort_every=1, ncycles=1, tags=False,
-            species=None):
+            species=None, variant=0):
     from sputnipic_b200.sim import Simulation
-    sim = Simulation(wl, tile=tile, resort_every=resort_every, species=species)
+    sim = Simulation(wl, tile=tile, resort_every=resort_every, species=species, variant=variant)
     sim.set_fields([torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in fields])
     for s, p in enumerate(parts):
         d = {k: torch.from_numpy(np.ascontiguousarray(p[k])).cuda() for k in "xyzuvwq"}
@@ -70,13 +70,14 @@ def compare_particles(sim_p, ref_p, wl):
     assert mism <= 1e-4 * len(order) + 2, mism
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("tile", [(8, 4, 4), (4, 4, 4), (2, 2, 2)])
-def test_small_gem_moments_vs_fp64(cuda, orc64, tile):
+def test_small_gem_moments_vs_fp64(cuda, orc64, tile, variant):
     torch = cuda
     wl = W.small_gem()
     fields = W.gem_fields(wl)
     parts = [W.gem_particles(wl, s) for s in range(4)]
-    sim = run_sim(torch, wl, fields, parts, tile=tile)
+    sim = run_sim(torch, wl, fields, parts, tile=tile, variant=variant)
     for s in range(4):
         _, m64 = oracle64(orc64, wl, fields, parts[s], wl.species[s].qom)
         err = rel_l2(sim.moments(s).cpu().numpy(), m64)
@@ -99,13 +100,14 @@ def test_small_gem_particles_vs_fp64(cuda, orc64):
     sim.close()
 
 
-@pytest.mark.parametrize("resort_every", [1, 4])
-def test_ten_cycles_vs_fp64(cuda, orc64, resort_every):
+@pytest.mark.parametrize("resort_every,variant", [(1, 0), (4, 1), (8, 0)])
+def test_ten_cycles_vs_fp64(cuda, orc64, resort_every, variant):
     torch = cuda
     wl = W.small_gem()
     fields = W.gem_fields(wl)
     parts = [W.gem_particles(wl, s) for s in range(4)]
-    sim = run_sim(torch, wl, fields, parts, resort_every=resort_every, ncycles=10)
+    sim = run_sim(torch, wl, fields, parts, resort_every=resort_every, ncycles=10,
+                  variant=variant)
     for s in range(4):
         _, m64 = oracle64(orc64, wl, fields, parts[s], wl.species[s].qom, ncycles=10)
         err = rel_l2(sim.moments(s).cpu().numpy(), m64)
@@ -124,7 +126,7 @@ def test_edge_fixture_vs_reference_fp64(cuda, golden_edge, qi):
                                      w0=0, ppc=1),))
     fields = [d[f"field_{n}"] for n in oracle.FIELDS]
     part = {k: d[f"in_{k}"] for k in "xyzuvwq"}
-    sim = run_sim(torch, wl, fields, [part], tile=(2, 2, 2))
+    sim = run_sim(torch, wl, fields, [part], tile=(2, 2, 2), variant=qi)
     err = rel_l2(sim.moments(0).cpu().numpy(), d[f"fp64_q{qi}_p2g"])
     assert (err <= 1e-5).all(), err
     sim.close()
@@ -169,7 +171,7 @@ def test_charge_conservation_and_counts_gem_grid(cuda):
     inv = 1.0 / (wl.dx * wl.dy * wl.dz)
     for i in range(2):
         m = sim.moments(i)
-        assert abs(float(m[0].sum()) - qsum[i] * inv) <= 1e-9 * abs(qsum[i] * inv)
+        assert abs(float(m[0].sum()) - qsum[i] * inv) <= 1e-6 * abs(qsum[i] * inv)
         p = sim.particles(i)
         assert p["x"].numel() == wl.species_count((0, 2)[i])
         for k, L in (("x", wl.Lx), ("y", wl.Ly), ("z", wl.Lz)):
