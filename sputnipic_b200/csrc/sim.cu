@@ -180,6 +180,10 @@ struct Tile {
   static constexpr int BX = TX + 3, BY = TY + 3, BZ = TZ + 3;
   static constexpr int BN = BX * BY * BZ;    // staged nodes
   static constexpr int TC = TX * TY * TZ;    // cells per tile
+  // floats per field stage, padded so every stage starts on the 128-byte
+  // boundary a TMA tensor copy's shared-memory destination needs
+  static constexpr int SF = ((8 * BN + 31) / 32) * 32;
+  static_assert((SF * 4) % 128 == 0, "field stages must stay 128-byte aligned");
 };
 
 // Trilinear gather of E and B at (cell g, fraction f) per axis: from the
@@ -408,13 +412,17 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
     k_cycle(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P) {
   using T = Tile<TX, TY, TZ>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x BN * 8
-  float *sAcc = sF0 + 2 * 8 * T::BN;                                // 10 * BN
+  float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
+  float *sAcc = sF0 + 2 * T::SF;                                    // 10 * BN
   MoverEntry *sQ = reinterpret_cast<MoverEntry *>(sAcc + 10 * T::BN);  // NW * QCAP
   uint64_t *bar = reinterpret_cast<uint64_t *>(sQ + SIM_NW * QCAP);   // 2 barriers
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   MoverEntry *myQ = sQ + warp * QCAP;
+  if (smem_addr(sF0) & 127u) {   // TMA destinations need 128-byte alignment
+    if (tid == 0) atomicOr(P.err, 8);
+    return;
+  }
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
@@ -430,7 +438,7 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
     fence_proxy_async();
     mbar_expect_tx(bar + stage, box_bytes);
     // box origin: node c0 on every axis (the lower node of halo cell c0-1)
-    tma_load_4d(sF0 + stage * 8 * T::BN, &fmap, 0, z * TZ, y * TY, x * TX, bar + stage);
+    tma_load_4d(sF0 + stage * T::SF, &fmap, 0, z * TZ, y * TY, x * TX, bar + stage);
   };
   if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
   int bad = 0, it = 0;
@@ -446,7 +454,7 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
       mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
       return;
     }
-    const float *sF = sF0 + stage * 8 * T::BN;
+    const float *sF = sF0 + stage * T::SF;
     const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
     const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
 
@@ -879,7 +887,7 @@ int encode_field_map(spb_sim *s) {
 template <int TX, int TY, int TZ>
 size_t cycle_smem() {
   using T = Tile<TX, TY, TZ>;
-  return 2 * (size_t)T::BN * 8 * 4 + (size_t)T::BN * 10 * 4 +
+  return 2 * (size_t)T::SF * 4 + (size_t)T::BN * 10 * 4 +
          (size_t)SIM_NW * QCAP * sizeof(MoverEntry) + 16;
 }
 
@@ -1356,6 +1364,7 @@ extern "C" int spb_sim_check(spb_sim *s, void *stream) {
     SPB_CUDA(cudaMemset(s->d_err, 0, sizeof(int)));
     if (h & 2) return fail(SPB_ERR_TIMEOUT, "a staged field tile never arrived (bounded wait)");
     if (h & 4) return fail(SPB_ERR_CUDA, "the counting sort produced an out-of-range slot");
+    if (h & 8) return fail(SPB_ERR_UNSUPPORTED, "shared memory not 128-byte aligned for TMA");
     return fail(SPB_ERR_OUT_OF_GRID, "a particle left the node array and was clamped");
   }
   return SPB_OK;

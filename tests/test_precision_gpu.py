@@ -158,7 +158,7 @@ def test_charge_conservation_and_counts_gem_grid(cuda):
     torch = cuda
     from sputnipic_b200.device import gen_fields, gen_particles
     from sputnipic_b200.sim import Simulation
-    wl = W.gem(species=W.gem_species((8, 8, 8, 8)))
+    wl = W.gem(lattice=0, species=W.gem_species((8, 8, 8, 8)))
     sim = Simulation(wl, species=[0, 2])
     sim.set_fields(gen_fields(wl))
     qsum = []
