@@ -252,6 +252,31 @@ int spb_sim_timing(spb_sim *sim, double *cycle_ms, int *ncycle, double *sort_ms,
                    int *nsort);
 
 /* ---------------------------------------------------------------------------
+ * Particle load + cell sort that allocates nothing. No counterpart in the
+ * reference: it is the conversion and counting sort behind
+ * spb_sim_load_species, for callers that cannot call cudaMalloc where they
+ * sort (codes that hand all device memory to their own pool allocator at
+ * start-up, or loops that cannot afford an allocation's implicit
+ * synchronisation). The caller passes inputs (reference-layout positions in
+ * [0, L], velocities, charges; device pointers) and outputs (precision-form
+ * arrays of n elements, cell_start of nxc*nyc*nzc + 1 ints); only desc's
+ * grid and tile fields are read. Scratch is a fixed __device__ array for at
+ * most SPB_NOALLOC_MAX_CELLS cells (about 8 MB per device, held until the
+ * process exits); larger grids return SPB_ERR_CAPACITY. All calls share that
+ * array: calls that overlap on the GPU race. The first call on a device
+ * looks up the array's device address, so make it before any stream capture.
+ * The call synchronises `stream` before returning.
+ * ------------------------------------------------------------------------- */
+#define SPB_NOALLOC_MAX_CELLS (1L << 20)
+int spb_sort_particles_noalloc(const spb_sim_desc *desc, const float *x,
+                               const float *y, const float *z, const float *u,
+                               const float *v, const float *w, const float *q,
+                               long n, uint32_t *cell, float *ox, float *oy,
+                               float *oz, float *u_out, float *v_out,
+                               float *w_out, float *q_out, int *cell_start,
+                               void *stream);
+
+/* ---------------------------------------------------------------------------
  * Seeded synthetic GEM (Harris current sheet) inputs, generated on the device.
  * No counterpart in the reference's hot path: the reference builds its inputs
  * on the host with initGEM (src/IC.cpp:7-188). Same hash and formulas as

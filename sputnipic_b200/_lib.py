@@ -217,6 +217,8 @@ def load():
     _proto(lib, "spb_sim_apply_bc_ids", c_int, [P, c_int, P])
     _proto(lib, "spb_sim_particles", c_int, [P, c_int] + [P] * 7 + [c_int, P])
     _proto(lib, "spb_sim_check", c_int, [P, P])
+    _proto(lib, "spb_sort_particles_noalloc", c_int,
+           [R(SimDesc)] + [P] * 7 + [c_long] + [P] * 8 + [P, P])
     _proto(lib, "spb_sim_set_timing", c_int, [P, c_int])
     _proto(lib, "spb_sim_timing", c_int, [P, R(c_double), R(c_int), R(c_double), R(c_int)])
     _lib = lib
