@@ -93,72 +93,54 @@ __device__ __forceinline__ void fence_proxy_async() {
 
 // Gather cell and fraction of a predicted position p (cells, relative to the
 // particle's cell c). Below the domain the reference's int() truncates toward
-// zero, so the cell rounds up and the fraction goes negative.
-__device__ __forceinline__ void locate(float p, int c, int N, int &g, float &f, int &bad) {
-  p = fminf(fmaxf(p, -(float)(c + 4)), (float)(N - c + 4));
-  const float s = floorf(p);
-  g = c + (int)s;
-  f = p - s;
-  if (g < 0 && f != 0.0f) {
-    g += 1;
-    f -= 1.0f;
-  }
-  if (g < -1) {
-    bad = 1;
-    g = -1;
-  }
-  if (g > N) {
-    bad = 1;
-    g = N;
-  }
+// zero, so the cell rounds up and the fraction goes negative. Branch-free;
+// cells outside [-1, N] are left to the gather's bounds handling.
+__device__ __forceinline__ void locate(float p, int c, int N, int &g, float &f) {
+  const float lim = (float)(N + 8);
+  const float s = fminf(fmaxf(floorf(p), -lim), lim);
+  int gg = c + __float2int_rz(s);
+  float ff = p - s;
+  const bool trunc = (gg < 0) & (ff != 0.0f);
+  g = trunc ? gg + 1 : gg;
+  f = trunc ? ff - 1.0f : ff;
 }
 
 // Particle BC on one axis in cell units: "x > L" first, then "x < 0"
-// (src/Mover.cpp:103-157). On entry o is in [0, 1).
+// (src/Mover.cpp:103-157). On entry o is in [0, 1). Branch-free.
 __device__ __forceinline__ void bc_cell(int &c, float &o, float &vel, int N, int periodic) {
-  if (c > N || (c == N && o > 0.0f)) {
-    if (periodic) {
-      c -= N;
-    } else {
-      vel = -vel;
-      if (o > 0.0f) {
-        c = 2 * N - c - 1;
-        o = 1.0f - o;
-      } else {
-        c = 2 * N - c;
-      }
-    }
+  {
+    const bool over = (c > N) | ((c == N) & (o > 0.0f));
+    const bool pos = o > 0.0f;
+    const int cr = pos ? 2 * N - c - 1 : 2 * N - c;     // mirror of x about L
+    const float orf = pos ? 1.0f - o : o;
+    c = over ? (periodic ? c - N : cr) : c;
+    o = (over & !periodic) ? orf : o;
+    vel = (over & !periodic) ? -vel : vel;
   }
-  if (c < 0) {
-    if (periodic) {
-      c += N;
-    } else {
-      vel = -vel;
-      if (o > 0.0f) {
-        c = -c - 1;
-        o = 1.0f - o;
-      } else {
-        c = -c;
-      }
-    }
+  {
+    const bool under = c < 0;
+    const bool pos = o > 0.0f;
+    const int cr = pos ? -c - 1 : -c;                    // mirror of x about 0
+    const float orf = pos ? 1.0f - o : o;
+    c = under ? (periodic ? c + N : cr) : c;
+    o = (under & !periodic) ? orf : o;
+    vel = (under & !periodic) ? -vel : vel;
   }
-  if (c == N && o == 0.0f) {   // x == L exactly: top face of the last cell
-    c = N - 1;
-    o = 1.0f;
-  }
+  const bool top = (c == N) & (o == 0.0f);   // x == L exactly: top face of the last cell
+  c = top ? N - 1 : c;
+  o = top ? 1.0f : o;
 }
 
 // Final position update on one axis: p = o + displacement, new cell and offset.
 __device__ __forceinline__ void advance(int &c, float &o, float disp, int N) {
-  float p = o + disp;
-  p = fminf(fmaxf(p, -(float)(c + 4)), (float)(N - c + 4));
-  const float s = floorf(p);
-  c += (int)s;
+  const float lim = (float)(N + 8);
+  const float p = o + disp;
+  const float s = fminf(fmaxf(floorf(p), -lim), lim);
+  c += __float2int_rz(s);
   o = p - s;
-  if (o >= 1.0f) {
-    c += 1;
-    o = 0.0f;
-  }
+  const bool wrap = o >= 1.0f;
+  c = wrap ? c + 1 : c;
+  o = wrap ? 0.0f : o;
 }
 
 // E and B as three packed pairs (Ex,Ey), (Ez,Bx), (By,Bz): the node record in
@@ -186,8 +168,10 @@ struct Tile {
   static_assert((SF * 4) % 128 == 0, "field stages must stay 128-byte aligned");
 };
 
-// Trilinear gather of E and B at (cell g, fraction f) per axis: from the
-// staged tile when the 8 nodes are inside it, else from HBM/L2.
+// Trilinear gather of E and B at (cell g, fraction f) per axis from the staged
+// tile. Every lane reads the tile (indices clamped into it); lanes whose 8
+// nodes lie outside the tile then re-gather from HBM/L2, a warp-uniform branch
+// that is skipped when no lane needs it. All 32 lanes must call.
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ Field6 gather(const CycleParams &P, const float *__restrict__ sF,
                                          int c0x, int c0y, int c0z, int gx, int gy, int gz,
@@ -196,9 +180,11 @@ __device__ __forceinline__ Field6 gather(const CycleParams &P, const float *__re
   const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
   Field6 F = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   const int bx = gx + 1 - c0x, by = gy + 1 - c0y, bz = gz + 1 - c0z;
-  if ((unsigned)bx <= (unsigned)(TX + 1) && (unsigned)by <= (unsigned)(TY + 1) &&
-      (unsigned)bz <= (unsigned)(TZ + 1)) {
-    const int n0 = (bx * T::BY + by) * T::BZ + bz;
+  const bool inbox = ((unsigned)bx <= (unsigned)(TX + 1)) & ((unsigned)by <= (unsigned)(TY + 1)) &
+                     ((unsigned)bz <= (unsigned)(TZ + 1));
+  {
+    const int n0 = (min(max(bx, 0), TX + 1) * T::BY + min(max(by, 0), TY + 1)) * T::BZ +
+                   min(max(bz, 0), TZ + 1);
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -212,27 +198,34 @@ __device__ __forceinline__ Field6 gather(const CycleParams &P, const float *__re
           acc_node(F, wab * wz[c], A, B);
         }
       }
-  } else {
-    const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
-    const long n0 = (long)(gx + 1) * sx + (long)(gy + 1) * sy + (gz + 1);
+  }
+  if (__any_sync(0xffffffffu, !inbox)) {
+    if (!inbox) {
+      F = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
+      const int hx = min(max(gx, -1), P.nxc), hy = min(max(gy, -1), P.nyc),
+                hz = min(max(gz, -1), P.nzc);
+      const long n0 = (long)(hx + 1) * sx + (long)(hy + 1) * sy + (hz + 1);
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const float wab = wx[a] * wy[b];
+        for (int b = 0; b < 2; ++b) {
+          const float wab = wx[a] * wy[b];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const long n = n0 + a * sx + b * sy + c;
-          const float4 A = __ldg(reinterpret_cast<const float4 *>(P.fields8 + 8 * n));
-          const float2 B = __ldg(reinterpret_cast<const float2 *>(P.fields8 + 8 * n + 4));
-          acc_node(F, wab * wz[c], A, B);
+          for (int c = 0; c < 2; ++c) {
+            const long n = n0 + a * sx + b * sy + c;
+            const float4 A = __ldg(reinterpret_cast<const float4 *>(P.fields8 + 8 * n));
+            const float2 B = __ldg(reinterpret_cast<const float2 *>(P.fields8 + 8 * n + 4));
+            acc_node(F, wab * wz[c], A, B);
+          }
         }
-      }
+    }
   }
   return F;
 }
 
-// mover_PC for one particle in cell units (src/Mover.cpp:33-157).
+// mover_PC for one particle in cell units (src/Mover.cpp:33-157). All 32 lanes
+// of the warp must call (the gather votes).
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ void push(const CycleParams &P, const float *__restrict__ sF, int c0x,
                                      int c0y, int c0z, float qomdt2, int &cx, int &cy, int &cz,
@@ -245,15 +238,15 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
     int gx = cx, gy = cy, gz = cz;
     float fx = ox, fy = oy, fz = oz;
     if (it > 0) {   // the first gather is at the start position: (c, o) as stored
-      locate(ox + dx, cx, P.nxc, gx, fx, bad);
-      locate(oy + dy, cy, P.nyc, gy, fy, bad);
-      locate(oz + dz, cz, P.nzc, gz, fz, bad);
+      locate(ox + dx, cx, P.nxc, gx, fx);
+      locate(oy + dy, cy, P.nyc, gy, fy);
+      locate(oz + dz, cz, P.nzc, gz, fz);
     }
     const Field6 F = gather<TX, TY, TZ>(P, sF, c0x, c0y, c0z, gx, gy, gz, fx, fy, fz);
     const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
     const float bx = F.ezbx.y, by = F.byz.x, bz = F.byz.y;
     const float omdtsq = qomdt2 * qomdt2 * (bx * bx + by * by + bz * bz);
-    const float denom = __frcp_rn(1.0f + omdtsq);
+    const float denom = __fdividef(1.0f, 1.0f + omdtsq);
     const float ut = fmaf(qomdt2, ex, u);
     const float vt = fmaf(qomdt2, ey, v);
     const float wt = fmaf(qomdt2, ez, w);
@@ -274,12 +267,10 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   bc_cell(cx, ox, u, P.nxc, P.periodic[0]);
   bc_cell(cy, oy, v, P.nyc, P.periodic[1]);
   bc_cell(cz, oz, w, P.nzc, P.periodic[2]);
-  if (cx < 0 || cx >= P.nxc || cy < 0 || cy >= P.nyc || cz < 0 || cz >= P.nzc) {
-    bad = 1;
-    cx = min(max(cx, 0), P.nxc - 1);
-    cy = min(max(cy, 0), P.nyc - 1);
-    cz = min(max(cz, 0), P.nzc - 1);
-  }
+  bad |= (cx < 0) | (cx >= P.nxc) | (cy < 0) | (cy >= P.nyc) | (cz < 0) | (cz >= P.nzc);
+  cx = min(max(cx, 0), P.nxc - 1);
+  cy = min(max(cy, 0), P.nyc - 1);
+  cz = min(max(cz, 0), P.nzc - 1);
 }
 
 // Deposit terms of one particle added to 40 packed accumulators:
@@ -343,12 +334,25 @@ struct MoverEntry {  // one queued deposit: final cell and state
   float ox, oy, oz, q, u, v, w;
 };
 
-// Deposit of one particle with shared-memory atomics (inside the staged box)
-// or FP64 global atomics (outside it).
+// Tile partials are 64-bit fixed point: a term t is added as
+// round(t * fix), fix = 2^40 / max|q| (a power of two, so the scaling is
+// exact). Integer shared-memory atomics are native and do not retry under
+// contention, unlike float ones; the sums are exact, so their order does not
+// matter. |t * fix| beyond 2^62 (|velocity| in the thousands) is flagged.
+__device__ __forceinline__ void add_fixed(unsigned long long *a, float t, float fix, int &bad) {
+  const float x = t * fix;
+  bad |= !(fabsf(x) < 4.0e18f);
+  atomicAdd(a, (unsigned long long)__float2ll_rn(fminf(fmaxf(x, -4.0e18f), 4.0e18f)));
+}
+
+// Deposit of one queued particle per lane with shared-memory atomics (inside
+// the staged box) or FP64 global atomics (outside it; a warp-uniform branch
+// skipped when no lane needs it). All 32 lanes call; `active` lanes deposit.
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ void deposit_scatter(const CycleParams &P, const SpeciesDev &S,
-                                                float *__restrict__ sAcc, int c0x, int c0y,
-                                                int c0z, const MoverEntry &e) {
+                                                unsigned long long *__restrict__ sAcc, int c0x,
+                                                int c0y, int c0z, const MoverEntry &e,
+                                                bool active, int &bad) {
   using T = Tile<TX, TY, TZ>;
   const int cx = cell_x(e.cell), cy = cell_y(e.cell), cz = cell_z(e.cell);
   const float wx[2] = {e.q * (1.0f - e.ox), e.q * e.ox};
@@ -356,8 +360,9 @@ __device__ __forceinline__ void deposit_scatter(const CycleParams &P, const Spec
   const float mf[10] = {1.0f,      e.u,       e.v,       e.w,       e.u * e.u,
                         e.u * e.v, e.u * e.w, e.v * e.v, e.v * e.w, e.w * e.w};
   const int bx = cx + 1 - c0x, by = cy + 1 - c0y, bz = cz + 1 - c0z;
-  if ((unsigned)bx <= (unsigned)(TX + 1) && (unsigned)by <= (unsigned)(TY + 1) &&
-      (unsigned)bz <= (unsigned)(TZ + 1)) {
+  const bool inbox = ((unsigned)bx <= (unsigned)(TX + 1)) & ((unsigned)by <= (unsigned)(TY + 1)) &
+                     ((unsigned)bz <= (unsigned)(TZ + 1));
+  if (active & inbox) {
     const int n0 = (bx * T::BY + by) * T::BZ + bz;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
@@ -368,30 +373,33 @@ __device__ __forceinline__ void deposit_scatter(const CycleParams &P, const Spec
           const float W = wx[a] * wy[b] * wz[c];
           const int n = n0 + (a * T::BY + b) * T::BZ + c;
 #pragma unroll
-          for (int m = 0; m < 10; ++m) atomicAdd(sAcc + m * T::BN + n, W * mf[m]);
+          for (int m = 0; m < 10; ++m) add_fixed(sAcc + m * T::BN + n, W * mf[m], S.fix, bad);
         }
-  } else {
-    const long nodes = (long)P.nxn * P.nyn * P.nzn;
-    const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
-    const long n0 = (long)(cx + 1) * sx + (long)(cy + 1) * sy + (cz + 1);
+  }
+  if (__any_sync(0xffffffffu, active & !inbox)) {
+    if (active & !inbox) {
+      const long nodes = (long)P.nxn * P.nyn * P.nzn;
+      const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
+      const long n0 = (long)(cx + 1) * sx + (long)(cy + 1) * sy + (cz + 1);
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b)
+        for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const double W = (double)(wx[a] * wy[b] * wz[c]) * P.scale;
-          const long n = n0 + a * sx + b * sy + c;
+          for (int c = 0; c < 2; ++c) {
+            const double W = (double)(wx[a] * wy[b] * wz[c]) * P.scale;
+            const long n = n0 + a * sx + b * sy + c;
 #pragma unroll
-          for (int m = 0; m < 10; ++m) atomicAdd(S.mom + m * nodes + n, W * (double)mf[m]);
-        }
+            for (int m = 0; m < 10; ++m) atomicAdd(S.mom + m * nodes + n, W * (double)mf[m]);
+          }
+    }
   }
 }
 
 // Adds the warp totals of the segment cell's 8 nodes into the tile partials.
 template <int TX, int TY, int TZ>
-__device__ __forceinline__ void flush_cell(float2 (&acc)[40], float *__restrict__ sAcc, int lx,
-                                           int ly, int lz, int lane) {
+__device__ __forceinline__ void flush_cell(float2 (&acc)[40], unsigned long long *__restrict__ sAcc,
+                                           int lx, int ly, int lz, int lane, float fix, int &bad) {
   using T = Tile<TX, TY, TZ>;
   float r[5];
   warp_sum80(acc, r, lane);
@@ -401,7 +409,7 @@ __device__ __forceinline__ void flush_cell(float2 (&acc)[40], float *__restrict_
   const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
 #pragma unroll
   for (int k = 0; k < 5; ++k)
-    if (k >= lo && k < hi) atomicAdd(sAcc + (mbase + k) * T::BN + n, r[k]);
+    if (k >= lo && k < hi) add_fixed(sAcc + (mbase + k) * T::BN + n, r[k], fix, bad);
 }
 
 // ACC = true: each lane accumulates the terms of all its particles of a cell
@@ -413,7 +421,8 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
   using T = Tile<TX, TY, TZ>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
-  float *sAcc = sF0 + 2 * T::SF;                                    // 10 * BN
+  unsigned long long *sAcc =
+      reinterpret_cast<unsigned long long *>(sF0 + 2 * T::SF);      // 10 * BN fixed point
   MoverEntry *sQ = reinterpret_cast<MoverEntry *>(sAcc + 10 * T::BN);  // NW * QCAP
   uint64_t *bar = reinterpret_cast<uint64_t *>(sQ + SIM_NW * QCAP);   // 2 barriers
 
@@ -427,7 +436,7 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
   }
-  for (int i = tid; i < 10 * T::BN; i += SIM_TPB) sAcc[i] = 0.0f;
+  for (int i = tid; i < 10 * T::BN; i += SIM_TPB) sAcc[i] = 0ull;
   __syncthreads();
 
   const int ntiles = P.ntx * P.nty * P.ntz;
@@ -478,20 +487,22 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
         for (int base = b; base < e; base += 32) {
           const int i = base + lane;
           const bool valid = i < e;
-          uint32_t cell = 0;
-          float ox = 0.f, oy = 0.f, oz = 0.f, u = 0.f, v = 0.f, w = 0.f, q = 0.f;
-          if (valid) {
-            cell = S.cell[i];
-            ox = S.ox[i];
-            oy = S.oy[i];
-            oz = S.oz[i];
-            u = S.u[i];
-            v = S.v[i];
-            w = S.w[i];
-            q = S.q[i];
+          // idle lanes of the last slot push a copy of the cell's last particle
+          // (results discarded), so the whole warp runs one instruction stream
+          const int ii = valid ? i : e - 1;
+          uint32_t cell = S.cell[ii];
+          float ox = S.ox[ii], oy = S.oy[ii], oz = S.oz[ii];
+          float u = S.u[ii], v = S.v[ii], w = S.w[ii];
+          const float q = valid ? S.q[ii] : 0.0f;
+          {
             int cx = cell_x(cell), cy = cell_y(cell), cz = cell_z(cell);
-            push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, bad);
+            int pbad = 0;
+            push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
+            bad |= valid ? pbad : 0;
             cell = pack_cell(cx, cy, cz);
+          }
+          __syncwarp();
+          if (valid) {
             S.cell[i] = cell;
             S.ox[i] = ox;
             S.oy[i] = oy;
@@ -500,14 +511,14 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
             S.v[i] = v;
             S.w[i] = w;
           }
-          const bool mover = valid && cell != seg;
+          const bool mover = valid & (cell != seg);
           // particles that stay in the segment cell: register terms
           if (!ACC) {
 #pragma unroll
             for (int k = 0; k < 40; ++k) acc[k] = make_float2(0.f, 0.f);
           }
-          add_terms(acc, (valid && !mover) ? q : 0.0f, ox, oy, oz, u, v, w, lane);
-          if (!ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane);
+          add_terms(acc, mover ? 0.0f : q, ox, oy, oz, u, v, w, lane);
+          if (!ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane, S.fix, bad);
           // particles that changed cell: per-warp queue, shared atomics
           const unsigned mb = __ballot_sync(FULL, mover);
           if (mb) {
@@ -518,7 +529,7 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
             qcount += __popc(mb);
             __syncwarp();
             if (qcount >= 32) {
-              deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane]);
+              deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane], true, bad);
               __syncwarp();
               if (lane < qcount - 32) myQ[lane] = myQ[32 + lane];
               qcount -= 32;
@@ -526,20 +537,21 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
             }
           }
         }
-        if (ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane);
+        if (ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane, S.fix, bad);
       }
       // remaining queued movers of this warp
-      if (lane < qcount) deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane]);
+      if (qcount > 0)
+        deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane], lane < qcount, bad);
       __syncthreads();
-      // flush the tile's FP32 partials into the FP64 moments, and clear them
+      // flush the tile's partials into the FP64 moments, and clear them
       for (int i = tid; i < 10 * T::BN; i += SIM_TPB) {
-        const float val = sAcc[i];
-        if (val != 0.0f) {
+        const long long val = (long long)sAcc[i];
+        if (val != 0) {
           const int m = i / T::BN, n = i % T::BN;
           const int bz = n % T::BZ, by = (n / T::BZ) % T::BY, bx = n / (T::BZ * T::BY);
           const long g = ((long)(c0x + bx) * P.nyn + (c0y + by)) * P.nzn + (c0z + bz);
-          atomicAdd(S.mom + m * nodes + g, (double)val * P.scale);
-          sAcc[i] = 0.0f;
+          atomicAdd(S.mom + m * nodes + g, (double)val * S.unfix);
+          sAcc[i] = 0ull;
         }
       }
       __syncthreads();
@@ -602,6 +614,17 @@ __global__ void k_load(GridScalars g, const float *__restrict__ x, const float *
     qo[i] = q[i];
   }
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
+// max |q| as the bit pattern of a non-negative float (ordered like an int)
+__global__ void k_absmax(const float *__restrict__ q, long n, unsigned *__restrict__ out) {
+  float m = 0.0f;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(q[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
 
 __global__ void k_unload(GridScalars g, const uint32_t *__restrict__ cell,
@@ -800,6 +823,7 @@ namespace {
 struct SimSpecies {
   long n = 0, cap = 0;
   double qom = 0;
+  float fix = 1.0f;     // fixed-point scale of the tile partials (2^40 / max|q|)
   uint32_t *cell[2] = {};
   float *f[2][7] = {};   // ox oy oz u v w q, double-buffered for the sort
   int cur = 0;
@@ -887,7 +911,7 @@ int encode_field_map(spb_sim *s) {
 template <int TX, int TY, int TZ>
 size_t cycle_smem() {
   using T = Tile<TX, TY, TZ>;
-  return 2 * (size_t)T::SF * 4 + (size_t)T::BN * 10 * 4 +
+  return 2 * (size_t)T::SF * 4 + (size_t)T::BN * 10 * 8 +
          (size_t)SIM_NW * QCAP * sizeof(MoverEntry) + 16;
 }
 
@@ -927,6 +951,8 @@ CycleParams make_params(spb_sim *s) {
     D.mom = q.mom;
     D.n = q.n;
     D.qomdt2 = (float)(q.qom * (0.5 * s->d.dt) / s->d.c);
+    D.fix = q.fix;
+    D.unfix = P.scale / (double)q.fix;
   }
   return P;
 }
@@ -1266,6 +1292,26 @@ extern "C" int spb_sim_load_species(spb_sim *s, int species, const float *x, con
     SPB_CUDA(cudaGetLastError());
     g_launches++;
     s->launches++;
+  }
+  // fixed-point scale of the tile partials from max |q| (q never changes)
+  S.fix = 1.0f;
+  if (n > 0) {
+    unsigned *d_max = reinterpret_cast<unsigned *>(s->scan_tmp);
+    SPB_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
+    k_absmax<<<blocks_for(n, 256), 256, 0, st>>>(S.f[0][6], n, d_max);
+    SPB_CUDA(cudaGetLastError());
+    g_launches++;
+    s->launches++;
+    unsigned h = 0;
+    SPB_CUDA(cudaMemcpyAsync(&h, d_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+    float qmax;
+    std::memcpy(&qmax, &h, sizeof(float));
+    if (qmax > 0.0f && std::isfinite(qmax)) {
+      int e;
+      std::frexp(qmax, &e);                   // qmax < 2^e
+      S.fix = std::ldexp(1.0f, 40 - e);      // |q| * fix < 2^40
+    }
   }
   const TileImpl *ti = find_tile(s->tile);
   if (int rc = ti->sort(s, S, st)) return rc;

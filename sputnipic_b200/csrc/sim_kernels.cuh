@@ -47,6 +47,8 @@ struct SpeciesDev {
   double *mom;            // [10][nodes]
   long n;
   float qomdt2;
+  float fix;              // fixed-point scale of the tile partials: 2^40 / max|q| (power of 2)
+  double unfix;           // invVOL / fix, applied when the partials are flushed
 };
 
 struct CycleParams {

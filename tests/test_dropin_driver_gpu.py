@@ -6,11 +6,13 @@ Both are built by tests/dropin_driver/Makefile from the reference sources
 (single-process MPI and no-op HDF5 header stubs; the binaries travel with the
 repository). They run the same small GEM deck for 3 cycles and their VTK
 outputs are compared:
-  cycle 1 densities: relative L2 <= 1e-5 (same particles, FP32 sums in
-      another order; see the plain-form parity tests)
-  cycle 1 E and B, and every output of cycles 2-3: relative L2 <= 1e-3 (the
-      field solve iterates to GMRES/CG tolerances, so tiny moment
-      differences move the fields within those tolerances)
+  cycle 1 species densities (rhoe, rhoi): relative L2 <= 1e-5 (same
+      particles, FP32 sums in another order; see the plain-form parity tests)
+  the net density rho_net (electron and ion densities nearly cancel, so its
+      relative error is that of the species scaled by their ratio), cycle 1
+      E and B, and every output of cycles 2-3: relative L2 <= 1e-3 (the field
+      solve iterates to GMRES/CG tolerances, so tiny moment differences move
+      the fields within those tolerances)
 """
 import os
 import re
@@ -88,10 +90,13 @@ def test_reference_driver_with_dropin_matches_reference_mover(cuda, tmp_path):
     out_b200 = run(os.path.join(BUILD, "sputnipic_b200"), str(tmp_path / "b200"))
     cg = [re.findall(r"CG converged at iteration # (\d+)", o) for o in (out_ref, out_b200)]
     assert len(cg[0]) == len(cg[1]) == 3
+    bad = []
     for cyc in (1, 2, 3):
         for name in ("rhoe", "rhoi", "rho_net", "E", "B"):
             a = read_vtk(str(tmp_path / "cpu" / "data" / f"{name}_{cyc}.vtk"))
             b = read_vtk(str(tmp_path / "b200" / "data" / f"{name}_{cyc}.vtk"))
             err = np.linalg.norm(b - a) / max(np.linalg.norm(a), 1e-300)
-            tol = 1e-5 if (cyc == 1 and name.startswith("rho")) else 1e-3
-            assert err <= tol, (name, cyc, err)
+            tol = 1e-5 if (cyc == 1 and name in ("rhoe", "rhoi")) else 1e-3
+            if not err <= tol:
+                bad.append((name, cyc, err, tol))
+    assert not bad, bad
