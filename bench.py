@@ -174,10 +174,10 @@ def algorithmic_bytes(kind: str, n: int, nodes: int, ns: int = 1) -> int:
         return 48 * n + 24 * nodes
     if kind == "p2g":         # plain: read x..w, q; read+write the ten FP32 moments
         return 28 * n + 80 * nodes
-    if kind == "cycle":       # precision: read cell, offsets, u..w, q (32 B); write 28 B;
-        return 60 * n + 24 * nodes + 80 * nodes * ns   # fields once; FP64 moments written
-    if kind == "sort":        # counting sort: read cell; read + write 32 B per particle
-        return 68 * n
+    if kind == "push":        # precision: read + write 32-byte records; fields (32 B/node)
+        return 64 * n + 32 * nodes
+    if kind == "deposit":     # precision: read 32-byte records; FP64 moments written once
+        return 32 * n + 80 * nodes * ns
     raise ValueError(kind)
 
 
@@ -265,8 +265,9 @@ def measure_plain(args, torch, wl, fields, parts, dist, stream):
 
 
 def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
-    """Precision form: one fused mover + deposit kernel per cycle for all
-    species, counting sort every `resort` cycles (amortised in the steps)."""
+    """Precision form: per cycle one push kernel and one deposit kernel for
+    all species (particles in per-cell buckets, no sort); overflow checks
+    every `resort` cycles (counted in the steps)."""
     from sputnipic_b200 import _lib
     from sputnipic_b200.sim import Simulation
     ns = len(parts)
@@ -275,7 +276,7 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     if args.autotune:
         from sputnipic_b200.sim import autotune
         tune = autotune(wl, fields, parts)
-        args.tile, args.variant, args.resort = list(tune["tile"]), tune["variant"], tune["resort_every"]
+        args.tile, args.variant = list(tune["tile"]), tune["variant"]
     sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort, variant=args.variant)
     sim.set_fields(fields)
     for s, p in enumerate(parts):
@@ -287,37 +288,51 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
         raise RuntimeError(f"precision warm-up status {rc}: {_lib.last_error()}")
     lib = _lib.load()
     sim.set_timing(True)
-    sim.timing()
+    sim.kernel_timing()
     l0 = lib.spb_launch_count()
     local_rank = torch.cuda.current_device()
     with Clocks(local_rank) as clk:
         ms = device_timed(torch, dist, stream, args.steps, lambda: sim.cycle(1))
     launches = lib.spb_launch_count() - l0
-    cyc_ms, ncyc, sort_ms, nsort = sim.timing()
+    kt = sim.kernel_timing()
     sim.set_timing(False)
     rc = sim.check()
     if rc:
         raise RuntimeError(f"precision status {rc}: {_lib.last_error()}")
+    overflow = [sim.overflow(s) for s in range(ns)]
+    slots = [round(sim.bucket_slots(s) / wl.cells, 2) for s in range(ns)]
     peak, peak_kind = peaks()
-    alg = algorithmic_bytes("cycle", n, wl.nodes, ns)
-    kms = cyc_ms / max(ncyc, 1)
-    achieved = alg / (kms / 1e3) / 1e9
-    traffic = load_traffic().get("precision_cycle")
+    nc = max(kt["cycles"], 1)
+    traffic = load_traffic()
+    kernels = {}
+    for k, name in (("push", "k_push (mover, all species)"),
+                    ("deposit", "k_deposit (10-moment deposit, all species)")):
+        kms = kt[k + "_ms"] / nc
+        alg = algorithmic_bytes(k, n, wl.nodes, ns)
+        ach = alg / (kms / 1e3) / 1e9
+        tr = traffic.get("k_" + k)
+        kernels[k] = {"kernel": name, "ms_mean": kms, "algorithmic_bytes": alg,
+                      "achieved": ach, "frac": ach / peak, "share_of_step": kt[k + "_ms"] / ms,
+                      "traffic": (tr["dram_bytes_per_particle"] * n if tr else None)}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_mean"])
+    d = kernels[dom]
+    cyc_ms = kernels["push"]["ms_mean"] + kernels["deposit"]["ms_mean"]
+    cyc_alg = kernels["push"]["algorithmic_bytes"] + kernels["deposit"]["algorithmic_bytes"]
     roofline = {
-        "kernel": "k_cycle (fused mover + deposit, all species)", "bound": "hbm",
-        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": (traffic["dram_bytes_per_particle"] * n if traffic else None),
-        "algorithmic_bytes": alg, "kernel_ms_mean": kms,
+        "kernel": d["kernel"], "bound": "hbm", "achieved": d["achieved"], "peak": peak,
+        "unit": "GB/s", "frac": d["frac"], "traffic": d["traffic"],
+        "algorithmic_bytes": d["algorithmic_bytes"], "kernel_ms_mean": d["ms_mean"],
         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-        "share_of_step": cyc_ms / ms,
-        "sort": {"ms_mean": sort_ms / max(nsort, 1), "launches": nsort,
-                 "share_of_step": sort_ms / ms,
-                 "achieved_gbs": (algorithmic_bytes("sort", n // ns, 0) /
-                                  ((sort_ms / max(nsort, 1)) / 1e3) / 1e9) if nsort else None},
+        "share_of_step": d["share_of_step"], "kernels": kernels,
+        "cycle": {"kernels_ms": cyc_ms, "algorithmic_bytes": cyc_alg,
+                  "achieved": cyc_alg / (cyc_ms / 1e3) / 1e9,
+                  "frac": cyc_alg / (cyc_ms / 1e3) / 1e9 / peak},
+        "relayouts": {"count": kt["relayouts"], "ms": kt["relayout_ms"]},
     }
     sim.close()
     return {"value": n * world * args.steps / (ms / 1e3), "ms": ms, "roofline": roofline,
-            "clocks": clk.summary(), "launches": launches, "autotune": tune}
+            "clocks": clk.summary(), "launches": launches, "autotune": tune,
+            "buckets": {"mean_slots_per_cell": slots, "overflow_entries": overflow}}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -376,10 +391,11 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": f"{wl.name}: {ns} species x {ntot // ns:,} particles, "
                                    f"{wl.species[0].ppc:g} ppc, NiterMover {wl.niter}, "
                                    "one mover + 10-moment deposit cycle",
-                       "form": "precision (int32 cell + fp32 offset, fp32 push, "
-                               "fp32 smem partials -> fp64 moments)",
-                       "tile": list(args.tile), "resort_every": args.resort,
-                       "deposit_variant": args.variant,
+                       "form": "precision (per-cell buckets of fp32 offsets, charge and "
+                               "velocities; fp32 push; fp32 per-cell register sums -> "
+                               "fp64 moments)",
+                       "tile": list(args.tile), "overflow_check_every": args.resort,
+                       "push_variant": args.variant, "buckets": prec["buckets"],
                        "autotune": prec["autotune"],
                        "particles_per_gpu": ntot, "grid_cells": [wl.nxc, wl.nyc, wl.nzc],
                        "parallelism": f"particle decomposition x{world}" if world > 1 else "1 GPU",
@@ -463,10 +479,13 @@ def main():
     ap.add_argument("--ppc", type=float, default=125,
                     help="smaller profiling cases only; the benchmark uses 125")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--resort", type=int, default=4)
-    ap.add_argument("--variant", type=int, default=1)
+    ap.add_argument("--resort", type=int, default=4,
+                    help="cycles between overflow checks (a species using its overflow "
+                         "list is re-laid out)")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="push kernel residency: 0 two CTAs per SM, 1 three, 2 four")
     ap.add_argument("--autotune", action="store_true",
-                    help="pick tile, deposit variant and resort interval first")
+                    help="pick the tile shape and push variant first (timed on this workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

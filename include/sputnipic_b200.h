@@ -180,12 +180,15 @@ long spb_grid_launches(const spb_grid_ctx *ctx);
  * driver that calls mover_PC and interpP2G for every species
  * (src/sputniPIC_CPU.cpp:232-256; src/Mover.cpp:4-162 and :385-572).
  *
- * Particles are stored as an int32 cell index (packed cz | cy<<11 | cx<<21)
- * plus FP32 in-cell offsets, FP32 velocities and charge, cell-sorted in
- * tile-major order by an on-device counting sort. One fused kernel per cycle
- * runs the NiterMover predictor-corrector push (FP32, E/B gathered from a
- * TMA-staged tile of nodes) and deposits the ten moments as FP32
- * shared-memory partials flushed into FP64 global moments.
+ * Particles live in HBM bucketed by cell: every cell owns a fixed number of
+ * record slots (two float4 per particle: FP32 in-cell offsets, charge,
+ * velocities; the cell is implicit), cells numbered tile-major; particles that
+ * find their cell's bucket full go to a per-species overflow list. A cycle is
+ * two kernels: the push runs the NiterMover predictor-corrector (FP32, E/B
+ * gathered from a TMA-staged tile of nodes) and writes every particle into
+ * the bucket of its new cell in a second buffer set, so the particles stay
+ * grouped by cell with no sort; the deposit sums each cell's bucket in
+ * registers (FP32) and adds the node sums into FP64 global moments.
  * Moments are the raw interpP2G sums (zeroed at the start of every cycle, no
  * applyBCids), FP64, [10][nxn*nyn*nzn] per species in the reference order.
  * ------------------------------------------------------------------------- */
@@ -203,10 +206,15 @@ typedef struct spb_sim_desc {
   double qom[SPB_SIM_MAX_SPECIES];
   long capacity[SPB_SIM_MAX_SPECIES]; /* optional: particles to reserve for */
   int tile[3];              /* cells per tile (0,0,0: default 8x4x4) */
-  int resort_every;         /* cycles between counting sorts (>= 1) */
-  int ctas;                 /* persistent CTAs (0: one or two per SM) */
-  int variant;              /* deposit: 0 per-lane register sums per cell,
-                               1 warp sums per 32 particles (more occupancy) */
+  int resort_every;         /* cycles between overflow checks (>= 1): a species
+                               whose overflow list is in use is re-laid out */
+  int ctas;                 /* persistent CTAs of the push (0: per variant) */
+  int variant;              /* push kernel residency: 0 two CTAs per SM (up to
+                               128 registers), 1 three (up to 80), 2 four
+                               (up to 64) */
+  int bucket_slots;         /* record slots of every cell's bucket (0: each
+                               cell's count at the last layout + max(16,
+                               count/4), rounded up to 4) */
 } spb_sim_desc;
 
 /* Whether a tile shape has an instantiated kernel. */
@@ -221,35 +229,47 @@ long spb_sim_launches(const spb_sim *sim);
 int spb_sim_set_fields(spb_sim *sim, const float *const fields[6], int on_device,
                        void *stream);
 /* Load one species from reference-style float arrays (positions in domain
- * units, inside [0, L]); converts to cell + offset and sorts. */
+ * units, inside [0, L]); converts to cell + offset and lays the particles out
+ * in buckets (synchronises `stream`). */
 int spb_sim_load_species(spb_sim *sim, int species, const float *x, const float *y,
                          const float *z, const float *u, const float *v,
                          const float *w, const float *q, long n, int on_device,
                          void *stream);
 /* ncycles of mover + deposit for all species (the last cycle's moments
- * remain). Resorts every desc.resort_every cycles. */
+ * remain). Every desc.resort_every cycles the overflow lists are checked
+ * (a synchronisation) and species using theirs are re-laid out, which
+ * resizes every cell's bucket to its current count plus slack. */
 int spb_sim_cycle(spb_sim *sim, int ncycles, void *stream);
-/* Counting sort of every species now. */
+/* Re-lay out every species now: buckets sized from the current counts, the
+ * buckets and the overflow list copied into them (synchronises `stream`). */
 int spb_sim_resort(spb_sim *sim, void *stream);
+/* Record slots of a species' bucket layout, summed over the cells (-1: bad
+ * arguments). */
+long spb_sim_bucket_slots(const spb_sim *sim, int species);
+/* Entries in a species' overflow list (synchronises `stream`; -1 on error). */
+long spb_sim_overflow(spb_sim *sim, int species, void *stream);
 /* FP64 moments of a species: 10*nodes doubles. */
 int spb_sim_moments(spb_sim *sim, int species, double *out, int on_device,
                     void *stream);
 /* applyBCids (src/BC.cpp:362-615) on a species' FP64 moments, in place. */
 int spb_sim_apply_bc_ids(spb_sim *sim, int species, void *stream);
 /* Positions x = (cell + offset) * dx, velocities and (if q is not NULL)
- * charges, as floats, in the simulation's current (sorted) order. */
+ * charges, as floats: cells in tile-major order, each cell's particles in
+ * bucket order, then the overflow list. */
 int spb_sim_particles(spb_sim *sim, int species, float *x, float *y, float *z,
                       float *u, float *v, float *w, float *q, int on_device,
                       void *stream);
 /* Synchronise; SPB_ERR_OUT_OF_GRID / SPB_ERR_TIMEOUT from the kernels. */
 int spb_sim_check(spb_sim *sim, void *stream);
-/* CUDA-event timing of the fused cycle kernel and of the sorts, recorded on
- * the launching stream while enabled. spb_sim_timing synchronises, returns
- * the summed milliseconds and launch counts since the last query, and
- * clears them. */
+/* CUDA-event timing of the cycle kernels (push + deposit) and of the
+ * re-layouts, recorded on the launching stream while enabled. The queries
+ * synchronise, return the summed milliseconds and counts since the last
+ * query, and clear them. */
 int spb_sim_set_timing(spb_sim *sim, int on);
 int spb_sim_timing(spb_sim *sim, double *cycle_ms, int *ncycle, double *sort_ms,
                    int *nsort);
+int spb_sim_kernel_timing(spb_sim *sim, double *push_ms, double *deposit_ms,
+                          int *ncycles, double *relayout_ms, int *nrelayouts);
 
 /* ---------------------------------------------------------------------------
  * Particle load + cell sort that allocates nothing. No counterpart in the

@@ -136,7 +136,7 @@ class SimDesc(ctypes.Structure):
                 ("dt", c_double), ("c", c_double), ("niter", c_int), ("periodic", c_int * 3),
                 ("ns", c_int), ("qom", c_double * 8), ("capacity", c_long * 8),
                 ("tile", c_int * 3), ("resort_every", c_int), ("ctas", c_int),
-                ("variant", c_int)]
+                ("variant", c_int), ("bucket_slots", c_int)]
 
 
 def ctypes_layout() -> dict:
@@ -221,6 +221,10 @@ def load():
            [R(SimDesc)] + [P] * 7 + [c_long] + [P] * 8 + [P, P])
     _proto(lib, "spb_sim_set_timing", c_int, [P, c_int])
     _proto(lib, "spb_sim_timing", c_int, [P, R(c_double), R(c_int), R(c_double), R(c_int)])
+    _proto(lib, "spb_sim_kernel_timing", c_int,
+           [P, R(c_double), R(c_double), R(c_int), R(c_double), R(c_int)])
+    _proto(lib, "spb_sim_bucket_slots", c_long, [P, c_int])
+    _proto(lib, "spb_sim_overflow", c_long, [P, c_int, P])
     _lib = lib
     return lib
 

@@ -51,6 +51,9 @@ struct PackedFields {
 // Device error word bits.
 enum : int {
   ERRBIT_OUT_OF_GRID = 1,   // a cell index fell outside the node array
+  ERRBIT_TIMEOUT = 2,       // a bounded wait for a TMA copy ran out
+  ERRBIT_SMEM_ALIGN = 8,    // dynamic shared memory not 128-byte aligned
+  ERRBIT_LOST = 16,         // a bucket and the overflow list were both full
 };
 
 inline long ceil_div(long a, long b) { return (a + b - 1) / b; }

@@ -1,6 +1,7 @@
-// Precision form of the mover + deposit (spb_sim_*): HBM-resident, cell-sorted
-// particles with int32 cell + FP32 in-cell offsets, FP32 push and gather,
-// FP32 shared-memory deposit partials flushed into FP64 global moments.
+// Precision form of the mover + deposit (spb_sim_*): HBM-resident particles
+// bucketed by cell, int32 cell (implicit in the bucket) + FP32 in-cell
+// offsets, FP32 push and gather, FP32 per-cell deposit sums added into FP64
+// global moments.
 //
 // The arithmetic is the reference's mover_PC / interpP2G (src/Mover.cpp:4-162,
 // :385-572) restated in cell units: a position is (cell c, offset o) with
@@ -13,6 +14,10 @@
 //     offset (extrapolation), not from the guard cell;
 //   - the particle BC tests "x > L" and then "x < 0" (src/Mover.cpp:103-157);
 //   - the deposit uses the post-BC position and velocity, floor cell.
+//
+// A cycle is two kernels: k_push moves every particle and writes it into the
+// bucket of its new cell (second buffer set), k_deposit sums each cell's
+// bucket in registers and adds the node sums into the moments.
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -31,7 +36,6 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int SIM_TPB = 256;                 // 8 warps per CTA
 constexpr int SIM_NW = SIM_TPB / 32;
-constexpr int QCAP = 64;                     // mover queue entries per warp
 constexpr long long WAIT_CYCLES = 200000000; // bounded mbarrier wait (~0.1 s)
 
 // ---------------------------------------------------------------------------
@@ -85,6 +89,17 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
 
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Untiled bulk copy global -> this CTA's shared memory (no multicast),
+// completion on `bar`. Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -329,118 +344,101 @@ __device__ __forceinline__ void warp_sum80(float2 (&acc)[40], float (&r)[5], int
   for (int k = 0; k < 5; ++k) r[k] += __shfl_xor_sync(FULL, r[k], 1);
 }
 
-struct MoverEntry {  // one queued deposit: final cell and state
-  uint32_t cell;
-  float ox, oy, oz, q, u, v, w;
+// Stores one pushed record in slot `slot` of the bucket [dbase, dend) of cell
+// `key`, or appends it to the overflow list when the bucket is full. Returns
+// 1 if the overflow list was full too (the particle is lost; reported).
+__device__ __forceinline__ int put_at(const SpeciesDev &S, int key, long long dbase,
+                                      long long dend, int slot, float4 a, float4 b) {
+  if (dbase + slot < dend) {
+    float4 *d = S.rout + 2 * (dbase + slot);
+    d[0] = a;
+    d[1] = b;
+    return 0;
+  }
+  const int o = atomicAdd(S.ocout, 1);
+  if (o >= S.ocap) return 1;
+  S.oout[2 * (long)o] = a;
+  S.oout[2 * (long)o + 1] = b;
+  S.okout[o] = key;
+  return 0;
+}
+
+// A pushed slot of 32 particles whose stores wait for their counter updates:
+// the updates are issued right after the push and consumed one slot later,
+// so their round trip overlaps the next slot's push. The records wait in a
+// per-warp shared-memory staging area (two float4 per lane).
+struct Pending {
+  long long dbase, dend;  // destination bucket
+  int key;                // destination cell
+  int mslot;              // slot from this lane's own counter update (a particle that moved)
+  int sbase0;             // lane 0: first slot of the warp's particles that stayed
+  unsigned sm;            // lanes whose particle stayed in the bucket's cell
+  bool valid, stay;
 };
 
-// Tile partials are 64-bit fixed point: a term t is added as
-// round(t * fix), fix = 2^40 / max|q| (a power of two, so the scaling is
-// exact). Integer shared-memory atomics are native and do not retry under
-// contention, unlike float ones; the sums are exact, so their order does not
-// matter. |t * fix| beyond 2^62 (|velocity| in the thousands) is flagged.
-__device__ __forceinline__ void add_fixed(unsigned long long *a, float t, float fix, int &bad) {
-  const float x = t * fix;
-  bad |= !(fabsf(x) < 4.0e18f);
-  atomicAdd(a, (unsigned long long)__float2ll_rn(fminf(fmaxf(x, -4.0e18f), 4.0e18f)));
-}
-
-// Deposit of one queued particle per lane with shared-memory atomics (inside
-// the staged box) or FP64 global atomics (outside it; a warp-uniform branch
-// skipped when no lane needs it). All 32 lanes call; `active` lanes deposit.
-template <int TX, int TY, int TZ>
-__device__ __forceinline__ void deposit_scatter(const CycleParams &P, const SpeciesDev &S,
-                                                unsigned long long *__restrict__ sAcc, int c0x,
-                                                int c0y, int c0z, const MoverEntry &e,
-                                                bool active, int &bad) {
-  using T = Tile<TX, TY, TZ>;
-  const int cx = cell_x(e.cell), cy = cell_y(e.cell), cz = cell_z(e.cell);
-  const float wx[2] = {e.q * (1.0f - e.ox), e.q * e.ox};
-  const float wy[2] = {1.0f - e.oy, e.oy}, wz[2] = {1.0f - e.oz, e.oz};
-  const float mf[10] = {1.0f,      e.u,       e.v,       e.w,       e.u * e.u,
-                        e.u * e.v, e.u * e.w, e.v * e.v, e.v * e.w, e.w * e.w};
-  const int bx = cx + 1 - c0x, by = cy + 1 - c0y, bz = cz + 1 - c0z;
-  const bool inbox = ((unsigned)bx <= (unsigned)(TX + 1)) & ((unsigned)by <= (unsigned)(TY + 1)) &
-                     ((unsigned)bz <= (unsigned)(TZ + 1));
-  if (active & inbox) {
-    const int n0 = (bx * T::BY + by) * T::BZ + bz;
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 2; ++b)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const float W = wx[a] * wy[b] * wz[c];
-          const int n = n0 + (a * T::BY + b) * T::BZ + c;
-#pragma unroll
-          for (int m = 0; m < 10; ++m) add_fixed(sAcc + m * T::BN + n, W * mf[m], S.fix, bad);
-        }
-  }
-  if (__any_sync(0xffffffffu, active & !inbox)) {
-    if (active & !inbox) {
-      const long nodes = (long)P.nxn * P.nyn * P.nzn;
-      const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
-      const long n0 = (long)(cx + 1) * sx + (long)(cy + 1) * sy + (cz + 1);
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const double W = (double)(wx[a] * wy[b] * wz[c]) * P.scale;
-            const long n = n0 + a * sx + b * sy + c;
-#pragma unroll
-            for (int m = 0; m < 10; ++m) atomicAdd(S.mom + m * nodes + n, W * (double)mf[m]);
-          }
-    }
+// Completes a pending slot. All 32 lanes call.
+__device__ __forceinline__ void flush(const SpeciesDev &S, const Pending &p, const float4 *stage,
+                                      int lane, int &lost) {
+  const int sbase = __shfl_sync(FULL, p.sbase0, 0);
+  if (p.valid) {
+    const int slot = p.stay ? sbase + __popc(p.sm & ((1u << lane) - 1u)) : p.mslot;
+    lost |= put_at(S, p.key, p.dbase, p.dend, slot, stage[lane], stage[32 + lane]);
   }
 }
 
-// Adds the warp totals of the segment cell's 8 nodes into the tile partials.
-template <int TX, int TY, int TZ>
-__device__ __forceinline__ void flush_cell(float2 (&acc)[40], unsigned long long *__restrict__ sAcc,
-                                           int lx, int ly, int lz, int lane, float fix, int &bad) {
-  using T = Tile<TX, TY, TZ>;
-  float r[5];
-  warp_sum80(acc, r, lane);
-  const int a = (lane >> 4) & 1, bb = (lane >> 3) & 1, c = (lane >> 2) & 1;
-  const int mbase = 5 * ((lane >> 1) & 1);
-  const int n = ((lx + 1 + a) * T::BY + (ly + 1 + bb)) * T::BZ + (lz + 1 + c);
-  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
-#pragma unroll
-  for (int k = 0; k < 5; ++k)
-    if (k >= lo && k < hi) add_fixed(sAcc + (mbase + k) * T::BN + n, r[k], fix, bad);
+// Issues the counter updates of a pushed slot and stages its records. All 32
+// lanes call, after the previous slot's flush.
+__device__ __forceinline__ void issue_slot(const SpeciesDev &S, Pending &p, float4 *stage,
+                                          int key, long long b0, long long b1, int nkey,
+                                          bool valid, float4 a, float4 b, int lane) {
+  p.stay = valid & (nkey == key);
+  p.sm = __ballot_sync(FULL, p.stay);
+  p.sbase0 = 0;
+  if (lane == 0 && p.sm) p.sbase0 = atomicAdd(S.cout + key, __popc(p.sm));
+  p.mslot = 0;
+  p.key = nkey;
+  p.dbase = b0;
+  p.dend = b1;
+  if (valid & !p.stay) {
+    p.mslot = atomicAdd(S.cout + nkey, 1);
+    p.dbase = S.base[nkey];
+    p.dend = S.base[nkey + 1];
+  }
+  p.valid = valid;
+  stage[lane] = a;
+  stage[32 + lane] = b;
 }
 
-// ACC = true: each lane accumulates the terms of all its particles of a cell
-// in registers and the warp sums once per cell. ACC = false: the warp sums
-// after every 32 particles (fewer live registers, more occupancy).
-template <int TX, int TY, int TZ, bool ACC>
-__global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
-    k_cycle(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P) {
+// The mover (mover_PC, src/Mover.cpp:4-162) for every species. Persistent
+// CTAs walk tiles of TX x TY x TZ cells; one thread stages the tile's E/B
+// nodes plus a one-cell halo into shared memory with a TMA tensor copy (two
+// stages: the next tile's copy overlaps this tile's work). Warps walk the
+// tile's cells, one particle per lane; the gathers of the NiterMover
+// iterations read the staged tile (or L2 past the halo), and every pushed
+// particle is written into the bucket of its new cell. Afterwards the CTAs
+// push the overflow entries (gathers from L2).
+template <int TX, int TY, int TZ, int MINB>
+__global__ void __launch_bounds__(SIM_TPB, MINB)
+    k_push(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P) {
   using T = Tile<TX, TY, TZ>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
-  unsigned long long *sAcc =
-      reinterpret_cast<unsigned long long *>(sF0 + 2 * T::SF);      // 10 * BN fixed point
-  MoverEntry *sQ = reinterpret_cast<MoverEntry *>(sAcc + 10 * T::BN);  // NW * QCAP
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sQ + SIM_NW * QCAP);   // 2 barriers
+  float4 *sRec = reinterpret_cast<float4 *>(sF0 + 2 * T::SF);       // NW x 64 staged records
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sRec + SIM_NW * 64); // 2 barriers
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  MoverEntry *myQ = sQ + warp * QCAP;
+  float4 *wrec = sRec + warp * 64;   // this warp's staged records
   if (smem_addr(sF0) & 127u) {   // TMA destinations need 128-byte alignment
-    if (tid == 0) atomicOr(P.err, 8);
+    if (tid == 0) atomicOr(P.err, ERRBIT_SMEM_ALIGN);
     return;
   }
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
   }
-  for (int i = tid; i < 10 * T::BN; i += SIM_TPB) sAcc[i] = 0ull;
   __syncthreads();
 
   const int ntiles = P.ntx * P.nty * P.ntz;
-  const long nodes = (long)P.nxn * P.nyn * P.nzn;
   const unsigned box_bytes = (unsigned)(T::BN * 8 * sizeof(float));
   auto issue = [&](int t, int stage) {
     const int z = t % P.ntz, y = (t / P.ntz) % P.nty, x = t / (P.ntz * P.nty);
@@ -450,15 +448,17 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
     tma_load_4d(sF0 + stage * T::SF, &fmap, 0, z * TZ, y * TY, x * TX, bar + stage);
   };
   if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
-  int bad = 0, it = 0;
+  int bad = 0, lost = 0, it = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
     const int stage = it & 1;
     // prefetch the next tile's fields into the other stage (read by the
     // previous tile, which every thread finished before the last barrier)
     if (tid == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
-    if (!mbar_wait_bounded(bar + stage, (it >> 1) & 1)) {
-      // the staged fields never arrived: report, wait once more, give up
-      if (tid == 0) atomicOr(P.err, 2);
+    const bool arrived = mbar_wait_bounded(bar + stage, (it >> 1) & 1);
+    if (__syncthreads_or(!arrived)) {
+      // the staged fields never arrived (for some thread): the whole CTA
+      // reports, waits once more for its copies in flight, and gives up
+      if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
       mbar_wait_bounded(bar + stage, (it >> 1) & 1);
       mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
       return;
@@ -468,100 +468,246 @@ __global__ void __launch_bounds__(SIM_TPB, ACC ? 1 : 2)
     const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
 
     for (int s = 0; s < P.ns; ++s) {
-      const SpeciesDev S = P.sp[s];
-      const float qomdt2 = S.qomdt2;
-      int qcount = 0;
+      const SpeciesDev &S = P.sp[s];
+      Pending pend;
+      pend.valid = false;
+      pend.sbase0 = 0;
       for (int lc = warp; lc < T::TC; lc += SIM_NW) {
-        const long key = (long)tile * T::TC + lc;
-        const int b = (int)min((long)S.cell_start[key], S.n);
-        const int e = (int)min((long)S.cell_start[key + 1], S.n);
-        if (b >= e) continue;
-        const int lx = lc / (TY * TZ), ly = (lc / TZ) % TY, lz = lc % TZ;
-        const uint32_t seg = pack_cell(c0x + lx, c0y + ly, c0z + lz);
-        float2 acc[40];
-        if (ACC) {
+        const int key = tile * T::TC + lc;
+        const long long b0 = S.base[key], b1 = S.base[key + 1];
+        const int cnt = (int)min((long long)S.cin[key], b1 - b0);
+        if (cnt <= 0) continue;
+        const int cx0 = c0x + lc / (TY * TZ), cy0 = c0y + (lc / TZ) % TY, cz0 = c0z + lc % TZ;
+        const float4 *src = S.rin + 2 * b0;
+#pragma unroll 1
+        for (int base = 0; base < cnt; base += 32) {
+          const int i = base + lane;
+          const bool valid = i < cnt;
+          // idle lanes of the last slot push a copy of the cell's last
+          // particle (results discarded): one instruction stream per warp
+          const int ii = valid ? i : cnt - 1;
+          const float4 a = src[2 * ii], b = src[2 * ii + 1];
+          int cx = cx0, cy = cy0, cz = cz0;
+          float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
+          int pbad = 0;
+          push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
+          bad |= valid ? pbad : 0;
+          const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
+          flush(S, pend, wrec, lane, lost);   // the previous slot's counters are back
+          __syncwarp();
+          issue_slot(S, pend, wrec, key, b0, b1, nkey, valid, make_float4(ox, oy, oz, a.w),
+                     make_float4(u, v, w, 0.f), lane);
+        }
+      }
+      flush(S, pend, wrec, lane, lost);
+      __syncwarp();
+    }
+    __syncthreads();   // every warp is done with this stage before it is refilled
+  }
+
+  // overflow entries: pushed with gathers from L2 (the staged-tile origin is
+  // placed out of reach, so every gather takes the global path)
+  for (int s = 0; s < P.ns; ++s) {
+    const SpeciesDev &S = P.sp[s];
+    const int on = min(*S.ocin, S.ocap);
+    for (long base = ((long)blockIdx.x * SIM_NW + warp) * 32; base < on;
+         base += (long)gridDim.x * SIM_TPB) {
+      const int i = (int)base + lane;
+      const bool valid = i < on;
+      const int ii = valid ? i : on - 1;
+      const int key = S.okin[ii];
+      const float4 a = S.oin[2 * (long)ii], b = S.oin[2 * (long)ii + 1];
+      int cx, cy, cz;
+      key_cell<TX, TY, TZ>(key, P.nty, P.ntz, cx, cy, cz);
+      float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
+      int pbad = 0;
+      constexpr int FAR = -(1 << 20);
+      push<TX, TY, TZ>(P, sF0, FAR, FAR, FAR, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
+      bad |= valid ? pbad : 0;
+      const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
+      if (valid) {
+        const int slot = atomicAdd(S.cout + nkey, 1);
+        lost |= put_at(S, nkey, S.base[nkey], S.base[nkey + 1], slot,
+                       make_float4(ox, oy, oz, a.w), make_float4(u, v, w, 0.f));
+      }
+    }
+  }
+  if (bad) atomicOr(P.err, ERRBIT_OUT_OF_GRID);
+  if (lost) atomicOr(P.err, ERRBIT_LOST);
+}
+
+// Deposit of one particle with FP64 global atomics (overflow entries; a rare
+// path, kept rolled so that it does not raise the kernel's register count).
+__device__ __noinline__ void deposit_global(const CycleParams &P, const SpeciesDev &S, int cx,
+                                            int cy, int cz, float4 a, float4 b) {
+  const long nodes = (long)P.nxn * P.nyn * P.nzn;
+  const float u = b.x, v = b.y, w = b.z;
+  const float mf[10] = {1.0f, u, v, w, u * u, u * v, u * w, v * v, v * w, w * w};
+  const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
+  const long n0 = (long)(cx + 1) * sx + (long)(cy + 1) * sy + (cz + 1);
+#pragma unroll 1
+  for (int node = 0; node < 8; ++node) {
+    const int i = node >> 2, j = (node >> 1) & 1, k = node & 1;
+    const float wx = a.w * (i ? a.x : 1.0f - a.x);
+    const float wy = j ? a.y : 1.0f - a.y, wz = k ? a.z : 1.0f - a.z;
+    const double W = (double)(wx * wy * wz) * P.scale;
+    const long n = n0 + i * sx + j * sy + k;
+#pragma unroll
+    for (int m = 0; m < 10; ++m) atomicAdd(S.mom + m * nodes + n, W * (double)mf[m]);
+  }
+}
+
+constexpr int DCH = 128;   // records per bulk chunk of the deposit (4 KB)
+
+// The deposit (interpP2G, src/Mover.cpp:385-572) for every species, from the
+// buckets the push wrote. One warp per cell. Each warp streams its cells'
+// buckets through two shared-memory chunk buffers with bulk copies (one chunk
+// in flight while the previous one is summed); each lane accumulates the 80
+// terms (8 nodes x 10 moments) of its particles in packed FP32 registers,
+// the warp sums them by recursive halving, and the cell's 80 totals go to
+// shared memory. Each node of the tile then adds up the totals of its (up to
+// 8) cells in the tile and one FP64 atomic per node and moment adds the sum
+// into the moments. Overflow entries deposit one by one with FP64 atomics.
+template <int TX, int TY, int TZ>
+__global__ void __launch_bounds__(SIM_TPB, 2) k_deposit(const __grid_constant__ CycleParams P) {
+  using T = Tile<TX, TY, TZ>;
+  constexpr int NX = TX + 1, NY = TY + 1, NZ = TZ + 1, NB = NX * NY * NZ;
+  constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
+  static_assert(T::TC % SIM_NW == 0 && NC <= 32, "cells per warp must fit a warp's lanes");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float4 *sBuf = reinterpret_cast<float4 *>(smem_raw);                 // NW x 2 x DCH records
+  float *sCell = reinterpret_cast<float *>(sBuf + SIM_NW * 2 * DCH * 2);  // TC x 8 x 10
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sCell + T::TC * 80);     // NW x 2
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float4 *buf = sBuf + warp * 2 * DCH * 2;
+  uint64_t *bar = bars + warp * 2;
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+  }
+  __syncthreads();
+  const int ntiles = P.ntx * P.nty * P.ntz;
+  const long nodes = (long)P.nxn * P.nyn * P.nzn;
+  // lane -> (corner, moments) of the warp totals (see warp_sum80)
+  const int corner = (lane >> 2) & 7, mbase = 5 * ((lane >> 1) & 1);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+  unsigned phase = 0, inflight = 0;   // per buffer: parity of the next wait, copy issued
+  bool dead = false;                  // a bounded wait ran out
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
+    const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
+    for (int s = 0; s < P.ns; ++s) {
+      const SpeciesDev &S = P.sp[s];
+      // lane j < NC holds bucket start and particle count of the warp's j-th
+      // cell (tile-local cell warp + j * NW)
+      long long cb = 0;
+      int cc = 0;
+      if (lane < NC) {
+        const int key = tile * T::TC + warp + lane * SIM_NW;
+        cb = S.base[key];
+        cc = (int)min((long long)S.cout[key], S.base[key + 1] - cb);
+      }
+      int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
+      auto issue_next = [&]() {         // all lanes call; lane 0 copies
+        while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
+          ++pj;
+          poff = 0;
+        }
+        if (pj < NC && !dead) {
+          const int len = min(DCH, __shfl_sync(FULL, cc, pj) - poff);
+          const long long b0 = __shfl_sync(FULL, cb, pj);
+          if (lane == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(bar + nbuf, (unsigned)len * 32u);
+            bulk_load(buf + nbuf * DCH * 2, S.rout + 2 * (b0 + poff), (unsigned)len * 32u,
+                      bar + nbuf);
+          }
+          inflight |= 1u << nbuf;
+          poff += len;
+          nbuf ^= 1;
+        }
+      };
+      issue_next();
+      int cbuf = 0;
+      for (int j = 0; j < NC; ++j) {
+        const int cnt = __shfl_sync(FULL, cc, j);
+        float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        if (cnt > 0 && !dead) {
+          float2 acc[40];
 #pragma unroll
           for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
-        }
 #pragma unroll 1
-        for (int base = b; base < e; base += 32) {
-          const int i = base + lane;
-          const bool valid = i < e;
-          // idle lanes of the last slot push a copy of the cell's last particle
-          // (results discarded), so the whole warp runs one instruction stream
-          const int ii = valid ? i : e - 1;
-          uint32_t cell = S.cell[ii];
-          float ox = S.ox[ii], oy = S.oy[ii], oz = S.oz[ii];
-          float u = S.u[ii], v = S.v[ii], w = S.w[ii];
-          const float q = valid ? S.q[ii] : 0.0f;
-          {
-            int cx = cell_x(cell), cy = cell_y(cell), cz = cell_z(cell);
-            int pbad = 0;
-            push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
-            bad |= valid ? pbad : 0;
-            cell = pack_cell(cx, cy, cz);
-          }
-          __syncwarp();
-          if (valid) {
-            S.cell[i] = cell;
-            S.ox[i] = ox;
-            S.oy[i] = oy;
-            S.oz[i] = oz;
-            S.u[i] = u;
-            S.v[i] = v;
-            S.w[i] = w;
-          }
-          const bool mover = valid & (cell != seg);
-          // particles that stay in the segment cell: register terms
-          if (!ACC) {
-#pragma unroll
-            for (int k = 0; k < 40; ++k) acc[k] = make_float2(0.f, 0.f);
-          }
-          add_terms(acc, mover ? 0.0f : q, ox, oy, oz, u, v, w, lane);
-          if (!ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane, S.fix, bad);
-          // particles that changed cell: per-warp queue, shared atomics
-          const unsigned mb = __ballot_sync(FULL, mover);
-          if (mb) {
-            if (mover) {
-              const int slot = qcount + __popc(mb & ((1u << lane) - 1u));
-              myQ[slot] = MoverEntry{cell, ox, oy, oz, q, u, v, w};
+          for (int off = 0; off < cnt; off += DCH) {
+            issue_next();   // the following chunk streams in while this one is summed
+            const bool ok = mbar_wait_bounded(bar + cbuf, (phase >> cbuf) & 1u);
+            if (!__all_sync(FULL, ok)) {
+              dead = true;
+              break;
             }
-            qcount += __popc(mb);
-            __syncwarp();
-            if (qcount >= 32) {
-              deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane], true, bad);
-              __syncwarp();
-              if (lane < qcount - 32) myQ[lane] = myQ[32 + lane];
-              qcount -= 32;
-              __syncwarp();
+            phase ^= 1u << cbuf;
+            inflight &= ~(1u << cbuf);
+            const int len = min(DCH, cnt - off);
+            const float4 *rb = buf + cbuf * DCH * 2;
+#pragma unroll 1
+            for (int base = 0; base < len; base += 32) {
+              const bool valid = base + lane < len;
+              const int ii = min(base + lane, len - 1);
+              const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
+              add_terms(acc, valid ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, lane);
             }
+            __syncwarp();   // every lane is done with this buffer before it is refilled
+            cbuf ^= 1;
           }
+          warp_sum80(acc, r, lane);
         }
-        if (ACC) flush_cell<TX, TY, TZ>(acc, sAcc, lx, ly, lz, lane, S.fix, bad);
+        float *dst = sCell + (warp + j * SIM_NW) * 80 + corner * 10 + mbase;
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          if (k >= lo && k < hi) dst[k] = r[k];
       }
-      // remaining queued movers of this warp
-      if (qcount > 0)
-        deposit_scatter<TX, TY, TZ>(P, S, sAcc, c0x, c0y, c0z, myQ[lane], lane < qcount, bad);
-      __syncthreads();
-      // flush the tile's partials into the FP64 moments, and clear them
-      for (int i = tid; i < 10 * T::BN; i += SIM_TPB) {
-        const long long val = (long long)sAcc[i];
-        if (val != 0) {
-          const int m = i / T::BN, n = i % T::BN;
-          const int bz = n % T::BZ, by = (n / T::BZ) % T::BY, bx = n / (T::BZ * T::BY);
-          const long g = ((long)(c0x + bx) * P.nyn + (c0y + by)) * P.nzn + (c0z + bz);
-          atomicAdd(S.mom + m * nodes + g, (double)val * S.unfix);
-          sAcc[i] = 0ull;
+      if (__syncthreads_or(dead)) {
+        // a chunk never arrived: report, wait (bounded) for the copies this
+        // warp still has in flight, and give up
+        if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+        for (int b = 0; b < 2; ++b)
+          if (inflight & (1u << b)) mbar_wait_bounded(bar + b, (phase >> b) & 1u);
+        return;
+      }
+      for (int idx = tid; idx < 10 * NB; idx += SIM_TPB) {
+        const int m = idx / NB, nb = idx % NB;
+        const int bz = nb % NZ, by = (nb / NZ) % NY, bx = nb / (NZ * NY);
+        float sum = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int lx = bx - a, ly = by - b, lz = bz - c;
+              if (lx >= 0 && lx < TX && ly >= 0 && ly < TY && lz >= 0 && lz < TZ)
+                sum += sCell[((lx * TY + ly) * TZ + lz) * 80 + (a * 4 + b * 2 + c) * 10 + m];
+            }
+        if (sum != 0.0f) {
+          const long g = ((long)(c0x + bx + 1) * P.nyn + (c0y + by + 1)) * P.nzn + (c0z + bz + 1);
+          atomicAdd(S.mom + m * nodes + g, (double)sum * P.scale);
         }
       }
       __syncthreads();
     }
   }
-  if (bad) atomicOr(P.err, ERRBIT_OUT_OF_GRID);
+  for (int s = 0; s < P.ns; ++s) {
+    const SpeciesDev &S = P.sp[s];
+    const int on = min(*S.ocout, S.ocap);
+    for (long i = (long)blockIdx.x * SIM_TPB + tid; i < on; i += (long)gridDim.x * SIM_TPB) {
+      int cx, cy, cz;
+      key_cell<TX, TY, TZ>(S.okout[i], P.nty, P.ntz, cx, cy, cz);
+      deposit_global(P, S, cx, cy, cz, S.oout[2 * i], S.oout[2 * i + 1]);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
-// conversion, sort, field packing, readback
+// layout (load, re-layout), readback, field packing, boundary fold
 // ---------------------------------------------------------------------------
 struct GridScalars {
   int nxc, nyc, nzc;
@@ -591,164 +737,228 @@ __device__ __forceinline__ void to_cell(float x, double inv, int N, int &c, floa
   }
 }
 
-__global__ void k_load(GridScalars g, const float *__restrict__ x, const float *__restrict__ y,
-                       const float *__restrict__ z, const float *__restrict__ u,
-                       const float *__restrict__ v, const float *__restrict__ w,
-                       const float *__restrict__ q, long n, uint32_t *cell, float *ox, float *oy,
-                       float *oz, float *uo, float *vo, float *wo, float *qo, int *err) {
+// Particles per cell of reference-layout positions.
+template <int TX, int TY, int TZ>
+__global__ void k_count_keys(GridScalars g, int nty, int ntz, const float *__restrict__ x,
+                             const float *__restrict__ y, const float *__restrict__ z, long n,
+                             int *__restrict__ count, int *err) {
+  const int lane = threadIdx.x & 31;
   int bad = 0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
        i += (long)gridDim.x * blockDim.x) {
     int cx, cy, cz;
-    float a, b, c;
-    to_cell(x[i], g.invdx, g.nxc, cx, a, bad);
-    to_cell(y[i], g.invdy, g.nyc, cy, b, bad);
-    to_cell(z[i], g.invdz, g.nzc, cz, c, bad);
-    cell[i] = pack_cell(cx, cy, cz);
-    ox[i] = a;
-    oy[i] = b;
-    oz[i] = c;
-    uo[i] = u[i];
-    vo[i] = v[i];
-    wo[i] = w[i];
-    qo[i] = q[i];
+    float o;
+    to_cell(x[i], g.invdx, g.nxc, cx, o, bad);
+    to_cell(y[i], g.invdy, g.nyc, cy, o, bad);
+    to_cell(z[i], g.invdz, g.nzc, cz, o, bad);
+    const int key = tile_key<TX, TY, TZ>(cx, cy, cz, nty, ntz);
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    if (lane == __ffs(peers) - 1) atomicAdd(count + key, __popc(peers));
   }
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
-// max |q| as the bit pattern of a non-negative float (ordered like an int)
-__global__ void k_absmax(const float *__restrict__ q, long n, unsigned *__restrict__ out) {
-  float m = 0.0f;
+// Particles per cell of the buckets (clamped counters) ...
+__global__ void k_count_buckets(const long long *__restrict__ base, const int *__restrict__ cnt,
+                                long ncells, int *__restrict__ count) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < ncells;
+       k += (long)gridDim.x * blockDim.x)
+    count[k] = (int)min((long long)cnt[k], base[k + 1] - base[k]);
+}
+
+// ... plus the overflow list (a separate launch: it adds to those counts).
+__global__ void k_count_overflow(const int *__restrict__ okey, const int *__restrict__ ocnt,
+                                 int ocap, int *__restrict__ count) {
+  const int on = min(*ocnt, ocap);
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < on;
+       j += (long)gridDim.x * blockDim.x)
+    atomicAdd(count + okey[j], 1);
+}
+
+// Bucket capacity of each cell from its particle count: fixed (`fixed` > 0)
+// or the count plus max(16, count/4) slots, rounded up to a multiple of 4
+// (128-byte aligned buckets).
+__global__ void k_capacity(const int *__restrict__ count, long ncells, int fixed,
+                           long long *__restrict__ cap) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < ncells;
+       k += (long)gridDim.x * blockDim.x) {
+    const long long c = count[k];
+    cap[k] = fixed > 0 ? fixed : ((c + max(16LL, c / 4) + 3) / 4) * 4;
+  }
+}
+
+// Reference-layout particles into the buckets S.rout (counters S.cout and the
+// overflow list zeroed beforehand).
+template <int TX, int TY, int TZ>
+__global__ void k_fill(GridScalars g, int nty, int ntz, const float *__restrict__ x,
+                       const float *__restrict__ y, const float *__restrict__ z,
+                       const float *__restrict__ u, const float *__restrict__ v,
+                       const float *__restrict__ w, const float *__restrict__ q, long n,
+                       SpeciesDev S, int *err) {
+  int bad = 0, lost = 0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    int cx, cy, cz;
+    float ox, oy, oz;
+    to_cell(x[i], g.invdx, g.nxc, cx, ox, bad);
+    to_cell(y[i], g.invdy, g.nyc, cy, oy, bad);
+    to_cell(z[i], g.invdz, g.nzc, cz, oz, bad);
+    const int key = tile_key<TX, TY, TZ>(cx, cy, cz, nty, ntz);
+    const int slot = atomicAdd(S.cout + key, 1);
+    lost |= put_at(S, key, S.base[key], S.base[key + 1], slot, make_float4(ox, oy, oz, q[i]),
+                   make_float4(u[i], v[i], w[i], 0.f));
+  }
+  if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+  if (lost) atomicOr(err, ERRBIT_LOST);
+}
+
+// Re-layout: buckets (old layout, buffer set `in`) and overflow list into
+// the buckets of the new layout S.base / S.rout (counters zeroed beforehand).
+// One warp per cell copies its bucket; then the overflow entries are placed.
+// Every cell's new capacity covers its particles, so nothing overflows unless
+// the capacities were fixed by the caller.
+__global__ void k_relayout(const long long *__restrict__ obase, const float4 *__restrict__ rin,
+                           const int *__restrict__ cin, long ncells,
+                           const float4 *__restrict__ oin, const int *__restrict__ okin,
+                           const int *__restrict__ ocin, int ocap_in, SpeciesDev S, int *err) {
+  const int lane = threadIdx.x & 31;
+  const long warps = (long)gridDim.x * (blockDim.x >> 5);
+  int lost = 0;
+  for (long key = blockIdx.x * (long)(blockDim.x >> 5) + (threadIdx.x >> 5); key < ncells;
+       key += warps) {
+    const long long ob = obase[key];
+    const int c = (int)min((long long)cin[key], obase[key + 1] - ob);
+    if (c <= 0) continue;
+    int first = 0;
+    if (lane == 0) first = atomicAdd(S.cout + key, c);
+    first = __shfl_sync(FULL, first, 0);
+    const long long nb = S.base[key], ne = S.base[key + 1];
+    for (int j = lane; j < c; j += 32)
+      lost |= put_at(S, (int)key, nb, ne, first + j, rin[2 * (ob + j)], rin[2 * (ob + j) + 1]);
+  }
+  const int on = min(*ocin, ocap_in);
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < on;
+       j += (long)gridDim.x * blockDim.x) {
+    const int key = okin[j];
+    const int slot = atomicAdd(S.cout + key, 1);
+    lost |= put_at(S, key, S.base[key], S.base[key + 1], slot, oin[2 * j], oin[2 * j + 1]);
+  }
+  if (lost) atomicOr(err, ERRBIT_LOST);
+}
+
+__global__ void k_clamp_counts(const long long *__restrict__ base, const int *__restrict__ cnt,
+                               long k, long long *__restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < k;
        i += (long)gridDim.x * blockDim.x)
-    m = fmaxf(m, fabsf(q[i]));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+    out[i] = min((long long)cnt[i], base[i + 1] - base[i]);
 }
 
-__global__ void k_unload(GridScalars g, const uint32_t *__restrict__ cell,
-                         const float *__restrict__ ox, const float *__restrict__ oy,
-                         const float *__restrict__ oz, const float *__restrict__ u,
-                         const float *__restrict__ v, const float *__restrict__ w,
-                         const float *__restrict__ q, long n, float *x, float *y, float *z,
-                         float *uo, float *vo, float *wo, float *qo) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const uint32_t c = cell[i];
-    x[i] = (float)(((double)cell_x(c) + (double)ox[i]) * g.dx);
-    y[i] = (float)(((double)cell_y(c) + (double)oy[i]) * g.dy);
-    z[i] = (float)(((double)cell_z(c) + (double)oz[i]) * g.dz);
-    uo[i] = u[i];
-    vo[i] = v[i];
-    wo[i] = w[i];
-    if (qo) qo[i] = q[i];
-  }
+struct Unload {
+  float *x, *y, *z, *u, *v, *w, *q;   // q may be null
+  long n;                             // output length
+};
+
+__device__ __forceinline__ void unload_one(const GridScalars &g, const Unload &o, long at, int cx,
+                                           int cy, int cz, float4 a, float4 b) {
+  if (at >= o.n) return;   // only if the counters were corrupted
+  o.x[at] = (float)(((double)cx + (double)a.x) * g.dx);
+  o.y[at] = (float)(((double)cy + (double)a.y) * g.dy);
+  o.z[at] = (float)(((double)cz + (double)a.z) * g.dz);
+  o.u[at] = b.x;
+  o.v[at] = b.y;
+  o.w[at] = b.z;
+  if (o.q) o.q[at] = a.w;
 }
 
+// Buckets (cell order, tile-major) then overflow entries into flat
+// reference-layout arrays; offset[] is the exclusive scan of the clamped
+// counts, offset[ncells] their total.
 template <int TX, int TY, int TZ>
-__global__ void k_sort_count(const uint32_t *__restrict__ cell, long n, int nty, int ntz,
-                             int *__restrict__ count) {
+__global__ void k_unload(GridScalars g, int nty, int ntz, long ncells, const float4 *__restrict__ rec,
+                         const long long *__restrict__ base, const int *__restrict__ cnt,
+                         const long long *__restrict__ offset, const float4 *__restrict__ orec,
+                         const int *__restrict__ okey, const int *__restrict__ ocnt, int ocap,
+                         Unload o) {
   const int lane = threadIdx.x & 31;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const uint32_t c = cell[i];
-    const int key = tile_key<TX, TY, TZ>(cell_x(c), cell_y(c), cell_z(c), nty, ntz);
-    const unsigned active = __activemask();
-    const unsigned peers = __match_any_sync(active, key);
-    if (lane == __ffs(peers) - 1) atomicAdd(count + key, __popc(peers));
+  const long warps = (long)gridDim.x * (blockDim.x >> 5);
+  for (long key = blockIdx.x * (long)(blockDim.x >> 5) + (threadIdx.x >> 5); key < ncells;
+       key += warps) {
+    const long long b0 = base[key];
+    const int c = (int)min((long long)cnt[key], base[key + 1] - b0);
+    if (c <= 0) continue;
+    int cx, cy, cz;
+    key_cell<TX, TY, TZ>((int)key, nty, ntz, cx, cy, cz);
+    const long off = offset[key];
+    for (int j = lane; j < c; j += 32)
+      unload_one(g, o, off + j, cx, cy, cz, rec[2 * (b0 + j)], rec[2 * (b0 + j) + 1]);
+  }
+  const int on = min(*ocnt, ocap);
+  const long ob = offset[ncells];
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < on;
+       j += (long)gridDim.x * blockDim.x) {
+    int cx, cy, cz;
+    key_cell<TX, TY, TZ>(okey[j], nty, ntz, cx, cy, cz);
+    unload_one(g, o, ob + j, cx, cy, cz, orec[2 * j], orec[2 * j + 1]);
   }
 }
 
-template <int TX, int TY, int TZ>
-__global__ void k_sort_scatter(const uint32_t *__restrict__ cell, const float *__restrict__ ox,
-                               const float *__restrict__ oy, const float *__restrict__ oz,
-                               const float *__restrict__ u, const float *__restrict__ v,
-                               const float *__restrict__ w, const float *__restrict__ q, long n,
-                               int nty, int ntz, int *__restrict__ cursor, uint32_t *cell2,
-                               float *ox2, float *oy2, float *oz2, float *u2, float *v2, float *w2,
-                               float *q2, int *err) {
-  const int lane = threadIdx.x & 31;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-       i += (long)gridDim.x * blockDim.x) {
-    const uint32_t c = cell[i];
-    const int key = tile_key<TX, TY, TZ>(cell_x(c), cell_y(c), cell_z(c), nty, ntz);
-    const unsigned active = __activemask();
-    const unsigned peers = __match_any_sync(active, key);
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(cursor + key, __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    const long d = base + __popc(peers & ((1u << lane) - 1u));
-    if (d < 0 || d >= n) {   // only reachable if the counts were corrupted
-      atomicOr(err, 4);
-      continue;
-    }
-    cell2[d] = c;
-    ox2[d] = ox[i];
-    oy2[d] = oy[i];
-    oz2[d] = oz[i];
-    u2[d] = u[i];
-    v2[d] = v[i];
-    w2[d] = w[i];
-    q2[d] = q[i];
-  }
-}
-
-// Exclusive scan of `count` (k entries) into out[0..k]; three passes.
+// Exclusive scan of k 64-bit entries into out[0..k]; three passes.
 constexpr int SCAN_B = 1024;
-__device__ __forceinline__ int block_exclusive_scan(int v, int *warp_sums, int &total) {
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long *warp_sums,
+                                                          long long &total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  int x = v;
+  long long x = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(FULL, x, o);
+    const long long y = __shfl_up_sync(FULL, x, o);
     if (lane >= o) x += y;
   }
   if (lane == 31) warp_sums[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    int s = lane < nw ? warp_sums[lane] : 0;
+    long long s = lane < nw ? warp_sums[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(FULL, s, o);
+      const long long y = __shfl_up_sync(FULL, s, o);
       if (lane >= o) s += y;
     }
     if (lane < nw) warp_sums[lane] = s;
   }
   __syncthreads();
-  const int pre = warp ? warp_sums[warp - 1] : 0;
+  const long long pre = warp ? warp_sums[warp - 1] : 0;
   total = warp_sums[nw - 1];
   __syncthreads();
   return pre + x - v;
 }
 
-__global__ void __launch_bounds__(SCAN_B) k_scan_blocks(const int *in, long k, int *out,
-                                                        int *block_sums) {
-  __shared__ int ws[32];
+__global__ void __launch_bounds__(SCAN_B) k_scan_blocks(const long long *in, long k,
+                                                        long long *out, long long *block_sums) {
+  __shared__ long long ws[32];
   const long i = blockIdx.x * (long)SCAN_B + threadIdx.x;
-  const int v = i < k ? in[i] : 0;
-  int total;
-  const int ex = block_exclusive_scan(v, ws, total);
+  const long long v = i < k ? in[i] : 0;
+  long long total;
+  const long long ex = block_exclusive_scan(v, ws, total);
   if (i < k) out[i] = ex;
   if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(SCAN_B) k_scan_sums(int *block_sums, int nb, int *grand) {
-  __shared__ int ws[32];
-  int carry = 0;
+__global__ void __launch_bounds__(SCAN_B) k_scan_sums(long long *block_sums, int nb,
+                                                      long long *grand) {
+  __shared__ long long ws[32];
+  long long carry = 0;
   for (int base = 0; base < nb; base += SCAN_B) {
     const int i = base + threadIdx.x;
-    const int v = i < nb ? block_sums[i] : 0;
-    int total;
-    const int ex = block_exclusive_scan(v, ws, total);
+    const long long v = i < nb ? block_sums[i] : 0;
+    long long total;
+    const long long ex = block_exclusive_scan(v, ws, total);
     if (i < nb) block_sums[i] = ex + carry;
     carry += total;
   }
   if (threadIdx.x == 0) *grand = carry;
 }
 
-__global__ void __launch_bounds__(SCAN_B) k_scan_add(int *out, long k, const int *block_sums) {
+__global__ void __launch_bounds__(SCAN_B) k_scan_add(long long *out, long k,
+                                                     const long long *block_sums) {
   const long i = blockIdx.x * (long)SCAN_B + threadIdx.x;
   if (i < k) out[i] += block_sums[blockIdx.x];
 }
@@ -821,18 +1031,26 @@ using namespace spb;
 namespace {
 
 struct SimSpecies {
-  long n = 0, cap = 0;
+  long n = 0;
   double qom = 0;
-  float fix = 1.0f;     // fixed-point scale of the tile partials (2^40 / max|q|)
-  uint32_t *cell[2] = {};
-  float *f[2][7] = {};   // ox oy oz u v w q, double-buffered for the sort
-  int cur = 0;
-  int *cell_start = nullptr;   // [ncells + 1]
-  double *mom = nullptr;       // [10][nodes]
-  bool sorted = false;
+  int ocap = 0;                 // overflow entries
+  float4 *rec[2] = {};          // buckets, [slots[b]][2] each
+  long long slots[2] = {0, 0};  // allocated record slots per buffer set
+  int *cnt[2] = {};             // per-cell fill counters
+  float4 *orec[2] = {};         // overflow records, [ocap][2]
+  int *okey[2] = {};            // overflow cell keys
+  int *ocnt = nullptr;          // [2] overflow entry counters
+  long long *base = nullptr;    // [ncells + 1] bucket layout of both buffer sets
+  long long *base2 = nullptr;   // [ncells + 1] the next layout (re-layout)
+  long long total = 0;          // record slots of the layout
+  int cur = 0;                  // the buffer set holding the particles
+  double *mom = nullptr;        // [10][nodes]
 };
 
-using LaunchFn = int (*)(spb_sim *, cudaStream_t);
+using EvPair = std::pair<cudaEvent_t, cudaEvent_t>;
+struct EvCycle {
+  cudaEvent_t b, m, e;          // before push, between push and deposit, after deposit
+};
 
 }  // namespace
 
@@ -848,41 +1066,28 @@ struct spb_sim {
   float *fields8 = nullptr;
   float *stage = nullptr;       // 6*nodes for host field uploads
   int *d_err = nullptr;
-  int *scan_tmp = nullptr;      // block sums + grand total
-  int *counts = nullptr;        // [ncells]
-  int *cursor = nullptr;        // [ncells + 1]
+  long long *scan_tmp = nullptr;  // scan block sums + grand total
+  int *counts = nullptr;          // [ncells] particles per cell
+  long long *lcap = nullptr;      // [ncells] capacities / clamped counts
+  long long *offset = nullptr;    // [ncells + 1] readback offsets
   CUtensorMap fmap{};
   bool fields_set = false;
-  int cycles_since_sort = 0;
-  int grid_ctas = 0;
+  int cycles_since_check = 0;
   std::vector<SimSpecies> sp;
   long launches = 0;
-  std::mutex mu;
-  // optional CUDA-event timing of the cycle kernel and of the sorts
+  // optional CUDA-event timing of the cycle kernels and of the relayouts
   bool timing = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_cycle, ev_sort;
+  std::vector<EvCycle> ev_cycle;
+  std::vector<EvPair> ev_relayout;
 };
 
 namespace {
 
-// Records an event pair around a launch when timing is on.
-struct Timed {
-  spb_sim *s;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> *v;
-  cudaStream_t st;
-  cudaEvent_t b = nullptr;
-  Timed(spb_sim *s_, std::vector<std::pair<cudaEvent_t, cudaEvent_t>> *v_, cudaStream_t st_)
-      : s(s_), v(v_), st(st_) {
-    if (s->timing && cudaEventCreate(&b) == cudaSuccess) cudaEventRecord(b, st);
-  }
-  ~Timed() {
-    cudaEvent_t e = nullptr;
-    if (b && cudaEventCreate(&e) == cudaSuccess) {
-      cudaEventRecord(e, st);
-      v->push_back({b, e});
-    }
-  }
-};
+cudaEvent_t record_event(spb_sim *s, cudaStream_t st) {
+  cudaEvent_t e = nullptr;
+  if (s->timing && cudaEventCreate(&e) == cudaSuccess) cudaEventRecord(e, st);
+  return e;
+}
 
 int encode_field_map(spb_sim *s) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -909,12 +1114,16 @@ int encode_field_map(spb_sim *s) {
 }
 
 template <int TX, int TY, int TZ>
-size_t cycle_smem() {
-  using T = Tile<TX, TY, TZ>;
-  return 2 * (size_t)T::SF * 4 + (size_t)T::BN * 10 * 8 +
-         (size_t)SIM_NW * QCAP * sizeof(MoverEntry) + 16;
+size_t push_smem() {
+  return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + (size_t)SIM_NW * 64 * sizeof(float4) + 16;
+}
+template <int TX, int TY, int TZ>
+size_t deposit_smem() {
+  return (size_t)SIM_NW * 2 * DCH * 2 * sizeof(float4) +
+         (size_t)Tile<TX, TY, TZ>::TC * 80 * sizeof(float) + SIM_NW * 2 * sizeof(uint64_t);
 }
 
+// Kernel parameters for a cycle that reads buffer set `cur` and writes the other.
 CycleParams make_params(spb_sim *s) {
   CycleParams P{};
   P.nxc = s->N[0];
@@ -939,98 +1148,81 @@ CycleParams make_params(spb_sim *s) {
   for (int i = 0; i < P.ns; ++i) {
     SimSpecies &q = s->sp[i];
     SpeciesDev &D = P.sp[i];
-    D.cell = q.cell[q.cur];
-    D.ox = q.f[q.cur][0];
-    D.oy = q.f[q.cur][1];
-    D.oz = q.f[q.cur][2];
-    D.u = q.f[q.cur][3];
-    D.v = q.f[q.cur][4];
-    D.w = q.f[q.cur][5];
-    D.q = q.f[q.cur][6];
-    D.cell_start = q.cell_start;
+    const int c = q.cur, x = 1 - q.cur;
+    D.rin = q.rec[c];
+    D.rout = q.rec[x];
+    D.base = q.base;
+    D.cin = q.cnt[c];
+    D.cout = q.cnt[x];
+    D.oin = q.orec[c];
+    D.okin = q.okey[c];
+    D.ocin = q.ocnt + c;
+    D.oout = q.orec[x];
+    D.okout = q.okey[x];
+    D.ocout = q.ocnt + x;
     D.mom = q.mom;
-    D.n = q.n;
+    D.ocap = q.ocap;
     D.qomdt2 = (float)(q.qom * (0.5 * s->d.dt) / s->d.c);
-    D.fix = q.fix;
-    D.unfix = P.scale / (double)q.fix;
   }
   return P;
 }
 
-template <int TX, int TY, int TZ, bool ACC>
+// One cycle: zero the moments and the write-side counters, push, deposit.
+template <int TX, int TY, int TZ, int MINB>
 int launch_cycle_v(spb_sim *s, cudaStream_t st) {
-  const size_t smem = cycle_smem<TX, TY, TZ>();
+  for (auto &q : s->sp) {
+    if (!q.rec[0]) return fail(SPB_ERR_INVALID, "spb_sim_cycle: a species was never loaded");
+    SPB_CUDA(cudaMemsetAsync(q.mom, 0, 10 * s->nodes * sizeof(double), st));
+    SPB_CUDA(cudaMemsetAsync(q.cnt[1 - q.cur], 0, s->ncells * sizeof(int), st));
+    SPB_CUDA(cudaMemsetAsync(q.ocnt + (1 - q.cur), 0, sizeof(int), st));
+  }
+  const size_t psm = push_smem<TX, TY, TZ>(), dsm = deposit_smem<TX, TY, TZ>();
   static bool attr = false;
   if (!attr) {
-    SPB_CUDA(cudaFuncSetAttribute(k_cycle<TX, TY, TZ, ACC>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
     attr = true;
   }
   const CycleParams P = make_params(s);
   const int ntiles = s->nt[0] * s->nt[1] * s->nt[2];
-  const int per_sm = ACC ? 1 : 2;
-  const int ctas = std::min(ntiles, s->grid_ctas > 0 ? s->grid_ctas : per_sm * num_sms());
-  Timed tm(s, &s->ev_cycle, st);
-  k_cycle<TX, TY, TZ, ACC><<<ctas, SIM_TPB, smem, st>>>(s->fmap, P);
+  static int pocc = 0, docc = 0;   // resident CTAs per SM
+  if (!pocc) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB>, SIM_TPB,
+                                                      psm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ>, SIM_TPB,
+                                                      dsm) != cudaSuccess) {
+      cudaGetLastError();
+      pocc = MINB;
+      docc = 1;
+    }
+    pocc = std::max(pocc, 1);
+    docc = std::max(docc, 1);
+  }
+  const int pctas = std::min(ntiles, s->d.ctas > 0 ? s->d.ctas : pocc * num_sms());
+  const int dctas = std::min(ntiles, docc * num_sms());
+  EvCycle ev{record_event(s, st), nullptr, nullptr};
+  k_push<TX, TY, TZ, MINB><<<pctas, SIM_TPB, psm, st>>>(s->fmap, P);
   SPB_CUDA(cudaGetLastError());
-  g_launches++;
-  s->launches++;
+  ev.m = record_event(s, st);
+  k_deposit<TX, TY, TZ><<<dctas, SIM_TPB, dsm, st>>>(P);
+  SPB_CUDA(cudaGetLastError());
+  ev.e = record_event(s, st);
+  if (ev.b && ev.m && ev.e) s->ev_cycle.push_back(ev);
+  g_launches += 2;
+  s->launches += 2;
+  for (auto &q : s->sp) q.cur = 1 - q.cur;
   return SPB_OK;
 }
 
 template <int TX, int TY, int TZ>
 int launch_cycle(spb_sim *s, cudaStream_t st) {
-  return s->d.variant == 1 ? launch_cycle_v<TX, TY, TZ, false>(s, st)
-                           : launch_cycle_v<TX, TY, TZ, true>(s, st);
-}
-
-template <int TX, int TY, int TZ>
-int launch_sort(spb_sim *s, SimSpecies &q, cudaStream_t st) {
-  const long K = s->ncells;
-  Timed tm(s, &s->ev_sort, st);
-  SPB_CUDA(cudaMemsetAsync(s->counts, 0, K * sizeof(int), st));
-  const int tpb = 256;
-  k_sort_count<TX, TY, TZ><<<blocks_for(q.n, tpb), tpb, 0, st>>>(q.cell[q.cur], q.n, s->nt[1],
-                                                                 s->nt[2], s->counts);
-  SPB_CUDA(cudaGetLastError());
-  const int nb = (int)ceil_div(K, SCAN_B);
-  k_scan_blocks<<<nb, SCAN_B, 0, st>>>(s->counts, K, q.cell_start, s->scan_tmp);
-  k_scan_sums<<<1, SCAN_B, 0, st>>>(s->scan_tmp, nb, q.cell_start + K);
-  k_scan_add<<<nb, SCAN_B, 0, st>>>(q.cell_start, K, s->scan_tmp);
-  SPB_CUDA(cudaGetLastError());
-  SPB_CUDA(cudaMemcpyAsync(s->cursor, q.cell_start, (K + 1) * sizeof(int),
-                           cudaMemcpyDeviceToDevice, st));
-  const int src = q.cur, dst = 1 - q.cur;
-  k_sort_scatter<TX, TY, TZ><<<blocks_for(q.n, tpb), tpb, 0, st>>>(
-      q.cell[src], q.f[src][0], q.f[src][1], q.f[src][2], q.f[src][3], q.f[src][4], q.f[src][5],
-      q.f[src][6], q.n, s->nt[1], s->nt[2], s->cursor, q.cell[dst], q.f[dst][0], q.f[dst][1],
-      q.f[dst][2], q.f[dst][3], q.f[dst][4], q.f[dst][5], q.f[dst][6], s->d_err);
-  SPB_CUDA(cudaGetLastError());
-  g_launches += 5;
-  s->launches += 5;
-  q.cur = dst;
-  q.sorted = true;
-  return SPB_OK;
-}
-
-// Tile shapes the kernels are instantiated for.
-struct TileImpl {
-  int t[3];
-  int (*cycle)(spb_sim *, cudaStream_t);
-  int (*sort)(spb_sim *, SimSpecies &, cudaStream_t);
-  size_t (*smem)();
-};
-
-#define SPB_TILE(X, Y, Z) \
-  TileImpl { {X, Y, Z}, launch_cycle<X, Y, Z>, launch_sort<X, Y, Z>, cycle_smem<X, Y, Z> }
-const TileImpl kTiles[] = {SPB_TILE(8, 4, 4), SPB_TILE(4, 4, 4), SPB_TILE(2, 2, 2),
-                           SPB_TILE(8, 8, 4)};
-#undef SPB_TILE
-
-const TileImpl *find_tile(const int t[3]) {
-  for (const TileImpl &ti : kTiles)
-    if (ti.t[0] == t[0] && ti.t[1] == t[1] && ti.t[2] == t[2]) return &ti;
-  return nullptr;
+  switch (s->d.variant) {
+    case 1: return launch_cycle_v<TX, TY, TZ, 3>(s, st);
+    case 2: return launch_cycle_v<TX, TY, TZ, 4>(s, st);
+    default: return launch_cycle_v<TX, TY, TZ, 2>(s, st);
+  }
 }
 
 GridScalars scalars(const spb_sim *s) {
@@ -1047,20 +1239,226 @@ GridScalars scalars(const spb_sim *s) {
   return g;
 }
 
-void free_species(SimSpecies &q) {
+void free_set(SimSpecies &q, int b) {
+  cudaFree(q.rec[b]);
+  q.rec[b] = nullptr;
+  q.slots[b] = 0;
+}
+
+void free_buckets(SimSpecies &q) {
   for (int b = 0; b < 2; ++b) {
-    cudaFree(q.cell[b]);
-    q.cell[b] = nullptr;
-    for (float *&p : q.f[b]) {
-      cudaFree(p);
-      p = nullptr;
+    free_set(q, b);
+    cudaFree(q.cnt[b]);
+    cudaFree(q.orec[b]);
+    cudaFree(q.okey[b]);
+    q.orec[b] = nullptr;
+    q.cnt[b] = q.okey[b] = nullptr;
+  }
+  cudaFree(q.ocnt);
+  cudaFree(q.base);
+  cudaFree(q.base2);
+  q.ocnt = nullptr;
+  q.base = q.base2 = nullptr;
+  q.ocap = 0;
+  q.total = 0;
+}
+
+// Per-species arrays whose size does not depend on the layout.
+int alloc_fixed(spb_sim *s, SimSpecies &q, int ocap) {
+  if (q.base && q.ocap == ocap) return SPB_OK;
+  free_buckets(q);
+  bool ok = cudaMalloc(&q.ocnt, 2 * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&q.base, (s->ncells + 1) * sizeof(long long)) == cudaSuccess &&
+            cudaMalloc(&q.base2, (s->ncells + 1) * sizeof(long long)) == cudaSuccess;
+  for (int b = 0; b < 2 && ok; ++b)
+    ok = cudaMalloc(&q.cnt[b], s->ncells * sizeof(int)) == cudaSuccess &&
+         cudaMalloc(&q.orec[b], (size_t)ocap * 2 * sizeof(float4)) == cudaSuccess &&
+         cudaMalloc(&q.okey[b], (size_t)ocap * sizeof(int)) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    free_buckets(q);
+    return fail(SPB_ERR_ALLOC, "overflow list / counter allocation failed");
+  }
+  q.ocap = ocap;
+  return SPB_OK;
+}
+
+// Makes buffer set b hold at least `slots` records (1/16 headroom when it grows).
+int ensure_set(SimSpecies &q, int b, long long slots, cudaStream_t st) {
+  if (q.slots[b] >= slots && q.rec[b]) return SPB_OK;
+  SPB_CUDA(cudaStreamSynchronize(st));
+  free_set(q, b);
+  const long long want = std::max<long long>(slots + slots / 16, 32);
+  if (cudaMalloc(&q.rec[b], (size_t)want * 2 * sizeof(float4)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SPB_ERR_ALLOC, "bucket allocation failed (64 bytes per record slot)");
+  }
+  q.slots[b] = want;
+  return SPB_OK;
+}
+
+// base[0..ncells] = exclusive scan of v[0..ncells); returns base[ncells]
+// (synchronises the stream).
+int scan_layout(spb_sim *s, const long long *v, long long *out, long long *total,
+                cudaStream_t st) {
+  const long K = s->ncells;
+  const int nb = (int)ceil_div(K, SCAN_B);
+  k_scan_blocks<<<nb, SCAN_B, 0, st>>>(v, K, out, s->scan_tmp);
+  k_scan_sums<<<1, SCAN_B, 0, st>>>(s->scan_tmp, nb, out + K);
+  k_scan_add<<<nb, SCAN_B, 0, st>>>(out, K, s->scan_tmp);
+  SPB_CUDA(cudaGetLastError());
+  g_launches += 3;
+  s->launches += 3;
+  if (total) {
+    SPB_CUDA(cudaMemcpyAsync(total, out + K, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+  }
+  return SPB_OK;
+}
+
+SpeciesDev write_side(SimSpecies &q, int b, const long long *base) {
+  SpeciesDev D{};
+  D.rout = q.rec[b];
+  D.base = base;
+  D.cout = q.cnt[b];
+  D.oout = q.orec[b];
+  D.okout = q.okey[b];
+  D.ocout = q.ocnt + b;
+  D.ocap = q.ocap;
+  return D;
+}
+
+// Lays out n reference-layout particles (device arrays) in fresh buckets:
+// counts per cell, bucket capacities (count + slack, or desc.bucket_slots),
+// fills buffer set 0.
+template <int TX, int TY, int TZ>
+int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStream_t st) {
+  const GridScalars g = scalars(s);
+  const long ocap = s->d.bucket_slots > 0 ? std::max<long>(65536, n)
+                                          : std::max<long>(65536, n / 32);
+  if (ocap > (1L << 31) - 1) return fail(SPB_ERR_CAPACITY, "overflow list too large");
+  if (int rc = alloc_fixed(s, q, (int)ocap)) return rc;
+  SPB_CUDA(cudaMemsetAsync(s->counts, 0, s->ncells * sizeof(int), st));
+  if (n > 0) {
+    k_count_keys<TX, TY, TZ><<<blocks_for(n, 256), 256, 0, st>>>(g, s->nt[1], s->nt[2], src[0],
+                                                                  src[1], src[2], n, s->counts,
+                                                                  s->d_err);
+    SPB_CUDA(cudaGetLastError());
+  }
+  k_capacity<<<blocks_for(s->ncells, 256), 256, 0, st>>>(s->counts, s->ncells,
+                                                         s->d.bucket_slots, s->lcap);
+  SPB_CUDA(cudaGetLastError());
+  g_launches += 2;
+  s->launches += 2;
+  long long total = 0;
+  if (int rc = scan_layout(s, s->lcap, q.base, &total, st)) return rc;
+  if (int rc = ensure_set(q, 0, total, st)) return rc;
+  if (int rc = ensure_set(q, 1, total, st)) return rc;
+  SPB_CUDA(cudaMemsetAsync(q.cnt[0], 0, s->ncells * sizeof(int), st));
+  SPB_CUDA(cudaMemsetAsync(q.ocnt, 0, 2 * sizeof(int), st));
+  if (n > 0) {
+    k_fill<TX, TY, TZ><<<blocks_for(n, 256), 256, 0, st>>>(g, s->nt[1], s->nt[2], src[0], src[1],
+                                                           src[2], src[3], src[4], src[5], src[6],
+                                                           n, write_side(q, 0, q.base), s->d_err);
+    SPB_CUDA(cudaGetLastError());
+    g_launches++;
+    s->launches++;
+  }
+  q.total = total;
+  q.n = n;
+  q.cur = 0;
+  return SPB_OK;
+}
+
+// Re-layout in place of the buffer sets: bucket capacities from the current
+// counts (buckets + overflow list), then one copy from buffer set `cur` into
+// the other. 64 bytes per particle plus the per-cell passes.
+int relayout(spb_sim *s, SimSpecies &q, cudaStream_t st) {
+  if (!q.base) return SPB_OK;
+  const long K = s->ncells;
+  const int c = q.cur, x = 1 - q.cur;
+  k_count_buckets<<<blocks_for(K, 256), 256, 0, st>>>(q.base, q.cnt[c], K, s->counts);
+  k_count_overflow<<<blocks_for(q.ocap, 256), 256, 0, st>>>(q.okey[c], q.ocnt + c, q.ocap,
+                                                            s->counts);
+  k_capacity<<<blocks_for(K, 256), 256, 0, st>>>(s->counts, K, s->d.bucket_slots, s->lcap);
+  SPB_CUDA(cudaGetLastError());
+  g_launches += 3;
+  s->launches += 3;
+  long long total = 0;
+  if (int rc = scan_layout(s, s->lcap, q.base2, &total, st)) return rc;
+  if (int rc = ensure_set(q, x, total, st)) return rc;
+  SPB_CUDA(cudaMemsetAsync(q.cnt[x], 0, K * sizeof(int), st));
+  SPB_CUDA(cudaMemsetAsync(q.ocnt + x, 0, sizeof(int), st));
+  k_relayout<<<blocks_for(K * 32, 256), 256, 0, st>>>(q.base, q.rec[c], q.cnt[c], K, q.orec[c],
+                                                       q.okey[c], q.ocnt + c, q.ocap,
+                                                       write_side(q, x, q.base2), s->d_err);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  s->launches++;
+  std::swap(q.base, q.base2);
+  q.total = total;
+  q.cur = x;
+  // the other set is written by the next cycle: it must hold the new layout too
+  return ensure_set(q, c, total, st);
+}
+
+// Particles of buffer set `cur` into flat device arrays (dst[6], q, may be null).
+template <int TX, int TY, int TZ>
+int unload(spb_sim *s, SimSpecies &q, float *const dst[7], cudaStream_t st) {
+  const long K = s->ncells;
+  k_clamp_counts<<<blocks_for(K, 256), 256, 0, st>>>(q.base, q.cnt[q.cur], K, s->lcap);
+  SPB_CUDA(cudaGetLastError());
+  if (int rc = scan_layout(s, s->lcap, s->offset, nullptr, st)) return rc;
+  Unload o{dst[0], dst[1], dst[2], dst[3], dst[4], dst[5], dst[6], q.n};
+  k_unload<TX, TY, TZ><<<blocks_for(K * 32, 256), 256, 0, st>>>(
+      scalars(s), s->nt[1], s->nt[2], K, q.rec[q.cur], q.base, q.cnt[q.cur], s->offset,
+      q.orec[q.cur], q.okey[q.cur], q.ocnt + q.cur, q.ocap, o);
+  SPB_CUDA(cudaGetLastError());
+  g_launches += 2;
+  s->launches += 2;
+  return SPB_OK;
+}
+
+// Tile shapes the kernels are instantiated for.
+struct TileImpl {
+  int t[3];
+  int (*cycle)(spb_sim *, cudaStream_t);
+  int (*build)(spb_sim *, SimSpecies &, const float *const *, long, cudaStream_t);
+  int (*unload)(spb_sim *, SimSpecies &, float *const *, cudaStream_t);
+};
+
+#define SPB_TILE(X, Y, Z) \
+  TileImpl { {X, Y, Z}, launch_cycle<X, Y, Z>, build<X, Y, Z>, unload<X, Y, Z> }
+const TileImpl kTiles[] = {SPB_TILE(8, 4, 4), SPB_TILE(4, 4, 4), SPB_TILE(2, 2, 2),
+                           SPB_TILE(8, 8, 4)};
+#undef SPB_TILE
+
+const TileImpl *find_tile(const int t[3]) {
+  for (const TileImpl &ti : kTiles)
+    if (ti.t[0] == t[0] && ti.t[1] == t[1] && ti.t[2] == t[2]) return &ti;
+  return nullptr;
+}
+
+// Temporary flat reference-layout arrays (7 x n floats).
+struct Flat {
+  float *buf = nullptr;
+  float *p[7] = {};
+  int alloc(long n) {
+    if (cudaMalloc(&buf, 7 * std::max<long>(n, 1) * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(SPB_ERR_ALLOC, "temporary particle arrays: allocation failed");
+    }
+    for (int a = 0; a < 7; ++a) p[a] = buf + a * n;
+    return SPB_OK;
+  }
+  void release(cudaStream_t st) {
+    if (buf) {
+      cudaStreamSynchronize(st);
+      cudaFree(buf);
+      buf = nullptr;
     }
   }
-  cudaFree(q.cell_start);
-  cudaFree(q.mom);
-  q.cell_start = nullptr;
-  q.mom = nullptr;
-}
+};
 
 }  // namespace
 
@@ -1076,8 +1474,11 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
     return fail(SPB_ERR_INVALID, "spb_sim_create: 1..8 species");
   if (d->nxc < 1 || d->nyc < 1 || d->nzc < 1 || d->nxc > 2047 || d->nyc > 1023 || d->nzc > 2047)
     return fail(SPB_ERR_UNSUPPORTED, "spb_sim_create: cells per axis must be in [1,2047]x[1,1023]x[1,2047]");
+  if ((long)d->nxc * d->nyc * d->nzc >= (1L << 31))
+    return fail(SPB_ERR_UNSUPPORTED, "spb_sim_create: at most 2^31 - 1 cells");
   if (d->niter < 1 || !(d->dt > 0) || !(d->c != 0))
     return fail(SPB_ERR_INVALID, "spb_sim_create: bad NiterMover, dt or c");
+  if (d->bucket_slots < 0) return fail(SPB_ERR_INVALID, "spb_sim_create: bucket_slots < 0");
   int tile[3] = {d->tile[0], d->tile[1], d->tile[2]};
   if (!tile[0] || !tile[1] || !tile[2]) {
     tile[0] = 8;
@@ -1111,7 +1512,6 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
   s->nzn = d->nzc + 3;
   s->nodes = (long)s->nxn * s->nyn * s->nzn;
   s->ncells = (long)d->nxc * d->nyc * d->nzc;
-  s->grid_ctas = d->ctas;
   auto bail = [&](int rc) {
     spb_sim_destroy(s);
     return rc;
@@ -1119,9 +1519,10 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
   const long nb = ceil_div(s->ncells, SCAN_B);
   if (cudaMalloc(&s->fields8, s->nodes * 8 * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&s->scan_tmp, (nb + 1) * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&s->scan_tmp, (nb + 1) * sizeof(long long)) != cudaSuccess ||
       cudaMalloc(&s->counts, s->ncells * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&s->cursor, (s->ncells + 1) * sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&s->lcap, s->ncells * sizeof(long long)) != cudaSuccess ||
+      cudaMalloc(&s->offset, (s->ncells + 1) * sizeof(long long)) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(SPB_ERR_ALLOC, "spb_sim_create: device allocation failed"));
   }
@@ -1133,37 +1534,47 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
   for (int i = 0; i < d->ns; ++i) {
     SimSpecies &q = s->sp[i];
     q.qom = d->qom[i];
-    if (cudaMalloc(&q.cell_start, (s->ncells + 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&q.mom, 10 * s->nodes * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&q.mom, 10 * s->nodes * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
       return bail(fail(SPB_ERR_ALLOC, "spb_sim_create: device allocation failed"));
     }
-    if (cudaMemset(q.mom, 0, 10 * s->nodes * sizeof(double)) != cudaSuccess ||
-        cudaMemset(q.cell_start, 0, (s->ncells + 1) * sizeof(int)) != cudaSuccess)
+    if (cudaMemset(q.mom, 0, 10 * s->nodes * sizeof(double)) != cudaSuccess)
       return bail(fail(SPB_ERR_CUDA, "spb_sim_create: memset failed"));
-    if (d->capacity[i] > 0) {
-      // reserve now so that later loads allocate nothing
-      q.cap = 0;
-    }
   }
   *out = s;
   return SPB_OK;
 }
 
 namespace {
-double drain(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &v, int *count) {
-  double ms = 0;
-  for (auto &p : v) {
-    float t = 0;
-    if (cudaEventSynchronize(p.second) == cudaSuccess &&
-        cudaEventElapsedTime(&t, p.first, p.second) == cudaSuccess)
-      ms += t;
-    cudaEventDestroy(p.first);
-    cudaEventDestroy(p.second);
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float t = 0;
+  if (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&t, a, b) != cudaSuccess)
+    return 0.0f;
+  return t;
+}
+
+void drain(spb_sim *s, double *push_ms, double *dep_ms, int *ncycles, double *relayout_ms,
+           int *nrelayouts) {
+  double p = 0, d = 0, r = 0;
+  for (auto &e : s->ev_cycle) {
+    p += elapsed(e.b, e.m);
+    d += elapsed(e.m, e.e);
+    cudaEventDestroy(e.b);
+    cudaEventDestroy(e.m);
+    cudaEventDestroy(e.e);
   }
-  if (count) *count = (int)v.size();
-  v.clear();
-  return ms;
+  for (auto &e : s->ev_relayout) {
+    r += elapsed(e.first, e.second);
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  if (push_ms) *push_ms = p;
+  if (dep_ms) *dep_ms = d;
+  if (relayout_ms) *relayout_ms = r;
+  if (ncycles) *ncycles = (int)s->ev_cycle.size();
+  if (nrelayouts) *nrelayouts = (int)s->ev_relayout.size();
+  s->ev_cycle.clear();
+  s->ev_relayout.clear();
 }
 }  // namespace
 
@@ -1176,23 +1587,33 @@ extern "C" int spb_sim_set_timing(spb_sim *s, int on) {
 extern "C" int spb_sim_timing(spb_sim *s, double *cycle_ms, int *ncycle, double *sort_ms,
                               int *nsort) {
   if (!s) return fail(SPB_ERR_INVALID, "spb_sim_timing: null simulation");
-  const double c = drain(s->ev_cycle, ncycle), o = drain(s->ev_sort, nsort);
-  if (cycle_ms) *cycle_ms = c;
-  if (sort_ms) *sort_ms = o;
+  double p = 0, d = 0;
+  drain(s, &p, &d, ncycle, sort_ms, nsort);
+  if (cycle_ms) *cycle_ms = p + d;
+  return SPB_OK;
+}
+
+extern "C" int spb_sim_kernel_timing(spb_sim *s, double *push_ms, double *deposit_ms,
+                                     int *ncycles, double *relayout_ms, int *nrelayouts) {
+  if (!s) return fail(SPB_ERR_INVALID, "spb_sim_kernel_timing: null simulation");
+  drain(s, push_ms, deposit_ms, ncycles, relayout_ms, nrelayouts);
   return SPB_OK;
 }
 
 extern "C" void spb_sim_destroy(spb_sim *s) {
   if (!s) return;
-  drain(s->ev_cycle, nullptr);
-  drain(s->ev_sort, nullptr);
-  for (auto &q : s->sp) free_species(q);
+  drain(s, nullptr, nullptr, nullptr, nullptr, nullptr);
+  for (auto &q : s->sp) {
+    free_buckets(q);
+    cudaFree(q.mom);
+  }
   cudaFree(s->fields8);
   cudaFree(s->stage);
   cudaFree(s->d_err);
   cudaFree(s->scan_tmp);
   cudaFree(s->counts);
-  cudaFree(s->cursor);
+  cudaFree(s->lcap);
+  cudaFree(s->offset);
   delete s;
 }
 
@@ -1202,6 +1623,25 @@ extern "C" long spb_sim_count(const spb_sim *s, int species) {
   return s->sp[species].n;
 }
 extern "C" long spb_sim_launches(const spb_sim *s) { return s ? s->launches : 0; }
+
+extern "C" long spb_sim_bucket_slots(const spb_sim *s, int species) {
+  if (!s || species < 0 || species >= (int)s->sp.size()) return -1;
+  return (long)s->sp[species].total;
+}
+
+extern "C" long spb_sim_overflow(spb_sim *s, int species, void *stream) {
+  if (!s || species < 0 || species >= (int)s->sp.size()) return -1;
+  SimSpecies &q = s->sp[species];
+  if (!q.ocnt) return 0;
+  int h = 0;
+  if (cudaMemcpyAsync(&h, q.ocnt + q.cur, sizeof(int), cudaMemcpyDeviceToHost,
+                      (cudaStream_t)stream) != cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return h;
+}
 
 extern "C" int spb_sim_set_fields(spb_sim *s, const float *const fields[6], int on_device,
                                   void *stream) {
@@ -1242,90 +1682,31 @@ extern "C" int spb_sim_load_species(spb_sim *s, int species, const float *x, con
   if (n >= (1L << 31) - 256)
     return fail(SPB_ERR_UNSUPPORTED, "spb_sim_load_species: at most 2^31 - 256 particles");
   cudaStream_t st = (cudaStream_t)stream;
-  SimSpecies &S = s->sp[species];
-  // capacity: padded to whole 128-particle chunks plus one spare chunk, so the
-  // 128-bit reads of a cell's last chunk stay inside the allocation
-  const long cap = (ceil_div(std::max<long>(n, 1), 128) + 1) * 128;
-  if (cap > S.cap) {
-    for (int b = 0; b < 2; ++b) {
-      cudaFree(S.cell[b]);
-      S.cell[b] = nullptr;
-      for (float *&p : S.f[b]) {
-        cudaFree(p);
-        p = nullptr;
-      }
-    }
-    S.cap = 0;
-    for (int b = 0; b < 2; ++b) {
-      if (cudaMalloc(&S.cell[b], cap * sizeof(uint32_t)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(SPB_ERR_ALLOC, "spb_sim_load_species: allocation failed");
-      }
-      SPB_CUDA(cudaMemsetAsync(S.cell[b], 0, cap * sizeof(uint32_t), st));
-      for (float *&p : S.f[b]) {
-        if (cudaMalloc(&p, cap * sizeof(float)) != cudaSuccess) {
-          cudaGetLastError();
-          return fail(SPB_ERR_ALLOC, "spb_sim_load_species: allocation failed");
-        }
-        SPB_CUDA(cudaMemsetAsync(p, 0, cap * sizeof(float), st));
-      }
-    }
-    S.cap = cap;
-  }
-  S.n = n;
-  S.cur = 0;
   const float *src[7] = {x, y, z, u, v, w, q};
-  float *tmp = nullptr;
+  Flat f;
   if (!on_device && n > 0) {
-    // stage through the second buffer set
+    if (int rc = f.alloc(n)) return rc;
     for (int a = 0; a < 7; ++a) {
-      SPB_CUDA(cudaMemcpyAsync(S.f[1][a], src[a], n * sizeof(float), cudaMemcpyHostToDevice, st));
-      src[a] = S.f[1][a];
-    }
-  }
-  (void)tmp;
-  if (n > 0) {
-    k_load<<<blocks_for(n, 256), 256, 0, st>>>(scalars(s), src[0], src[1], src[2], src[3], src[4],
-                                               src[5], src[6], n, S.cell[0], S.f[0][0], S.f[0][1],
-                                               S.f[0][2], S.f[0][3], S.f[0][4], S.f[0][5],
-                                               S.f[0][6], s->d_err);
-    SPB_CUDA(cudaGetLastError());
-    g_launches++;
-    s->launches++;
-  }
-  // fixed-point scale of the tile partials from max |q| (q never changes)
-  S.fix = 1.0f;
-  if (n > 0) {
-    unsigned *d_max = reinterpret_cast<unsigned *>(s->scan_tmp);
-    SPB_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
-    k_absmax<<<blocks_for(n, 256), 256, 0, st>>>(S.f[0][6], n, d_max);
-    SPB_CUDA(cudaGetLastError());
-    g_launches++;
-    s->launches++;
-    unsigned h = 0;
-    SPB_CUDA(cudaMemcpyAsync(&h, d_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    SPB_CUDA(cudaStreamSynchronize(st));
-    float qmax;
-    std::memcpy(&qmax, &h, sizeof(float));
-    if (qmax > 0.0f && std::isfinite(qmax)) {
-      int e;
-      std::frexp(qmax, &e);                   // qmax < 2^e
-      S.fix = std::ldexp(1.0f, 40 - e);      // |q| * fix < 2^40
+      SPB_CUDA(cudaMemcpyAsync(f.p[a], src[a], n * sizeof(float), cudaMemcpyHostToDevice, st));
+      src[a] = f.p[a];
     }
   }
   const TileImpl *ti = find_tile(s->tile);
-  if (int rc = ti->sort(s, S, st)) return rc;
-  s->cycles_since_sort = 0;
-  return SPB_OK;
+  const int rc = ti->build(s, s->sp[species], src, n, st);
+  f.release(st);
+  s->cycles_since_check = 0;
+  return rc;
 }
 
 extern "C" int spb_sim_resort(spb_sim *s, void *stream) {
   if (!s) return fail(SPB_ERR_INVALID, "spb_sim_resort: null simulation");
-  const TileImpl *ti = find_tile(s->tile);
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaEvent_t b = record_event(s, st);
   for (auto &q : s->sp)
-    if (q.n > 0)
-      if (int rc = ti->sort(s, q, (cudaStream_t)stream)) return rc;
-  s->cycles_since_sort = 0;
+    if (int rc = relayout(s, q, st)) return rc;
+  const cudaEvent_t e = record_event(s, st);
+  if (b && e) s->ev_relayout.push_back({b, e});
+  s->cycles_since_check = 0;
   return SPB_OK;
 }
 
@@ -1336,11 +1717,29 @@ extern "C" int spb_sim_cycle(spb_sim *s, int ncycles, void *stream) {
   const TileImpl *ti = find_tile(s->tile);
   const int k = std::max(1, s->d.resort_every);
   for (int c = 0; c < ncycles; ++c) {
-    if (s->cycles_since_sort >= k)
-      if (int rc = spb_sim_resort(s, stream)) return rc;
-    for (auto &q : s->sp) SPB_CUDA(cudaMemsetAsync(q.mom, 0, 10 * s->nodes * sizeof(double), st));
+    if (s->cycles_since_check >= k) {
+      // re-lay out the species whose overflow list is in use
+      const cudaEvent_t b = record_event(s, st);
+      bool any = false;
+      for (int i = 0; i < (int)s->sp.size(); ++i) {
+        const long o = spb_sim_overflow(s, i, stream);
+        if (o < 0) return fail(SPB_ERR_CUDA, "spb_sim_cycle: overflow counter read failed");
+        if (o > 0) {
+          if (int rc = relayout(s, s->sp[i], st)) return rc;
+          any = true;
+        }
+      }
+      const cudaEvent_t e = record_event(s, st);
+      if (b && e && any) {
+        s->ev_relayout.push_back({b, e});
+      } else {
+        if (b) cudaEventDestroy(b);
+        if (e) cudaEventDestroy(e);
+      }
+      s->cycles_since_check = 0;
+    }
     if (int rc = ti->cycle(s, st)) return rc;
-    s->cycles_since_sort++;
+    s->cycles_since_check++;
   }
   return SPB_OK;
 }
@@ -1379,26 +1778,24 @@ extern "C" int spb_sim_particles(spb_sim *s, int species, float *x, float *y, fl
   if (!s || species < 0 || species >= (int)s->sp.size())
     return fail(SPB_ERR_INVALID, "spb_sim_particles: bad arguments");
   SimSpecies &S = s->sp[species];
-  if (S.n == 0) return SPB_OK;
+  if (S.n == 0 || !S.rec[0]) return SPB_OK;
   if (!x || !y || !z || !u || !v || !w)
     return fail(SPB_ERR_INVALID, "spb_sim_particles: null output array");
   cudaStream_t st = (cudaStream_t)stream;
+  const TileImpl *ti = find_tile(s->tile);
   float *dst[7] = {x, y, z, u, v, w, q};
+  if (on_device) return ti->unload(s, S, dst, st);
+  Flat f;
+  if (int rc = f.alloc(S.n)) return rc;
   float *tmp[7];
-  const int spare = 1 - S.cur;
-  for (int a = 0; a < 7; ++a) tmp[a] = on_device ? dst[a] : (dst[a] ? S.f[spare][a] : nullptr);
-  k_unload<<<blocks_for(S.n, 256), 256, 0, st>>>(
-      scalars(s), S.cell[S.cur], S.f[S.cur][0], S.f[S.cur][1], S.f[S.cur][2], S.f[S.cur][3],
-      S.f[S.cur][4], S.f[S.cur][5], S.f[S.cur][6], S.n, tmp[0], tmp[1], tmp[2], tmp[3], tmp[4],
-      tmp[5], tmp[6]);
-  SPB_CUDA(cudaGetLastError());
-  g_launches++;
-  s->launches++;
-  if (!on_device)
-    for (int a = 0; a < 7; ++a)
-      if (dst[a])
-        SPB_CUDA(cudaMemcpyAsync(dst[a], tmp[a], S.n * sizeof(float), cudaMemcpyDeviceToHost, st));
-  return SPB_OK;
+  for (int a = 0; a < 7; ++a) tmp[a] = dst[a] ? f.p[a] : nullptr;
+  int rc = ti->unload(s, S, tmp, st);
+  for (int a = 0; a < 7 && !rc; ++a)
+    if (dst[a] && cudaMemcpyAsync(dst[a], tmp[a], S.n * sizeof(float), cudaMemcpyDeviceToHost,
+                                  st) != cudaSuccess)
+      rc = fail_cuda(cudaGetLastError(), "spb_sim_particles: copy to host");
+  f.release(st);
+  return rc;
 }
 
 extern "C" int spb_sim_check(spb_sim *s, void *stream) {
@@ -1408,9 +1805,10 @@ extern "C" int spb_sim_check(spb_sim *s, void *stream) {
   SPB_CUDA(cudaMemcpy(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h) {
     SPB_CUDA(cudaMemset(s->d_err, 0, sizeof(int)));
-    if (h & 2) return fail(SPB_ERR_TIMEOUT, "a staged field tile never arrived (bounded wait)");
-    if (h & 4) return fail(SPB_ERR_CUDA, "the counting sort produced an out-of-range slot");
-    if (h & 8) return fail(SPB_ERR_UNSUPPORTED, "shared memory not 128-byte aligned for TMA");
+    if (h & ERRBIT_TIMEOUT) return fail(SPB_ERR_TIMEOUT, "a staged field tile never arrived (bounded wait)");
+    if (h & ERRBIT_SMEM_ALIGN) return fail(SPB_ERR_UNSUPPORTED, "shared memory not 128-byte aligned for TMA");
+    if (h & ERRBIT_LOST)
+      return fail(SPB_ERR_CAPACITY, "a cell's bucket and the overflow list were both full: particles lost");
     return fail(SPB_ERR_OUT_OF_GRID, "a particle left the node array and was clamped");
   }
   return SPB_OK;

@@ -1,27 +1,22 @@
-// Precision form: device data layout and the fused mover + deposit kernel.
+// Precision form: device data layout of the mover + deposit.
 //
-// Particles (per species, HBM-resident SoA, cell-sorted):
-//   cell  uint32  packed active-cell coordinates cz | cy << 11 | cx << 21
-//   ox, oy, oz    float in-cell offsets in cell units, [0, 1]
-//   u, v, w       float velocities
-//   q             float charge x statistical weight
+// Particles (per species, HBM-resident, bucketed by cell):
+//   cell k owns the record slots [base[k], base[k+1]); a record is two float4,
+//   (ox, oy, oz, q) and (u, v, w, 0): in-cell offsets in cell units, charge x
+//   statistical weight, velocities. A cell's particles are the first
+//   min(count, capacity) slots of its bucket; the capacity is the cell's count
+//   at the last layout plus slack, so memory stays ~1.25x the particles
+//   however they cluster. Particles that find their cell's bucket full are
+//   kept in a per-species overflow list (records + cell keys). Buckets are
+//   double-buffered with one shared layout: a cycle reads one set and writes
+//   every pushed particle straight into its new cell's bucket of the other,
+//   so particles stay grouped by cell without a sort.
+// Cells are numbered tile-major (tile_key): the cells of a TX x TY x TZ tile
+// are consecutive, so a tile's buckets are one contiguous range.
 // Fields: one 32-byte record per node (Ex, Ey, Ez, Bx, By, Bz, 0, 0), the
 // reference node layout [nxn][nyn][nzn] (include/Alloc.h:111-124).
 // Moments: FP64 [10][nxn*nyn*nzn] per species, the reference order
 // rhon, Jx, Jy, Jz, pxx, pxy, pxz, pyy, pyz, pzz (src/Mover.cpp:466-570).
-//
-// The kernel: persistent CTAs walk tiles of TX x TY x TZ cells. For each tile
-// one thread stages the tile's E/B nodes plus a one-cell halo into shared
-// memory with a TMA tensor copy; then, species by species, the warps walk the
-// tile's cells (particles are sorted tile-major, so every cell is one
-// contiguous segment) and push 4 consecutive particles per lane, read and
-// written with 128-bit accesses. The NiterMover predictor-corrector
-// iterations gather from the staged tile (or from L2 past the halo). The
-// deposit of particles that end in their segment's cell accumulates in
-// registers and is summed over the warp by recursive halving; particles that
-// changed cell go through a per-warp queue and shared-memory atomics. The
-// FP32 shared-memory partials of the tile are added to the FP64 global
-// moments with double atomics.
 #pragma once
 
 #include <cuda.h>
@@ -41,14 +36,20 @@ __host__ __device__ __forceinline__ int cell_y(uint32_t c) { return (int)((c >> 
 __host__ __device__ __forceinline__ int cell_z(uint32_t c) { return (int)(c & 2047u); }
 
 struct SpeciesDev {
-  uint32_t *cell;
-  float *ox, *oy, *oz, *u, *v, *w, *q;
-  const int *cell_start;  // [ncells + 1] tile-major segment starts
-  double *mom;            // [10][nodes]
-  long n;
-  float qomdt2;
-  float fix;              // fixed-point scale of the tile partials: 2^40 / max|q| (power of 2)
-  double unfix;           // invVOL / fix, applied when the partials are flushed
+  const float4 *rin;   // buckets read this cycle, [slots][2]
+  float4 *rout;        // buckets written this cycle (same layout)
+  const long long *base;   // [ncells + 1] first slot of each cell's bucket
+  const int *cin;      // per-cell fill counters of rin (may exceed the capacity: clamp)
+  int *cout;           // per-cell fill counters of rout (zero at the start of the cycle)
+  const float4 *oin;   // overflow records read this cycle, [ocap][2]
+  const int *okin;     // their cell keys
+  const int *ocin;     // overflow entries of oin (may exceed ocap: clamp)
+  float4 *oout;        // overflow written this cycle
+  int *okout;
+  int *ocout;
+  double *mom;         // [10][nodes]
+  int ocap;
+  float qomdt2;        // qom * (dt/2) / c
 };
 
 struct CycleParams {
@@ -59,19 +60,31 @@ struct CycleParams {
   int periodic[3];
   float hdt[3];               // (dt/2)/d per axis: half-step displacement per unit velocity
   float fdt[3];               // dt/d per axis
-  double scale;               // invVOL in double, applied when the partials are flushed
-  const float *fields8;       // packed node fields in HBM (gathers past the halo)
+  double scale;               // invVOL in double, applied when cell sums reach the moments
+  const float *fields8;       // packed node fields in HBM (gathers past the staged tile)
   int *err;
   int ns;
   SpeciesDev sp[SIM_MAX_SPECIES];
 };
 
-// Sort key: tile-major cell order.
+// Cell key: tile-major cell order. Tile extents are powers of two.
 template <int TX, int TY, int TZ>
 __host__ __device__ __forceinline__ int tile_key(int cx, int cy, int cz, int nty, int ntz) {
-  const int tx = cx / TX, ty = cy / TY, tz = cz / TZ;
-  const int lx = cx % TX, ly = cy % TY, lz = cz % TZ;
+  const unsigned x = (unsigned)cx, y = (unsigned)cy, z = (unsigned)cz;
+  const int tx = (int)(x / TX), ty = (int)(y / TY), tz = (int)(z / TZ);
+  const int lx = (int)(x % TX), ly = (int)(y % TY), lz = (int)(z % TZ);
   return ((tx * nty + ty) * ntz + tz) * (TX * TY * TZ) + (lx * TY + ly) * TZ + lz;
+}
+
+template <int TX, int TY, int TZ>
+__host__ __device__ __forceinline__ void key_cell(int key, int nty, int ntz, int &cx, int &cy,
+                                                  int &cz) {
+  constexpr int TC = TX * TY * TZ;
+  const int t = key / TC, lc = key % TC;
+  const int tz = t % ntz, ty = (t / ntz) % nty, tx = t / (ntz * nty);
+  cx = tx * TX + lc / (TY * TZ);
+  cy = ty * TY + (lc / TZ) % TY;
+  cz = tz * TZ + lc % TZ;
 }
 
 }  // namespace spb

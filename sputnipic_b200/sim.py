@@ -1,9 +1,12 @@
 """Precision form: a device-resident simulation of the mover + deposit
 (spb_sim_* of libsputnipic_b200.so) over torch CUDA tensors.
 
-Particles are kept in HBM as int32 cell + FP32 in-cell offsets, cell-sorted;
-one fused kernel per cycle pushes all species (FP32) and deposits the ten
-moments into FP64 global arrays. See include/sputnipic_b200.h.
+Particles are kept in HBM in per-cell buckets (FP32 in-cell offsets, charge
+and velocities; the cell is implicit) with an overflow list for full buckets.
+A cycle is a push kernel, which writes every particle into its new cell's
+bucket of a second buffer set, and a deposit kernel, which sums each bucket
+in registers and adds the node sums into FP64 moments. See
+include/sputnipic_b200.h.
 """
 from __future__ import annotations
 
@@ -20,7 +23,8 @@ def _stream(stream):
 
 
 class Simulation:
-    def __init__(self, wl, tile=(8, 4, 4), resort_every=1, ctas=0, species=None, variant=0):
+    def __init__(self, wl, tile=(8, 4, 4), resort_every=4, ctas=0, species=None, variant=0,
+                 bucket_slots=0):
         self.lib = _lib.load()
         self.wl = wl
         species = list(range(len(wl.species))) if species is None else list(species)
@@ -36,6 +40,7 @@ class Simulation:
         for a in range(3):
             d.tile[a] = tile[a]
         d.resort_every, d.ctas, d.variant = resort_every, ctas, variant
+        d.bucket_slots = bucket_slots
         h = ctypes.c_void_p()
         _lib.check(self.lib.spb_sim_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h
@@ -61,6 +66,17 @@ class Simulation:
     def count(self, s: int) -> int:
         return self.lib.spb_sim_count(self.h, s)
 
+    def bucket_slots(self, s: int) -> int:
+        """Record slots of species s's bucket layout (summed over cells)."""
+        return self.lib.spb_sim_bucket_slots(self.h, s)
+
+    def overflow(self, s: int, stream=None) -> int:
+        """Entries in species s's overflow list (synchronises)."""
+        n = self.lib.spb_sim_overflow(self.h, s, _stream(stream))
+        if n < 0:
+            raise RuntimeError("spb_sim_overflow failed")
+        return n
+
     def set_fields(self, fields, stream=None):
         """Six float32 tensors (CUDA or CPU) Ex, Ey, Ez, Bxn, Byn, Bzn."""
         on_dev = int(fields[0].is_cuda)
@@ -78,6 +94,7 @@ class Simulation:
         _lib.check(self.lib.spb_sim_cycle(self.h, ncycles, _stream(stream)))
 
     def resort(self, stream=None):
+        """Re-lay out every species (compact buckets + overflow list)."""
         _lib.check(self.lib.spb_sim_resort(self.h, _stream(stream)))
 
     def moments(self, s: int, bc: bool = False, stream=None):
@@ -92,7 +109,7 @@ class Simulation:
 
     def particles(self, s: int, stream=None) -> dict:
         """Positions (domain units), velocities and charges of species s,
-        float32 CUDA tensors in the simulation's (sorted) order."""
+        float32 CUDA tensors in cell order (then the overflow list)."""
         import torch
         n = self.count(s)
         out = {k: torch.empty(n, dtype=torch.float32, device="cuda") for k in "xyzuvwq"}
@@ -107,24 +124,29 @@ class Simulation:
         _lib.check(self.lib.spb_sim_set_timing(self.h, 1 if on else 0))
 
     def timing(self):
-        """(cycle kernel ms, launches, sort ms, sorts) since the last call."""
-        c, nc, o, no = ctypes.c_double(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
-        _lib.check(self.lib.spb_sim_timing(self.h, ctypes.byref(c), ctypes.byref(nc),
-                                           ctypes.byref(o), ctypes.byref(no)))
-        return c.value, nc.value, o.value, no.value
+        """(cycle kernels ms, cycles, re-layout ms, re-layouts) since the last
+        timing query."""
+        t = self.kernel_timing()
+        return t["push_ms"] + t["deposit_ms"], t["cycles"], t["relayout_ms"], t["relayouts"]
+
+    def kernel_timing(self) -> dict:
+        """Summed CUDA-event milliseconds of the push and deposit kernels and
+        of the re-layouts since the last timing query (clears them)."""
+        p, d, r = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        nc, nr = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.lib.spb_sim_kernel_timing(self.h, ctypes.byref(p), ctypes.byref(d),
+                                                  ctypes.byref(nc), ctypes.byref(r),
+                                                  ctypes.byref(nr)))
+        return {"push_ms": p.value, "deposit_ms": d.value, "cycles": nc.value,
+                "relayout_ms": r.value, "relayouts": nr.value}
 
 
-def autotune(wl, fields, parts, tiles=((8, 4, 4), (4, 4, 4), (8, 8, 4)), variants=(0, 1),
-             resorts=(1, 2, 4, 8), cycles=2, stream=None):
-    """Picks the tile shape, deposit variant and resort interval with the
-    highest particles/s on the given workload (device tensors; left intact).
-
-    Tile and variant are timed on `cycles` cycles right after a sort (CUDA
-    events around the cycle kernel). The resort interval k is then chosen from
-    a model of the measured costs: per cycle, the kernel time grows with the
-    cycles since the last sort (particles drift out of their cells), while a
-    sort costs a fixed time every k cycles.
-    Returns a dict with the choice and the measurements."""
+def autotune(wl, fields, parts, tiles=((8, 4, 4), (4, 4, 4), (8, 8, 4)), variants=(0, 1, 2),
+             cycles=3, stream=None):
+    """Picks the tile shape and push-kernel residency (variant) with the
+    shortest push + deposit time on the given workload (device tensors; left
+    intact), timed with CUDA events over `cycles` cycles after one warm-up
+    cycle. Returns a dict with the choice and the measurements."""
     import torch
     n = sum(p["x"].numel() for p in parts)
     best, trials = None, []
@@ -137,32 +159,17 @@ def autotune(wl, fields, parts, tiles=((8, 4, 4), (4, 4, 4), (8, 8, 4)), variant
             for s, p in enumerate(parts):
                 sim.load_species(s, p)
             sim.cycle(1)                       # warm-up (first launch, attributes)
-            sim.resort()
             sim.set_timing(True)
-            sim.timing()
+            sim.kernel_timing()
             sim.cycle(cycles)
-            ms, nc, _, _ = sim.timing()
-            sim.resort()
-            _, _, sort_ms, ns = sim.timing()
-            per = ms / max(nc, 1)
+            t = sim.kernel_timing()
+            sim.close()
+            per = (t["push_ms"] + t["deposit_ms"]) / max(t["cycles"], 1)
             trials.append({"tile": list(tile), "variant": var, "cycle_ms": per,
-                           "sort_ms": sort_ms})
+                           "push_ms": t["push_ms"] / max(t["cycles"], 1),
+                           "deposit_ms": t["deposit_ms"] / max(t["cycles"], 1)})
             if best is None or per < best[0]:
-                best = (per, tile, var, sort_ms, sim)
-            else:
-                sim.close()
-    per0, tile, var, sort_ms, sim = best
-    # drift cost: time cycles 1..max(resorts) after a sort
-    sim.resort()
-    sim.timing()
-    drift = []
-    for _ in range(max(resorts)):
-        sim.cycle(1)
-        drift.append(sim.timing()[0])
-    sim.close()
+                best = (per, tile, var)
     torch.cuda.synchronize()
-    costs = {k: (sum(drift[:k]) + sort_ms) / k for k in resorts}
-    k = min(costs, key=costs.get)
-    return {"tile": tile, "variant": var, "resort_every": k, "trials": trials,
-            "drift_ms": drift, "sort_ms": sort_ms, "ms_per_cycle_model": costs,
+    return {"tile": best[1], "variant": best[2], "cycle_ms": best[0], "trials": trials,
             "particles": n}
