@@ -313,7 +313,9 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
         tr = traffic.get("k_" + k)
         kernels[k] = {"kernel": name, "ms_mean": kms, "algorithmic_bytes": alg,
                       "achieved": ach, "frac": ach / peak, "share_of_step": kt[k + "_ms"] / ms,
-                      "traffic": (tr["dram_bytes_per_particle"] * n if tr else None)}
+                      "traffic": (tr["dram_bytes_per_particle"] * n +
+                                  tr.get("dram_bytes_per_node_species", 0.0) * wl.nodes * ns
+                                  if tr else None)}
     dom = max(kernels, key=lambda k: kernels[k]["ms_mean"])
     d = kernels[dom]
     cyc_ms = kernels["push"]["ms_mean"] + kernels["deposit"]["ms_mean"]

@@ -107,17 +107,21 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
 // ---------------------------------------------------------------------------
 
 // Gather cell and fraction of a predicted position p (cells, relative to the
-// particle's cell c). Below the domain the reference's int() truncates toward
-// zero, so the cell rounds up and the fraction goes negative. Branch-free;
-// cells outside [-1, N] are left to the gather's bounds handling.
+// particle's cell c), rounding down. Cells outside [-1, N] are left to the
+// gather's bounds handling.
 __device__ __forceinline__ void locate(float p, int c, int N, int &g, float &f) {
   const float lim = (float)(N + 8);
   const float s = fminf(fmaxf(floorf(p), -lim), lim);
-  int gg = c + __float2int_rz(s);
-  float ff = p - s;
-  const bool trunc = (gg < 0) & (ff != 0.0f);
-  g = trunc ? gg + 1 : gg;
-  f = trunc ? ff - 1.0f : ff;
+  g = c + __float2int_rz(s);
+  f = p - s;
+}
+
+// Below the domain the reference's int() truncates toward zero
+// (src/Mover.cpp:39-41): the cell rounds up and the fraction goes negative.
+__device__ __forceinline__ void truncate_below(int &g, float &f) {
+  const bool trunc = (g < 0) & (f != 0.0f);
+  g = trunc ? g + 1 : g;
+  f = trunc ? f - 1.0f : f;
 }
 
 // Particle BC on one axis in cell units: "x > L" first, then "x < 0"
@@ -256,6 +260,11 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
       locate(ox + dx, cx, P.nxc, gx, fx);
       locate(oy + dy, cy, P.nyc, gy, fy);
       locate(oz + dz, cz, P.nzc, gz, fz);
+      if (__any_sync(0xffffffffu, (gx | gy | gz) < 0)) {   // some lane is below the domain
+        truncate_below(gx, fx);
+        truncate_below(gy, fy);
+        truncate_below(gz, fz);
+      }
     }
     const Field6 F = gather<TX, TY, TZ>(P, sF, c0x, c0y, c0z, gx, gy, gz, fx, fy, fz);
     const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
@@ -279,13 +288,20 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   advance(cx, ox, up * P.fdt[0], P.nxc);
   advance(cy, oy, vp * P.fdt[1], P.nyc);
   advance(cz, oz, wp * P.fdt[2], P.nzc);
-  bc_cell(cx, ox, u, P.nxc, P.periodic[0]);
-  bc_cell(cy, oy, v, P.nyc, P.periodic[1]);
-  bc_cell(cz, oz, w, P.nzc, P.periodic[2]);
-  bad |= (cx < 0) | (cx >= P.nxc) | (cy < 0) | (cy >= P.nyc) | (cz < 0) | (cz >= P.nzc);
-  cx = min(max(cx, 0), P.nxc - 1);
-  cy = min(max(cy, 0), P.nyc - 1);
-  cz = min(max(cz, 0), P.nzc - 1);
+  // the particle BC, the range flag and the clamps change nothing for a
+  // particle whose new cell is inside the domain: skipped unless some lane
+  // needs them
+  const bool inside = ((unsigned)cx < (unsigned)P.nxc) & ((unsigned)cy < (unsigned)P.nyc) &
+                      ((unsigned)cz < (unsigned)P.nzc);
+  if (!__all_sync(0xffffffffu, inside)) {
+    bc_cell(cx, ox, u, P.nxc, P.periodic[0]);
+    bc_cell(cy, oy, v, P.nyc, P.periodic[1]);
+    bc_cell(cz, oz, w, P.nzc, P.periodic[2]);
+    bad |= (cx < 0) | (cx >= P.nxc) | (cy < 0) | (cy >= P.nyc) | (cz < 0) | (cz >= P.nzc);
+    cx = min(max(cx, 0), P.nxc - 1);
+    cy = min(max(cy, 0), P.nyc - 1);
+    cz = min(max(cz, 0), P.nzc - 1);
+  }
 }
 
 // Deposit terms of one particle added to 40 packed accumulators:
@@ -409,25 +425,33 @@ __device__ __forceinline__ void issue_slot(const SpeciesDev &S, Pending &p, floa
   stage[32 + lane] = b;
 }
 
+constexpr int PCH = 32;    // records per bulk chunk of the push (1 KB)
+
 // The mover (mover_PC, src/Mover.cpp:4-162) for every species. Persistent
 // CTAs walk tiles of TX x TY x TZ cells; one thread stages the tile's E/B
 // nodes plus a one-cell halo into shared memory with a TMA tensor copy (two
 // stages: the next tile's copy overlaps this tile's work). Warps walk the
-// tile's cells, one particle per lane; the gathers of the NiterMover
-// iterations read the staged tile (or L2 past the halo), and every pushed
-// particle is written into the bucket of its new cell. Afterwards the CTAs
-// push the overflow entries (gathers from L2).
+// tile's cells, one particle per lane, with the cells' records streamed
+// through two shared-memory chunk buffers per warp by bulk copies; the
+// gathers of the NiterMover iterations read the staged tile (or L2 past the
+// halo), and every pushed particle is written into the bucket of its new
+// cell. Afterwards the CTAs push the overflow entries (gathers from L2).
 template <int TX, int TY, int TZ, int MINB>
 __global__ void __launch_bounds__(SIM_TPB, MINB)
     k_push(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P) {
   using T = Tile<TX, TY, TZ>;
+  constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
+  static_assert(T::TC % SIM_NW == 0 && NC <= 32, "cells per warp must fit a warp's lanes");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
   float4 *sRec = reinterpret_cast<float4 *>(sF0 + 2 * T::SF);       // NW x 64 staged records
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sRec + SIM_NW * 64); // 2 barriers
+  float4 *sBuf = sRec + SIM_NW * 64;                                // NW x 2 x PCH records
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sBuf + SIM_NW * 2 * PCH * 2);  // 2 + 2 NW
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float4 *wrec = sRec + warp * 64;   // this warp's staged records
+  float4 *buf = sBuf + warp * 2 * PCH * 2;
+  uint64_t *cbar = bar + 2 + warp * 2;
   if (smem_addr(sF0) & 127u) {   // TMA destinations need 128-byte alignment
     if (tid == 0) atomicOr(P.err, ERRBIT_SMEM_ALIGN);
     return;
@@ -435,6 +459,10 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
+  }
+  if (lane == 0) {
+    mbar_init(cbar, 1);
+    mbar_init(cbar + 1, 1);
   }
   __syncthreads();
 
@@ -449,6 +477,8 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
   };
   if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
   int bad = 0, lost = 0, it = 0;
+  unsigned phase = 0, inflight = 0;   // record chunks, per buffer: next parity, copy issued
+  bool dead = false;                  // a bounded wait for a record chunk ran out
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
     const int stage = it & 1;
     // prefetch the next tile's fields into the other stage (read by the
@@ -469,40 +499,99 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
 
     for (int s = 0; s < P.ns; ++s) {
       const SpeciesDev &S = P.sp[s];
+      // lane j < NC holds bucket start, capacity and particle count of the
+      // warp's j-th cell (tile-local cell warp + j * NW)
+      long long cb = 0;
+      int ccap = 0, cc = 0;
+      if (lane < NC) {
+        const int key = tile * T::TC + warp + lane * SIM_NW;
+        cb = S.base[key];
+        ccap = (int)(S.base[key + 1] - cb);
+        cc = min(S.cin[key], ccap);
+      }
+      int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
+      auto issue_next = [&]() {         // all lanes call; lane 0 copies
+        while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
+          ++pj;
+          poff = 0;
+        }
+        if (pj < NC && !dead) {
+          const int len = min(PCH, __shfl_sync(FULL, cc, pj) - poff);
+          const long long b0 = __shfl_sync(FULL, cb, pj);
+          if (lane == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(cbar + nbuf, (unsigned)len * 32u);
+            bulk_load(buf + nbuf * PCH * 2, S.rin + 2 * (b0 + poff), (unsigned)len * 32u,
+                      cbar + nbuf);
+          }
+          inflight |= 1u << nbuf;
+          poff += len;
+          nbuf ^= 1;
+        }
+      };
       Pending pend;
       pend.valid = false;
       pend.sbase0 = 0;
-      for (int lc = warp; lc < T::TC; lc += SIM_NW) {
+      issue_next();
+      int cbuf = 0;
+      for (int j = 0; j < NC; ++j) {
+        const int cnt = __shfl_sync(FULL, cc, j);
+        if (cnt <= 0 || dead) continue;
+        const long long b0 = __shfl_sync(FULL, cb, j);
+        const long long b1 = b0 + __shfl_sync(FULL, ccap, j);
+        const int lc = warp + j * SIM_NW;
         const int key = tile * T::TC + lc;
-        const long long b0 = S.base[key], b1 = S.base[key + 1];
-        const int cnt = (int)min((long long)S.cin[key], b1 - b0);
-        if (cnt <= 0) continue;
         const int cx0 = c0x + lc / (TY * TZ), cy0 = c0y + (lc / TZ) % TY, cz0 = c0z + lc % TZ;
-        const float4 *src = S.rin + 2 * b0;
 #pragma unroll 1
-        for (int base = 0; base < cnt; base += 32) {
-          const int i = base + lane;
-          const bool valid = i < cnt;
-          // idle lanes of the last slot push a copy of the cell's last
-          // particle (results discarded): one instruction stream per warp
-          const int ii = valid ? i : cnt - 1;
-          const float4 a = src[2 * ii], b = src[2 * ii + 1];
-          int cx = cx0, cy = cy0, cz = cz0;
-          float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
-          int pbad = 0;
-          push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
-          bad |= valid ? pbad : 0;
-          const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
-          flush(S, pend, wrec, lane, lost);   // the previous slot's counters are back
-          __syncwarp();
-          issue_slot(S, pend, wrec, key, b0, b1, nkey, valid, make_float4(ox, oy, oz, a.w),
-                     make_float4(u, v, w, 0.f), lane);
+        for (int off = 0; off < cnt; off += PCH) {
+          issue_next();   // the following chunk streams in while this one is pushed
+          const bool ok = mbar_wait_bounded(cbar + cbuf, (phase >> cbuf) & 1u);
+          if (!__all_sync(FULL, ok)) {
+            dead = true;
+            break;
+          }
+          phase ^= 1u << cbuf;
+          inflight &= ~(1u << cbuf);
+          const int len = min(PCH, cnt - off);
+          const float4 *rb = buf + cbuf * PCH * 2;
+#pragma unroll 1
+          for (int base = 0; base < len; base += 32) {
+            const int i = base + lane;
+            const bool valid = i < len;
+            // idle lanes of the last slot push a copy of the chunk's last
+            // particle (results discarded): one instruction stream per warp
+            const int ii = valid ? i : len - 1;
+            const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
+            int cx = cx0, cy = cy0, cz = cz0;
+            float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
+            int pbad = 0;
+            push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
+                             pbad);
+            bad |= valid ? pbad : 0;
+            const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
+            flush(S, pend, wrec, lane, lost);   // the previous slot's counters are back
+            __syncwarp();
+            issue_slot(S, pend, wrec, key, b0, b1, nkey, valid, make_float4(ox, oy, oz, a.w),
+                       make_float4(u, v, w, 0.f), lane);
+          }
+          __syncwarp();   // every lane is done with this buffer before it is refilled
+          cbuf ^= 1;
         }
       }
       flush(S, pend, wrec, lane, lost);
       __syncwarp();
     }
-    __syncthreads();   // every warp is done with this stage before it is refilled
+    // every warp is done with this field stage before it is refilled
+    if (__syncthreads_or(dead)) {
+      // a record chunk never arrived: report, wait (bounded) for this warp's
+      // copies still in flight and for the prefetched field stage, give up
+      if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+      for (int b = 0; b < 2; ++b)
+        if (inflight & (1u << b)) mbar_wait_bounded(cbar + b, (phase >> b) & 1u);
+      if (tile + (int)gridDim.x < ntiles)
+        mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
+      return;
+    }
   }
 
   // overflow entries: pushed with gathers from L2 (the staged-tile origin is
@@ -1115,7 +1204,8 @@ int encode_field_map(spb_sim *s) {
 
 template <int TX, int TY, int TZ>
 size_t push_smem() {
-  return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + (size_t)SIM_NW * 64 * sizeof(float4) + 16;
+  return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + (size_t)SIM_NW * 64 * sizeof(float4) +
+         (size_t)SIM_NW * 2 * PCH * 2 * sizeof(float4) + (2 + 2 * SIM_NW) * sizeof(uint64_t);
 }
 template <int TX, int TY, int TZ>
 size_t deposit_smem() {
