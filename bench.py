@@ -44,11 +44,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from sputnipic_b200 import ranks as R  # noqa: E402
 from sputnipic_b200 import workload as W  # noqa: E402
 
 METRIC = "mover_p2g_particles_per_s"
 UNIT = "particles/s"
-# the reference GPU build, same GEM config, 5.208 s and 4.942 s
+# the reference GPU build's published times on the same GEM config, 5.208 s and 4.942 s
 # per mover+interp cycle of 262,144,000 particles (README.md:76,93)
 PUBLISHED_PPS = 262_144_000 / ((5.208 + 4.942) / 2)
 
@@ -202,12 +203,7 @@ def device_timed(torch, dist, stream, steps, fn):
         fn()
     t1.record(stream)
     torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    return ms
+    return R.max_over_ranks(t0.elapsed_time(t1), dist)
 
 
 def measure_plain(args, torch, wl, fields, parts, dist, stream):
@@ -241,7 +237,7 @@ def measure_plain(args, torch, wl, fields, parts, dist, stream):
             timed("p2g", counts[s], lambda: ctx.p2g(parts[s], mom[s]), record)
             ctx.apply_bc_ids(mom[s], wl.periodic)
         if dist is not None:
-            dist.all_reduce(mom)
+            R.reduce_moments(mom, dist)
 
     for _ in range(args.warmup):
         step()
@@ -332,7 +328,8 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
         "relayouts": {"count": kt["relayouts"], "ms": kt["relayout_ms"]},
     }
     sim.close()
-    return {"value": n * world * args.steps / (ms / 1e3), "ms": ms, "roofline": roofline,
+    return {"value": R.aggregate_rate(n, world, args.steps, ms / 1e3), "ms": ms,
+            "roofline": roofline,
             "clocks": clk.summary(), "launches": launches, "autotune": tune,
             "buckets": {"mean_slots_per_cell": slots, "overflow_entries": overflow}}
 
@@ -347,7 +344,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
     _lib.load()
-    wl = W.gem(seed=rank)
+    wl = R.rank_workload(W.gem(), rank)
     if args.nspecies != 4 or args.ppc != 125:
         wl = wl.with_(lattice=5 if args.ppc == 125 else 0,
                       species=W.gem_species((args.ppc,) * 4)[:args.nspecies])
@@ -456,13 +453,9 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
-    t = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = R.max_over_ranks(time.perf_counter() - t0, dist)
     dropin.release_all()
-    return {"value": sum(n) * world * steps / t, "unit": UNIT, "h2d_bytes_per_step": h2d,
+    return {"value": R.aggregate_rate(sum(n), world, steps, t), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "ms_per_step": 1e3 * t / steps,
             "path": "spb_mover_PC + spb_interpP2G on reference structs, COPY residency, "
                     "pinned host arrays; timed on the host clock"}
