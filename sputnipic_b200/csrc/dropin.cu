@@ -22,6 +22,7 @@
 // stream, so different species deposit concurrently. Field upload + mover
 // launch hold the grid context's lock until the mover finishes, because the
 // packed field buffer is shared.
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -38,6 +39,9 @@ namespace {
 
 struct Species {
   cudaStream_t stream = nullptr;
+  cudaStream_t pipe[2] = {};      // COPY residency: streams the particle chunks alternate on
+  cudaEvent_t ev_in = nullptr;    // fields / moments uploaded
+  cudaEvent_t ev_done[2] = {};    // a pipe stream's chunks finished
   long cap = 0;
   float *d[7] = {};           // x y z u v w q
   float *d_mom = nullptr;     // 10 * mom_nodes
@@ -54,6 +58,11 @@ struct Species {
     cudaFree(d_mom);
     cudaFree(d_err);
     if (stream) cudaStreamDestroy(stream);
+    for (int j = 0; j < 2; ++j) {
+      if (pipe[j]) cudaStreamDestroy(pipe[j]);
+      if (ev_done[j]) cudaEventDestroy(ev_done[j]);
+    }
+    if (ev_in) cudaEventDestroy(ev_in);
   }
 };
 
@@ -253,6 +262,104 @@ spb_push push_of(const struct particles *part, const struct parameters *param) {
 
 enum class Op { Mover, MoverV, Interp, Fused };
 
+// COPY residency for large species: the particles go through PCIe in chunks
+// of PIPE_CHUNK, alternating between two streams, so one chunk's upload, its
+// kernel and the previous chunk's download run at the same time (with pinned
+// host arrays; pageable arrays are copied synchronously by CUDA, which is
+// still correct). The results are those of one launch over all particles: the
+// mover is per particle and the deposit adds into the same moments.
+constexpr long PIPE_CHUNK = 1L << 22;
+
+int ensure_pipe(Species *sp) {
+  for (int j = 0; j < 2; ++j) {
+    if (!sp->pipe[j]) SPB_CUDA(cudaStreamCreateWithFlags(&sp->pipe[j], cudaStreamNonBlocking));
+    if (!sp->ev_done[j])
+      SPB_CUDA(cudaEventCreateWithFlags(&sp->ev_done[j], cudaEventDisableTiming));
+  }
+  if (!sp->ev_in) SPB_CUDA(cudaEventCreateWithFlags(&sp->ev_in, cudaEventDisableTiming));
+  return SPB_OK;
+}
+
+int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfield *field,
+                       struct interpDensSpecies *ids, spb_grid_ctx *ctx,
+                       struct parameters *param, long n) {
+  const bool moves = op != Op::Interp;
+  const bool deposits = op == Op::Interp || op == Op::Fused;
+  if (int rc = ensure_pipe(sp)) return rc;
+  float *h[7];
+  host_particle_arrays(part, h);
+  const int nin = deposits ? 7 : 6;   // arrays uploaded: x..w, and q to deposit
+  for (int a = 0; a < nin; ++a)
+    if (!h[a]) return fail(SPB_ERR_INVALID, "particle array is null");
+  const long nodes = spb_grid_nodes(ctx);
+  float *hm[10] = {};
+  float *dm[10] = {};
+  // fields are shared by all species: upload, launches and completion of the
+  // mover happen under the grid lock
+  std::unique_lock<std::mutex> glk(ctx->mu, std::defer_lock);
+  if (moves) {
+    glk.lock();
+    const float *f[6] = {field->Ex_flat, field->Ey_flat, field->Ez_flat,
+                         field->Bxn_flat, field->Byn_flat, field->Bzn_flat};
+    for (int a = 0; a < 6; ++a)
+      if (!f[a]) return fail(SPB_ERR_INVALID, "field array is null");
+    if (int rc = spb_grid_set_fields(ctx, f, 0, sp->stream)) return rc;
+  }
+  if (deposits) {
+    host_moment_arrays(ids, hm);
+    if (int rc = ensure_moments(sp, nodes)) return rc;
+    for (int m = 0; m < 10; ++m) {
+      if (!hm[m]) return fail(SPB_ERR_INVALID, "moment array is null");
+      dm[m] = sp->d_mom + m * nodes;
+      SPB_CUDA(cudaMemcpyAsync(dm[m], hm[m], nodes * sizeof(float), cudaMemcpyHostToDevice,
+                               sp->stream));
+    }
+  }
+  SPB_CUDA(cudaEventRecord(sp->ev_in, sp->stream));
+  for (int j = 0; j < 2; ++j) SPB_CUDA(cudaStreamWaitEvent(sp->pipe[j], sp->ev_in, 0));
+  const PushDev p = moves ? make_push(push_of(part, param)) : PushDev{};
+  const PackedFields F{ctx->d_eb4, ctx->d_eb2};
+  long k = 0;
+  for (long off = 0; off < n; off += PIPE_CHUNK, ++k) {
+    cudaStream_t s = sp->pipe[k & 1];
+    const long cnt = std::min(PIPE_CHUNK, n - off);
+    const size_t bytes = (size_t)cnt * sizeof(float);
+    float *d[7];
+    for (int a = 0; a < 7; ++a) d[a] = sp->d[a] + off;
+    for (int a = 0; a < nin; ++a)
+      SPB_CUDA(cudaMemcpyAsync(d[a], h[a] + off, bytes, cudaMemcpyHostToDevice, s));
+    int rc;
+    if (op == Op::Fused)
+      rc = launch_plain_mover_interp(ctx->geom, p, F, d[0], d[1], d[2], d[3], d[4], d[5], d[6],
+                                     cnt, dm, sp->d_err, s);
+    else if (moves)
+      rc = launch_plain_mover(ctx->geom, p, F, d[0], d[1], d[2], d[3], d[4], d[5], cnt,
+                              sp->d_err, s, op == Op::MoverV ? 1 : 0);
+    else
+      rc = launch_plain_p2g(ctx->geom, d[0], d[1], d[2], d[3], d[4], d[5], d[6], cnt, dm,
+                            sp->d_err, s);
+    if (rc) return rc;
+    ctx->launches++;
+    if (moves)
+      for (int a = 0; a < 6; ++a)
+        SPB_CUDA(cudaMemcpyAsync(h[a] + off, d[a], bytes, cudaMemcpyDeviceToHost, s));
+  }
+  for (int j = 0; j < 2; ++j) {
+    SPB_CUDA(cudaEventRecord(sp->ev_done[j], sp->pipe[j]));
+    SPB_CUDA(cudaStreamWaitEvent(sp->stream, sp->ev_done[j], 0));
+  }
+  if (deposits)
+    for (int m = 0; m < 10; ++m)
+      SPB_CUDA(cudaMemcpyAsync(hm[m], dm[m], nodes * sizeof(float), cudaMemcpyDeviceToHost,
+                               sp->stream));
+  SPB_CUDA(cudaStreamSynchronize(sp->stream));
+  sp->dev_current = true;
+  sp->nop = n;
+  sp->q_current = deposits;
+  sp->host_stale = false;
+  return take_device_error(sp);
+}
+
 // The common body of the four drop-ins.
 int run(Op op, struct particles *part, struct EMfield *field, struct interpDensSpecies *ids,
         struct grid *grd, struct parameters *param) {
@@ -277,6 +384,8 @@ int run(Op op, struct particles *part, struct EMfield *field, struct interpDensS
   const long n = part->nop;
   if (int rc = ensure_capacity(sp, n)) return rc;
   const bool device_mode = S().residency == SPB_RESIDENCY_DEVICE;
+  if (!device_mode && n > PIPE_CHUNK)
+    return run_copy_pipelined(op, sp, part, field, ids, ctx, param, n);
   // particles: upload unless the device copy is known to be current
   if (!device_mode || !sp->dev_current || sp->nop != n) {
     if (int rc = copy_particles(sp, part, 0, 6, true)) return rc;

@@ -299,3 +299,28 @@ def test_out_of_grid_particle_is_flagged_not_faulting(orc32):
     out = dropin.particle_arrays(P)
     for k in "xyzuvw":
         assert np.array_equal(out[k][good], sel[k])
+
+
+def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64):
+    """COPY residency moves species above 4M particles through PCIe in chunks on
+    alternating streams. 9.2M particles (two chunk boundaries and a ragged last
+    chunk): mover_PC bit-identical to the reference code, interpP2G within the
+    reordering bound, as for one launch."""
+    wl = W.small_gem(nxc=64, nyc=32, nzc=32, E_amp=1e-3,
+                     species=W.gem_species((140, 140, 140, 140)))
+    fields = W.gem_fields(wl)
+    part = W.gem_particles(wl, 0)
+    assert len(part["x"]) > 2 * (1 << 22)
+    ref = {k: part[k].copy() for k in "xyzuvwq"}
+    param, grd, field, P = build(wl, fields, [{k: part[k].copy() for k in "xyzuvwq"}])
+    ids = dropin.interp_dens_species_allocate(grd, 0)
+    assert dropin.mover_PC(P[0], field, grd, param) == 0
+    dropin.interpP2G(P[0], ids, grd, raise_on_error=True)
+    setup = oracle.setup_from(wl)
+    orc32.mover_pc(setup, fields, ref, wl.species[0].qom)
+    out = dropin.particle_arrays(P[0])
+    for k in "xyzuvw":
+        assert np.array_equal(out[k], ref[k]), k
+    mom = [np.zeros(wl.nodes, np.float32) for _ in range(10)]
+    orc32.interp_p2g(setup, ref, mom)
+    check_moments(np.stack(dropin.moments(ids)), np.stack(mom), abs_moments(orc64, setup, wl, ref))
