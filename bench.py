@@ -273,7 +273,8 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
         from sputnipic_b200.sim import autotune
         tune = autotune(wl, fields, parts)
         args.tile, args.variant = list(tune["tile"]), tune["variant"]
-    sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort, variant=args.variant)
+    sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort, variant=args.variant,
+                     graph=not args.no_graph)
     sim.set_fields(fields)
     for s, p in enumerate(parts):
         sim.load_species(s, p)
@@ -283,13 +284,17 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     if rc:
         raise RuntimeError(f"precision warm-up status {rc}: {_lib.last_error()}")
     lib = _lib.load()
-    sim.set_timing(True)
-    sim.kernel_timing()
     l0 = lib.spb_launch_count()
     local_rank = torch.cuda.current_device()
     with Clocks(local_rank) as clk:
         ms = device_timed(torch, dist, stream, args.steps, lambda: sim.cycle(1))
     launches = lib.spb_launch_count() - l0
+    # per-kernel breakdown: a separate pass with CUDA events around each kernel
+    # (direct launches), outside the timed region above
+    sim.set_timing(True)
+    sim.kernel_timing()
+    for _ in range(min(args.steps, 4)):
+        sim.cycle(1)
     kt = sim.kernel_timing()
     sim.set_timing(False)
     rc = sim.check()
@@ -308,7 +313,7 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
         ach = alg / (kms / 1e3) / 1e9
         tr = traffic.get("k_" + k)
         kernels[k] = {"kernel": name, "ms_mean": kms, "algorithmic_bytes": alg,
-                      "achieved": ach, "frac": ach / peak, "share_of_step": kt[k + "_ms"] / ms,
+                      "achieved": ach, "frac": ach / peak, "share_of_step": kms / (ms / args.steps),
                       "traffic": (tr["dram_bytes_per_particle"] * n +
                                   tr.get("dram_bytes_per_node_species", 0.0) * wl.nodes * ns
                                   if tr else None)}
@@ -394,6 +399,7 @@ def run_ours(args, rank, world, local_rank):
                                "velocities; fp32 push; fp32 per-cell register sums -> "
                                "fp64 moments)",
                        "tile": list(args.tile), "overflow_check_every": args.resort,
+                       "cuda_graph": not args.no_graph,
                        "push_variant": args.variant, "buckets": prec["buckets"],
                        "autotune": prec["autotune"],
                        "particles_per_gpu": ntot, "grid_cells": [wl.nxc, wl.nyc, wl.nzc],
@@ -481,6 +487,8 @@ def main():
                     help="push kernel residency: 0 two CTAs per SM, 1 three, 2 four")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the tile shape and push variant first (timed on this workload)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch each cycle directly instead of replaying a CUDA graph")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -215,6 +215,9 @@ typedef struct spb_sim_desc {
   int bucket_slots;         /* record slots of every cell's bucket (0: each
                                cell's count at the last layout + max(16,
                                count/4), rounded up to 4) */
+  int graph;                /* 1: each cycle's launches (zeroing, push,
+                               deposit) replay as a CUDA graph captured per
+                               buffer-parity pattern; not while timing */
 } spb_sim_desc;
 
 /* Whether a tile shape has an instantiated kernel. */

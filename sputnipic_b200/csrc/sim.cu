@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -1162,6 +1163,13 @@ struct spb_sim {
   CUtensorMap fmap{};
   bool fields_set = false;
   int cycles_since_check = 0;
+  // CUDA graphs of one cycle's launches, keyed by the species' buffer parities;
+  // captured and replayed on gstream, ordered after the caller's stream
+  std::map<unsigned, cudaGraphExec_t> graphs;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t gev[2] = {nullptr, nullptr};
+  long cycles_run = 0;
+  bool graph_failed = false;
   std::vector<SimSpecies> sp;
   long launches = 0;
   // optional CUDA-event timing of the cycle kernels and of the relayouts
@@ -1690,8 +1698,81 @@ extern "C" int spb_sim_kernel_timing(spb_sim *s, double *push_ms, double *deposi
   return SPB_OK;
 }
 
+namespace {
+
+void drop_graphs(spb_sim *s) {
+  for (auto &g : s->graphs) cudaGraphExecDestroy(g.second);
+  s->graphs.clear();
+}
+
+unsigned parity_key(const spb_sim *s) {
+  unsigned k = 0;
+  for (size_t i = 0; i < s->sp.size(); ++i) k |= (unsigned)s->sp[i].cur << i;
+  return k;
+}
+
+// One cycle. With desc.graph (and timing off) the cycle's launches (zeroing,
+// push, deposit) are captured once per buffer-parity pattern of the species
+// as a CUDA graph and replayed; the first cycle of a simulation runs directly
+// (it sets the kernels' attributes). Any capture failure falls back to
+// direct launches for the rest of the simulation's life.
+int run_cycle(spb_sim *s, const TileImpl *ti, cudaStream_t st) {
+  const bool use_graph = s->d.graph && !s->timing && !s->graph_failed && s->cycles_run > 0;
+  s->cycles_run++;
+  if (!use_graph) return ti->cycle(s, st);
+  if (!s->gstream) {
+    if (cudaStreamCreateWithFlags(&s->gstream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->gev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->gev[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      s->graph_failed = true;
+      return ti->cycle(s, st);
+    }
+  }
+  SPB_CUDA(cudaEventRecord(s->gev[0], st));
+  SPB_CUDA(cudaStreamWaitEvent(s->gstream, s->gev[0], 0));
+  const unsigned key = parity_key(s);
+  auto it = s->graphs.find(key);
+  if (it != s->graphs.end()) {
+    SPB_CUDA(cudaGraphLaunch(it->second, s->gstream));
+    for (auto &q : s->sp) q.cur = 1 - q.cur;
+    g_launches += 2;
+    s->launches += 2;
+  } else {
+    // capture (the captured call flips the buffer sets, as a direct launch does)
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    SPB_CUDA(cudaStreamBeginCapture(s->gstream, cudaStreamCaptureModeThreadLocal));
+    const int rc = ti->cycle(s, s->gstream);
+    const cudaError_t e1 = cudaStreamEndCapture(s->gstream, &g);
+    const cudaError_t e2 = (rc == SPB_OK && e1 == cudaSuccess)
+                               ? cudaGraphInstantiate(&ex, g, 0)
+                               : cudaErrorStreamCaptureInvalidated;
+    if (g) cudaGraphDestroy(g);
+    if (rc != SPB_OK || e1 != cudaSuccess || e2 != cudaSuccess) {
+      // undo the flip of the captured (never executed) call, then run directly
+      cudaGetLastError();
+      if (rc == SPB_OK)
+        for (auto &q : s->sp) q.cur = 1 - q.cur;
+      s->graph_failed = true;
+      return ti->cycle(s, st);
+    }
+    s->graphs[key] = ex;
+    SPB_CUDA(cudaGraphLaunch(ex, s->gstream));
+  }
+  SPB_CUDA(cudaEventRecord(s->gev[1], s->gstream));
+  SPB_CUDA(cudaStreamWaitEvent(st, s->gev[1], 0));
+  return SPB_OK;
+}
+
+}  // namespace
+
 extern "C" void spb_sim_destroy(spb_sim *s) {
   if (!s) return;
+  drop_graphs(s);
+  if (s->gstream) cudaStreamDestroy(s->gstream);
+  for (cudaEvent_t e : s->gev)
+    if (e) cudaEventDestroy(e);
   drain(s, nullptr, nullptr, nullptr, nullptr, nullptr);
   for (auto &q : s->sp) {
     free_buckets(q);
@@ -1782,6 +1863,7 @@ extern "C" int spb_sim_load_species(spb_sim *s, int species, const float *x, con
     }
   }
   const TileImpl *ti = find_tile(s->tile);
+  drop_graphs(s);   // the new layout's pointers differ from the captured ones
   const int rc = ti->build(s, s->sp[species], src, n, st);
   f.release(st);
   s->cycles_since_check = 0;
@@ -1792,6 +1874,7 @@ extern "C" int spb_sim_resort(spb_sim *s, void *stream) {
   if (!s) return fail(SPB_ERR_INVALID, "spb_sim_resort: null simulation");
   cudaStream_t st = (cudaStream_t)stream;
   const cudaEvent_t b = record_event(s, st);
+  drop_graphs(s);
   for (auto &q : s->sp)
     if (int rc = relayout(s, q, st)) return rc;
   const cudaEvent_t e = record_event(s, st);
@@ -1815,6 +1898,7 @@ extern "C" int spb_sim_cycle(spb_sim *s, int ncycles, void *stream) {
         const long o = spb_sim_overflow(s, i, stream);
         if (o < 0) return fail(SPB_ERR_CUDA, "spb_sim_cycle: overflow counter read failed");
         if (o > 0) {
+          drop_graphs(s);
           if (int rc = relayout(s, s->sp[i], st)) return rc;
           any = true;
         }
@@ -1828,7 +1912,7 @@ extern "C" int spb_sim_cycle(spb_sim *s, int ncycles, void *stream) {
       }
       s->cycles_since_check = 0;
     }
-    if (int rc = ti->cycle(s, st)) return rc;
+    if (int rc = run_cycle(s, ti, st)) return rc;
     s->cycles_since_check++;
   }
   return SPB_OK;
