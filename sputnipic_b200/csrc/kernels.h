@@ -11,6 +11,11 @@ int launch_pack_fields(const float *const f[6], float4 *eb4, float2 *eb2, long n
 int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F, float *x,
                        float *y, float *z, float *u, float *v, float *w, long n, int *err,
                        cudaStream_t s, int bc_variant = 0);
+// Whether mom[0..9] are equally spaced, as launch_plain_p2g and
+// launch_plain_mover_interp require.
+bool moments_strided(float *const mom[10]);
+// mom[m][i] += src[m * nodes + i].
+int launch_add_moments(const float *src, long nodes, float *const mom[10], cudaStream_t s);
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
                      const float *u, const float *v, const float *w, const float *q, long n,
                      float *const mom[10], int *err, cudaStream_t s);

@@ -17,6 +17,7 @@
 // 8-node gathers hit the packed fields, which stay L2-resident (14 MB at
 // 128x64x64 cells).
 #include "grid_ctx.h"
+#include "warp_sum.cuh"
 
 namespace spb {
 
@@ -28,6 +29,25 @@ constexpr int TPB = 256;
 struct Moments10 {
   float *m[10];
 };
+
+// The ten moment arrays of a deposit, equally spaced: moment m of node n is
+// base[m * stride + n] (one pointer, so the kernels index it arithmetically
+// instead of through a per-lane index into an array of pointers).
+struct MomStrided {
+  float *base;
+  long stride;
+};
+
+// Whether mom[0..9] are equally spaced (a [10][nodes] buffer is).
+bool as_strided(float *const mom[10], MomStrided &M) {
+  const long step = (long)((intptr_t)mom[1] - (intptr_t)mom[0]);
+  if (step % (long)sizeof(float)) return false;
+  for (int m = 2; m < 10; ++m)
+    if ((intptr_t)mom[m] - (intptr_t)mom[0] != (intptr_t)(m * step)) return false;
+  M.base = mom[0];
+  M.stride = step / (long)sizeof(float);
+  return true;
+}
 
 // The double product (x - start) * inv, limited to [-8, n + 8] so that the
 // int conversion below never overflows (NaN maps to -8). Exact for every
@@ -161,18 +181,26 @@ __device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
   }
 }
 
-// The 80 summands of one particle (src/Mover.cpp:399-570), value index
-// node*10 + moment with node = a*4 + b*2 + c for the node (ix-a, iy-b, iz-c).
-// Returns the linear index of node (ix, iy, iz).
-__device__ __forceinline__ long deposit_terms(const GeomDev &g, float x, float y,
-                                              float z, float u, float v, float w,
-                                              float q, float (&t)[80], int &bad) {
+// The 80 summands of one particle (src/Mover.cpp:399-570), each computed as
+// the reference does (weight = q * xi * eta * zeta * invVOL, then e.g.
+// (u * weight) * invVOL, no FMA), stored in the packed, lane-permuted layout of
+// warp_sum80: t[node * 5 + k] = (moment k, moment k + 5), node = a*4 + b*2 + c
+// with physical node (a ^ bit4(lane), b ^ bit3(lane), c ^ bit2(lane)); the
+// physical node (a, b, c) is (ix - a, iy - b, iz - c). Returns the linear index
+// of node (ix, iy, iz).
+__device__ __forceinline__ long deposit_terms(const GeomDev &g, float x, float y, float z,
+                                              float u, float v, float w, float q,
+                                              float2 (&t)[40], int lane, int &bad) {
   const int ix = clamp_cell(cell_floor(x, g.xStart, g.invdx, g.nxn), g.nxn, bad);
   const int iy = clamp_cell(cell_floor(y, g.yStart, g.invdy, g.nyn), g.nyn, bad);
   const int iz = clamp_cell(cell_floor(z, g.zStart, g.invdz, g.nzn), g.nzn, bad);
-  const float xi[2] = {x - __ldg(g.xn + ix - 1), __ldg(g.xn + ix) - x};
-  const float eta[2] = {y - __ldg(g.yn + iy - 1), __ldg(g.yn + iy) - y};
-  const float zeta[2] = {z - __ldg(g.zn + iz - 1), __ldg(g.zn + iz) - z};
+  const float xi0 = x - __ldg(g.xn + ix - 1), xi1 = __ldg(g.xn + ix) - x;
+  const float eta0 = y - __ldg(g.yn + iy - 1), eta1 = __ldg(g.yn + iy) - y;
+  const float zeta0 = z - __ldg(g.zn + iz - 1), zeta1 = __ldg(g.zn + iz) - z;
+  const bool pa = lane & 16, pb = lane & 8, pc = lane & 4;
+  const float xi[2] = {pa ? xi1 : xi0, pa ? xi0 : xi1};
+  const float eta[2] = {pb ? eta1 : eta0, pb ? eta0 : eta1};
+  const float zeta[2] = {pc ? zeta1 : zeta0, pc ? zeta0 : zeta1};
   const float uu = u * u, uv = u * v, uw = u * w, vv = v * v, vw = v * w, ww = w * w;
   const float inv = g.invVOL;
 #pragma unroll
@@ -182,77 +210,45 @@ __device__ __forceinline__ long deposit_terms(const GeomDev &g, float x, float y
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const float wgt = q * xi[a] * eta[b] * zeta[c] * inv;
-        float *o = t + (a * 4 + b * 2 + c) * 10;
-        o[0] = wgt * inv;
-        o[1] = (u * wgt) * inv;
-        o[2] = (v * wgt) * inv;
-        o[3] = (w * wgt) * inv;
-        o[4] = (uu * wgt) * inv;
-        o[5] = (uv * wgt) * inv;
-        o[6] = (uw * wgt) * inv;
-        o[7] = (vv * wgt) * inv;
-        o[8] = (vw * wgt) * inv;
-        o[9] = (ww * wgt) * inv;
+        float2 *o = t + (a * 4 + b * 2 + c) * 5;
+        o[0] = make_float2(wgt * inv, (uv * wgt) * inv);
+        o[1] = make_float2((u * wgt) * inv, (uw * wgt) * inv);
+        o[2] = make_float2((v * wgt) * inv, (vv * wgt) * inv);
+        o[3] = make_float2((w * wgt) * inv, (vw * wgt) * inv);
+        o[4] = make_float2((uu * wgt) * inv, (ww * wgt) * inv);
       }
   return ((long)ix * g.nyn + iy) * g.nzn + iz;
 }
 
-// Sums t[0..79] over the 32 lanes by recursive halving: at each xor-step
-// every lane keeps half of its values and receives the partner's partial sums
-// of that half (40+20+10+5+5 shuffles in all). Afterwards slot i (0..4) of
-// lane l holds the warp total of value index
-//   i + 5*b1 + 10*b2 + 20*b3 + 40*b4,  bK = bit K of l,
-// replicated in both lanes of each pair (l, l^1).
-__device__ __forceinline__ void warp_reduce80(float (&t)[80], int lane) {
-  {
-    const bool h = lane & 16;
-#pragma unroll
-    for (int i = 0; i < 40; ++i) {
-      const float send = h ? t[i] : t[i + 40];
-      const float keep = h ? t[i + 40] : t[i];
-      t[i] = keep + __shfl_xor_sync(FULL, send, 16);
-    }
-  }
-  {
-    const bool h = lane & 8;
-#pragma unroll
-    for (int i = 0; i < 20; ++i) {
-      const float send = h ? t[i] : t[i + 20];
-      const float keep = h ? t[i + 20] : t[i];
-      t[i] = keep + __shfl_xor_sync(FULL, send, 8);
-    }
-  }
-  {
-    const bool h = lane & 4;
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-      const float send = h ? t[i] : t[i + 10];
-      const float keep = h ? t[i + 10] : t[i];
-      t[i] = keep + __shfl_xor_sync(FULL, send, 4);
-    }
-  }
-  {
-    const bool h = lane & 2;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      const float send = h ? t[i] : t[i + 5];
-      const float keep = h ? t[i + 5] : t[i];
-      t[i] = keep + __shfl_xor_sync(FULL, send, 2);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 5; ++i) t[i] += __shfl_xor_sync(FULL, t[i], 1);
-}
+struct Particle {
+  float x, y, z, u, v, w, q;
+};
 
 // Adds one warp's deposits to the moments. For each of up to four distinct
-// cells among the warp's particles (cell-sorted particles give one or two),
-// the warp sums the members' 80 terms in registers and issues 80 atomics;
-// particles of further cells (unsorted input) issue 80 atomics each.
-__device__ __forceinline__ void deposit_warp(const GeomDev &g, const Moments10 &M,
-                                             bool valid, long key, float (&t)[80]) {
+// cells among the warp's particles (cell-ordered particles give one or two),
+// the members compute their terms and the warp sums them (warp_sum80) and
+// issues 80 atomics; lone particles of further cells (unordered input) issue
+// 80 atomics each. Terms are recomputed per round rather than kept, which
+// halves the registers. All 32 lanes call.
+__device__ __forceinline__ void deposit_warp(const GeomDev &g, const MomStrided &M, bool valid,
+                                             const Particle &p, int &bad) {
   const int lane = threadIdx.x & 31;
   const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
+  long key = 0;
+  if (valid) {
+    const int ix = clamp_cell(cell_floor(p.x, g.xStart, g.invdx, g.nxn), g.nxn, bad);
+    const int iy = clamp_cell(cell_floor(p.y, g.yStart, g.invdy, g.nyn), g.nyn, bad);
+    const int iz = clamp_cell(cell_floor(p.z, g.zStart, g.invdz, g.nzn), g.nzn, bad);
+    key = ((long)ix * g.nyn + iy) * g.nzn + iz;
+  }
+  // this lane's totals after warp_sum80: physical node (bit4, bit3, bit2),
+  // moments mbase + [lo, hi)
+  const int na = (lane >> 4) & 1, nb = (lane >> 3) & 1, nc = (lane >> 2) & 1;
+  const int mbase = 5 * ((lane >> 1) & 1);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+  int ignored = 0;
   unsigned remaining = __ballot_sync(FULL, valid);
+#pragma unroll 1
   for (int round = 0; round < 4 && remaining; ++round) {
     const int leader = __ffs(remaining) - 1;
     const long k = __shfl_sync(FULL, key, leader);
@@ -260,30 +256,34 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const Moments10 &
     const unsigned members = __ballot_sync(FULL, member);
     remaining &= ~members;
     if (__popc(members) < 2 && round > 0) continue;   // lone particle: direct atomics below
-    float r[80];
+    float2 t[40];
+    if (member) {
+      deposit_terms(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, ignored);
+    } else {
 #pragma unroll
-    for (int j = 0; j < 80; ++j) r[j] = member ? t[j] : 0.0f;
-    warp_reduce80(r, lane);
-    const int hi = 5 * ((lane >> 1) & 1) + 10 * ((lane >> 2) & 1) + 20 * ((lane >> 3) & 1) +
-                   40 * ((lane >> 4) & 1);
-    const int lo = (lane & 1) ? 3 : 0, cnt = (lane & 1) ? 2 : 3;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      if (i >= lo && i < lo + cnt) {
-        const int idx = hi + i;
-        const int node = idx / 10, m = idx % 10;
-        const long n = k - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);
-        atomicAdd(M.m[m] + n, r[i]);
-      }
+      for (int j = 0; j < 40; ++j) t[j] = make_float2(0.0f, 0.0f);
     }
+    float r[5];
+    warp_sum80(t, r, lane);
+    const long n = k - na * sx - nb * sy - nc;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+      if (i >= lo && i < hi) atomicAdd(M.base + (mbase + i) * M.stride + n, r[i]);
     if (member) valid = false;   // done
   }
   if (valid) {
+    float2 t[40];
+    deposit_terms(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, ignored);
+    const int pa = (lane >> 4) & 1, pb = (lane >> 3) & 1, pc = (lane >> 2) & 1;
 #pragma unroll
     for (int node = 0; node < 8; ++node) {
-      const long n = key - (node >> 2) * sx - ((node >> 1) & 1) * sy - (node & 1);
+      const int a = (node >> 2) ^ pa, b = ((node >> 1) & 1) ^ pb, c = (node & 1) ^ pc;
+      const long n = key - a * sx - b * sy - c;
 #pragma unroll
-      for (int m = 0; m < 10; ++m) atomicAdd(M.m[m] + n, t[node * 10 + m]);
+      for (int kk = 0; kk < 5; ++kk) {
+        atomicAdd(M.base + kk * M.stride + n, t[node * 5 + kk].x);
+        atomicAdd(M.base + (kk + 5) * M.stride + n, t[node * 5 + kk].y);
+      }
     }
   }
 }
@@ -330,31 +330,24 @@ __global__ void __launch_bounds__(TPB) k_plain_p2g(GeomDev g, const float *__res
                                                    const float *__restrict__ v,
                                                    const float *__restrict__ w,
                                                    const float *__restrict__ q, long n,
-                                                   Moments10 M, int *__restrict__ err) {
+                                                   MomStrided M, int *__restrict__ err) {
   const long i = blockIdx.x * (long)TPB + threadIdx.x;
   const bool valid = i < n;
-  float t[80];
-  long key = 0;
+  Particle p{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (valid) p = Particle{x[i], y[i], z[i], u[i], v[i], w[i], q[i]};
   int bad = 0;
-  if (valid) {
-    key = deposit_terms(g, x[i], y[i], z[i], u[i], v[i], w[i], q[i], t, bad);
-  } else {
-#pragma unroll
-    for (int j = 0; j < 80; ++j) t[j] = 0.0f;
-  }
-  deposit_warp(g, M, valid, key, t);
+  deposit_warp(g, M, valid, p, bad);
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
 __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
     GeomDev g, PushDev p, PackedFields F, float *__restrict__ x, float *__restrict__ y,
     float *__restrict__ z, float *__restrict__ u, float *__restrict__ v,
-    float *__restrict__ w, const float *__restrict__ q, long n, Moments10 M,
+    float *__restrict__ w, const float *__restrict__ q, long n, MomStrided M,
     int *__restrict__ err) {
   const long i = blockIdx.x * (long)TPB + threadIdx.x;
   const bool valid = i < n;
-  float t[80];
-  long key = 0;
+  Particle pt{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   int bad = 0;
   if (valid) {
     float px = x[i], py = y[i], pz = z[i], pu = u[i], pv = v[i], pw = w[i];
@@ -365,12 +358,9 @@ __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
     u[i] = pu;
     v[i] = pv;
     w[i] = pw;
-    key = deposit_terms(g, px, py, pz, pu, pv, pw, q[i], t, bad);
-  } else {
-#pragma unroll
-    for (int j = 0; j < 80; ++j) t[j] = 0.0f;
+    pt = Particle{px, py, pz, pu, pv, pw, q[i]};
   }
-  deposit_warp(g, M, valid, key, t);
+  deposit_warp(g, M, valid, pt, bad);
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
@@ -378,6 +368,16 @@ __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
 // the reference holds: periodic folds X, Y, Z, then non-periodic doubling X,
 // Y, Z. Thread t handles one (row, col) pair of the boundary planes of all
 // ten moments.
+// mom[m][i] += src[m * nodes + i] (moments deposited into a contiguous buffer)
+__global__ void __launch_bounds__(TPB) k_add_moments(const float *__restrict__ src, long nodes,
+                                                     Moments10 M) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nodes;
+       i += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int m = 0; m < 10; ++m) M.m[m][i] += src[m * nodes + i];
+  }
+}
+
 __global__ void __launch_bounds__(TPB) k_bc_fold(Moments10 M, int nxn, int nyn, int nzn,
                                                  int axis, int periodic) {
   int n1, n2;
@@ -445,12 +445,29 @@ int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F
   return SPB_OK;
 }
 
+bool moments_strided(float *const mom[10]) {
+  MomStrided M;
+  return as_strided(mom, M);
+}
+
+int launch_add_moments(const float *src, long nodes, float *const mom[10], cudaStream_t s) {
+  if (nodes <= 0) return SPB_OK;
+  Moments10 M;
+  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  k_add_moments<<<(unsigned)std::min<long>(ceil_div(nodes, TPB), 4096), TPB, 0, s>>>(src, nodes,
+                                                                                     M);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
                      const float *u, const float *v, const float *w, const float *q, long n,
                      float *const mom[10], int *err, cudaStream_t s) {
   if (n <= 0) return SPB_OK;
-  Moments10 M;
-  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  MomStrided M;
+  if (!as_strided(mom, M))
+    return fail(SPB_ERR_UNSUPPORTED, "the ten moment arrays must be equally spaced");
   k_plain_p2g<<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, M, err);
   SPB_CUDA(cudaGetLastError());
   g_launches++;
@@ -462,8 +479,9 @@ int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFi
                               const float *q, long n, float *const mom[10], int *err,
                               cudaStream_t s) {
   if (n <= 0) return SPB_OK;
-  Moments10 M;
-  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  MomStrided M;
+  if (!as_strided(mom, M))
+    return fail(SPB_ERR_UNSUPPORTED, "the ten moment arrays must be equally spaced");
   k_plain_mover_interp<<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n, M, err);
   SPB_CUDA(cudaGetLastError());
   g_launches++;

@@ -30,6 +30,7 @@
 #include "grid_ctx.h"
 #include "kernels.h"
 #include "sim_kernels.cuh"
+#include "warp_sum.cuh"
 
 namespace spb {
 namespace {
@@ -331,34 +332,6 @@ __device__ __forceinline__ void add_terms(float2 (&acc)[40], float q, float ox, 
       acc[(ab * 2 + 1) * 5 + k] = __ffma2_rn(W12, mf[k], acc[(ab * 2 + 1) * 5 + k]);
     }
   }
-}
-
-__device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
-  return make_float2(__shfl_xor_sync(FULL, v.x, m), __shfl_xor_sync(FULL, v.y, m));
-}
-
-// Sums the packed accumulators over the warp. Lanes hold their terms with
-// the x/y/z node halves swapped by lane bits 4/3/2, so the first three
-// halving steps need no selects: every lane keeps its lower half and
-// receives its partner's upper half. Afterwards lane l holds in r[0..4] the
-// totals of node (a, b, c) = (bit4, bit3, bit2) of l, moments
-// 5*bit1(l) .. 5*bit1(l)+4 (reference order).
-__device__ __forceinline__ void warp_sum80(float2 (&acc)[40], float (&r)[5], int lane) {
-#pragma unroll
-  for (int i = 0; i < 20; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 20], 16));
-#pragma unroll
-  for (int i = 0; i < 10; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 10], 8));
-#pragma unroll
-  for (int i = 0; i < 5; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 5], 4));
-  const bool h = lane & 2;
-#pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    const float send = h ? acc[k].x : acc[k].y;
-    const float keep = h ? acc[k].y : acc[k].x;
-    r[k] = keep + __shfl_xor_sync(FULL, send, 2);
-  }
-#pragma unroll
-  for (int k = 0; k < 5; ++k) r[k] += __shfl_xor_sync(FULL, r[k], 1);
 }
 
 // Stores one pushed record in slot `slot` of the bucket [dbase, dend) of cell

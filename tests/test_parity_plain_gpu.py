@@ -324,3 +324,33 @@ def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64):
     mom = [np.zeros(wl.nodes, np.float32) for _ in range(10)]
     orc32.interp_p2g(setup, ref, mom)
     check_moments(np.stack(dropin.moments(ids)), np.stack(mom), abs_moments(orc64, setup, wl, ref))
+
+
+def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64):
+    """spb_grid_p2g into ten separately allocated moment arrays (not equally
+    spaced: the deposit goes through a contiguous scratch and is added into
+    them) that already hold values: the result is those values plus the
+    deposit, within the reordering bound."""
+    torch = cuda
+    from sputnipic_b200.device import GridContext
+    wl = W.small_gem()
+    fields = W.gem_fields(wl)
+    setup = oracle.setup_from(wl)
+    ctx = GridContext(wl)
+    ctx.set_fields([torch.from_numpy(f).cuda() for f in fields])
+    host = W.gem_particles(wl, 1)
+    dev = {k: torch.from_numpy(host[k]).cuda() for k in "xyzuvwq"}
+    # slices of one buffer at irregular offsets: not equally spaced
+    offs = [m * wl.nodes + 4 * m * m for m in range(10)]
+    buf = torch.full((offs[-1] + wl.nodes,), 0.25, device="cuda")
+    mom = [buf[o:o + wl.nodes] for o in offs]
+    steps = {mom[m + 1].data_ptr() - mom[m].data_ptr() for m in range(9)}
+    assert len(steps) > 1
+    ctx.p2g(dev, mom)
+    assert ctx.check() == 0
+    m32 = [np.zeros(wl.nodes, np.float32) for _ in range(10)]
+    orc32.interp_p2g(setup, host, m32)
+    absm = abs_moments(orc64, setup, wl, host)
+    got = np.stack([m.cpu().numpy() for m in mom]).astype(np.float64) - 0.25
+    check_moments(got, np.stack(m32), absm + 0.25)
+    ctx.close()
