@@ -275,6 +275,77 @@ int spb_sim_kernel_timing(spb_sim *sim, double *push_ms, double *deposit_ms,
                           int *ncycles, double *relayout_ms, int *nrelayouts);
 
 /* ---------------------------------------------------------------------------
+ * Serving form: a stream of independent frozen-field test-particle jobs (the
+ * reference's particle tracking use, src/Tracking.cpp), each with its own
+ * grid, fields, species and cycle count. No counterpart in the reference's
+ * hot path, which runs one simulation.
+ *
+ * Jobs wait in a queue until their estimated HBM footprint fits the engine's
+ * budget, are then admitted (fields and particles uploaded into device-
+ * resident precision-form state), and run together: every spb_serve_step runs
+ * one cycle of every admitted job in one launch each of zeroing, push and
+ * deposit (the jobs' tiles concatenated), so jobs that arrive while others run
+ * join the next step. A job finishes after its cycle count; its results stay
+ * on the device until fetched and released. One host thread drives an engine;
+ * calls must not overlap. All jobs of an engine use its tile shape, so their
+ * cells per axis must be multiples of it.
+ * ------------------------------------------------------------------------- */
+typedef struct spb_serve spb_serve;
+
+typedef struct spb_serve_desc {
+  int tile[3];              /* tile shape of every job (0,0,0: 4x4x4) */
+  long long hbm_budget;     /* bytes the admitted jobs may hold (0: 90% of the
+                               free device memory at creation) */
+  int max_jobs;             /* jobs per launch (0 or above 64: 64) */
+  int check_every;          /* steps between overflow checks (0: 4) */
+} spb_serve_desc;
+
+typedef struct spb_job_desc {
+  int nxc, nyc, nzc;        /* active cells */
+  double Lx, Ly, Lz;
+  double dt, c;             /* param->dt, param->c */
+  int niter;                /* NiterMover */
+  int periodic[3];          /* param->PERIODICX/Y/Z */
+  int ns;                   /* species, 1..8 */
+  double qom[SPB_SIM_MAX_SPECIES];
+  int ncycles;              /* cycles to run (>= 1) */
+} spb_job_desc;
+
+enum { SPB_JOB_PENDING = 0, SPB_JOB_ACTIVE = 1, SPB_JOB_DONE = 2, SPB_JOB_FAILED = 3 };
+
+int spb_serve_create(const spb_serve_desc *desc, spb_serve **out);
+void spb_serve_destroy(spb_serve *srv);
+/* Queues a job. fields: Ex, Ey, Ez, Bxn, Byn, Bzn (nodes floats each);
+ * parts: ns x 7 arrays x, y, z, u, v, w, q (positions in [0, L]); counts[ns].
+ * The arrays stay the caller's and must stay valid until the job leaves the
+ * queue (status not PENDING). Returns the job id (>= 0) or -status. */
+long spb_serve_submit(spb_serve *srv, const spb_job_desc *job, const float *const fields[6],
+                      const float *const *parts, const long *counts, int on_device);
+/* Admits the queued jobs that fit (in order of arrival), runs one cycle of
+ * every admitted job, retires the jobs that reached their cycle count, and
+ * synchronises. Returns the number of jobs still admitted, or -status. */
+int spb_serve_step(spb_serve *srv);
+/* SPB_JOB_*, or -1 for an unknown id. */
+int spb_serve_status(const spb_serve *srv, long id);
+/* Status code of a failed job (why it failed). */
+int spb_serve_error(const spb_serve *srv, long id);
+/* Results of a finished job: particles of one species (as spb_sim_particles,
+ * any pointer may be NULL) and its raw FP64 moments of the last cycle
+ * (10 x nodes, NULL to skip). Synchronises. */
+int spb_serve_result(spb_serve *srv, long id, int species, float *x, float *y, float *z,
+                     float *u, float *v, float *w, float *q, double *moments,
+                     int on_device);
+/* Seconds since the engine's creation at which the job was submitted,
+ * admitted and finished (negative where not yet). */
+int spb_serve_times(const spb_serve *srv, long id, double t[3]);
+/* Frees a finished or failed job. */
+int spb_serve_release(spb_serve *srv, long id);
+/* Jobs queued, admitted and finished (not yet released); bytes held by the
+ * admitted and finished jobs, and the budget. */
+int spb_serve_counts(const spb_serve *srv, int *pending, int *active, int *done,
+                     long long *bytes_held, long long *budget);
+
+/* ---------------------------------------------------------------------------
  * Particle load + cell sort that allocates nothing. No counterpart in the
  * reference: it is the conversion and counting sort behind
  * spb_sim_load_species, for callers that cannot call cudaMalloc where they

@@ -139,6 +139,20 @@ class SimDesc(ctypes.Structure):
                 ("variant", c_int), ("bucket_slots", c_int), ("graph", c_int)]
 
 
+class ServeDesc(ctypes.Structure):
+    """spb_serve_desc of include/sputnipic_b200.h."""
+    _fields_ = [("tile", c_int * 3), ("hbm_budget", ctypes.c_longlong), ("max_jobs", c_int),
+                ("check_every", c_int)]
+
+
+class JobDesc(ctypes.Structure):
+    """spb_job_desc of include/sputnipic_b200.h."""
+    _fields_ = [("nxc", c_int), ("nyc", c_int), ("nzc", c_int),
+                ("Lx", c_double), ("Ly", c_double), ("Lz", c_double),
+                ("dt", c_double), ("c", c_double), ("niter", c_int), ("periodic", c_int * 3),
+                ("ns", c_int), ("qom", c_double * 8), ("ncycles", c_int)]
+
+
 def ctypes_layout() -> dict:
     """Offsets of the ctypes mirrors, keyed like spb_abi_layout_json."""
     out = {}
@@ -225,6 +239,17 @@ def load():
            [P, R(c_double), R(c_double), R(c_int), R(c_double), R(c_int)])
     _proto(lib, "spb_sim_bucket_slots", c_long, [P, c_int])
     _proto(lib, "spb_sim_overflow", c_long, [P, c_int, P])
+    _proto(lib, "spb_serve_create", c_int, [R(ServeDesc), R(P)])
+    _proto(lib, "spb_serve_destroy", None, [P])
+    _proto(lib, "spb_serve_submit", c_long, [P, R(JobDesc), P, P, P, c_int])
+    _proto(lib, "spb_serve_step", c_int, [P])
+    _proto(lib, "spb_serve_status", c_int, [P, c_long])
+    _proto(lib, "spb_serve_error", c_int, [P, c_long])
+    _proto(lib, "spb_serve_result", c_int, [P, c_long, c_int] + [P] * 8 + [c_int])
+    _proto(lib, "spb_serve_times", c_int, [P, c_long, P])
+    _proto(lib, "spb_serve_release", c_int, [P, c_long])
+    _proto(lib, "spb_serve_counts", c_int,
+           [P, R(c_int), R(c_int), R(c_int), R(ctypes.c_longlong), R(ctypes.c_longlong)])
     _lib = lib
     return lib
 

@@ -1,0 +1,318 @@
+// Serving form (spb_serve_*): a stream of independent frozen-field test-
+// particle jobs, each a precision-form simulation of its own grid, admitted by
+// free HBM and stepped together in one launch per kernel (spb::launch_jobs).
+//
+// Scheduling. Jobs queue in order of arrival. A step first admits queued jobs
+// while the next one's estimated footprint fits the budget and the launch has
+// room (first come, first served: a large job at the head waits rather than
+// being overtaken), then runs one cycle of every admitted job, then retires
+// the jobs that reached their cycle count. A job that can never fit (larger
+// than the whole budget) fails with SPB_ERR_CAPACITY instead of blocking.
+#include <chrono>
+#include <deque>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "grid_ctx.h"
+#include "sim_host.h"
+
+using namespace spb;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServeJob {
+  long id = 0;
+  spb_job_desc d{};
+  const float *fields[6] = {};
+  std::vector<const float *> parts;   // ns x 7
+  std::vector<long> counts;
+  int on_device = 0;
+  long long bytes = 0;                // estimated footprint, held while admitted
+  spb_sim *sim = nullptr;
+  int cycles = 0;
+  int state = SPB_JOB_PENDING;
+  int error = SPB_OK;
+  double t[3] = {-1.0, -1.0, -1.0};   // submitted, admitted, finished
+  ~ServeJob() {
+    if (sim) spb_sim_destroy(sim);
+  }
+};
+
+// Estimated device bytes of a job's simulation, from its grid and particle
+// counts: two bucket sets of 32-byte records at count + slack, overflow lists,
+// counters and layouts, FP64 moments, fields and scratch, and the temporary
+// flat arrays of a host upload.
+long long footprint(const spb_job_desc &d, const long *counts, int on_device) {
+  const long long ncells = (long long)d.nxc * d.nyc * d.nzc;
+  const long long nodes = (long long)(d.nxc + 3) * (d.nyc + 3) * (d.nzc + 3);
+  long long b = nodes * 32 + nodes * 24 + ncells * 20 + (1 << 20);
+  long long nmax = 0;
+  for (int s = 0; s < d.ns; ++s) {
+    const long long n = counts[s];
+    nmax = std::max(nmax, n);
+    const long long slots = n + n / 4 + 20 * ncells;
+    const long long ocap = std::max<long long>(65536, n / 32);
+    b += 2 * (slots + slots / 16) * 32 + 2 * ocap * 36 + 2 * ncells * 4 + 2 * (ncells + 1) * 8 +
+         nodes * 80;
+  }
+  if (!on_device) b += nmax * 28;
+  return b;
+}
+
+double seconds_since(Clock::time_point t0) {
+  return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct spb_serve {
+  spb_serve_desc d{};
+  int device = 0;
+  cudaStream_t st = nullptr;
+  JobBuffers buf;
+  long long budget = 0, used = 0;
+  long next_id = 0;
+  long steps = 0;
+  Clock::time_point t0;
+  std::deque<ServeJob *> pending;
+  std::vector<ServeJob *> active;
+  std::map<long, std::unique_ptr<ServeJob>> jobs;   // every job not yet released
+};
+
+namespace {
+
+ServeJob *find_job(const spb_serve *s, long id) {
+  auto it = s->jobs.find(id);
+  return it == s->jobs.end() ? nullptr : it->second.get();
+}
+
+void fail_job(spb_serve *s, ServeJob *j, int status) {
+  if (j->sim) {
+    spb_sim_destroy(j->sim);
+    j->sim = nullptr;
+  }
+  if (j->state == SPB_JOB_ACTIVE) s->used -= j->bytes;
+  j->state = SPB_JOB_FAILED;
+  j->error = status;
+  j->t[2] = seconds_since(s->t0);
+}
+
+// Creates the job's simulation and uploads its fields and particles.
+int admit(spb_serve *s, ServeJob *j) {
+  spb_sim_desc sd{};
+  sd.nxc = j->d.nxc;
+  sd.nyc = j->d.nyc;
+  sd.nzc = j->d.nzc;
+  sd.Lx = j->d.Lx;
+  sd.Ly = j->d.Ly;
+  sd.Lz = j->d.Lz;
+  sd.dt = j->d.dt;
+  sd.c = j->d.c;
+  sd.niter = j->d.niter;
+  for (int a = 0; a < 3; ++a) {
+    sd.periodic[a] = j->d.periodic[a];
+    sd.tile[a] = s->d.tile[a];
+  }
+  sd.ns = j->d.ns;
+  for (int i = 0; i < j->d.ns; ++i) sd.qom[i] = j->d.qom[i];
+  sd.resort_every = 1 << 30;   // the engine checks overflow lists itself
+  if (int rc = spb_sim_create(&sd, &j->sim)) return rc;
+  if (int rc = spb_sim_set_fields(j->sim, j->fields, j->on_device, s->st)) return rc;
+  for (int i = 0; i < j->d.ns; ++i) {
+    const float *const *p = j->parts.data() + 7 * i;
+    if (int rc = spb_sim_load_species(j->sim, i, p[0], p[1], p[2], p[3], p[4], p[5], p[6],
+                                      j->counts[i], j->on_device, s->st))
+      return rc;
+  }
+  return SPB_OK;
+}
+
+}  // namespace
+
+extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
+  if (!out) return fail(SPB_ERR_INVALID, "spb_serve_create: null argument");
+  *out = nullptr;
+  spb_serve_desc d = desc ? *desc : spb_serve_desc{};
+  if (!d.tile[0] || !d.tile[1] || !d.tile[2]) d.tile[0] = d.tile[1] = d.tile[2] = 4;
+  if (!spb_sim_tile_supported(d.tile[0], d.tile[1], d.tile[2]))
+    return fail(SPB_ERR_UNSUPPORTED, "spb_serve_create: tile shape not instantiated");
+  if (d.max_jobs <= 0 || d.max_jobs > SERVE_MAX_JOBS) d.max_jobs = SERVE_MAX_JOBS;
+  if (d.check_every <= 0) d.check_every = 4;
+  if (d.hbm_budget < 0) return fail(SPB_ERR_INVALID, "spb_serve_create: negative budget");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(SPB_ERR_NO_DEVICE, "no CUDA device");
+  }
+  auto s = std::make_unique<spb_serve>();
+  s->d = d;
+  SPB_CUDA(cudaGetDevice(&s->device));
+  SPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  if (d.hbm_budget > 0) {
+    s->budget = d.hbm_budget;
+  } else {
+    size_t free_b = 0, total_b = 0;
+    SPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    s->budget = (long long)(0.9 * (double)free_b);
+  }
+  s->t0 = Clock::now();
+  *out = s.release();
+  return SPB_OK;
+}
+
+extern "C" void spb_serve_destroy(spb_serve *s) {
+  if (!s) return;
+  if (s->st) cudaStreamSynchronize(s->st);
+  s->jobs.clear();
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+extern "C" long spb_serve_submit(spb_serve *s, const spb_job_desc *job,
+                                 const float *const fields[6], const float *const *parts,
+                                 const long *counts, int on_device) {
+  if (!s || !job || !fields || !parts || !counts)
+    return -fail(SPB_ERR_INVALID, "spb_serve_submit: null argument");
+  if (job->ns < 1 || job->ns > SPB_SIM_MAX_SPECIES || job->ncycles < 1)
+    return -fail(SPB_ERR_INVALID, "spb_serve_submit: 1..8 species and >= 1 cycle");
+  if (job->nxc % s->d.tile[0] || job->nyc % s->d.tile[1] || job->nzc % s->d.tile[2])
+    return -fail(SPB_ERR_UNSUPPORTED, "spb_serve_submit: cells per axis must be multiples of "
+                                      "the engine's tile shape");
+  for (int f = 0; f < 6; ++f)
+    if (!fields[f]) return -fail(SPB_ERR_INVALID, "spb_serve_submit: null field array");
+  for (int i = 0; i < job->ns; ++i) {
+    if (counts[i] < 0) return -fail(SPB_ERR_INVALID, "spb_serve_submit: negative count");
+    for (int a = 0; a < 7; ++a)
+      if (counts[i] > 0 && !parts[7 * i + a])
+        return -fail(SPB_ERR_INVALID, "spb_serve_submit: null particle array");
+  }
+  auto j = std::make_unique<ServeJob>();
+  j->id = s->next_id++;
+  j->d = *job;
+  for (int f = 0; f < 6; ++f) j->fields[f] = fields[f];
+  j->parts.assign(parts, parts + 7 * job->ns);
+  j->counts.assign(counts, counts + job->ns);
+  j->on_device = on_device;
+  j->bytes = footprint(*job, counts, on_device);
+  j->t[0] = seconds_since(s->t0);
+  ServeJob *raw = j.get();
+  s->jobs.emplace(raw->id, std::move(j));
+  s->pending.push_back(raw);
+  return raw->id;
+}
+
+extern "C" int spb_serve_step(spb_serve *s) {
+  if (!s) return -fail(SPB_ERR_INVALID, "spb_serve_step: null engine");
+  SPB_CUDA(cudaSetDevice(s->device));
+  // admit in order of arrival while the head fits
+  while (!s->pending.empty() && (int)s->active.size() < s->d.max_jobs) {
+    ServeJob *j = s->pending.front();
+    if (j->bytes > s->budget) {   // can never fit: fail it rather than block the queue
+      s->pending.pop_front();
+      fail_job(s, j, fail(SPB_ERR_CAPACITY, "job larger than the engine's HBM budget"));
+      continue;
+    }
+    if (s->used + j->bytes > s->budget) break;
+    s->pending.pop_front();
+    j->state = SPB_JOB_ACTIVE;
+    s->used += j->bytes;
+    j->t[1] = seconds_since(s->t0);
+    if (int rc = admit(s, j)) {
+      fail_job(s, j, rc);
+      continue;
+    }
+    s->active.push_back(j);
+  }
+  if (s->active.empty()) return 0;
+  // overflow lists in use: re-lay out those jobs (synchronises)
+  if (s->steps > 0 && s->steps % s->d.check_every == 0)
+    for (ServeJob *j : s->active)
+      for (int i = 0; i < j->d.ns; ++i)
+        if (spb_sim_overflow(j->sim, i, s->st) > 0) {
+          if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
+          break;
+        }
+  std::vector<spb_sim *> sims;
+  sims.reserve(s->active.size());
+  for (ServeJob *j : s->active) sims.push_back(j->sim);
+  if (int rc = launch_jobs(sims.data(), (int)sims.size(), s->buf, s->st)) return -rc;
+  SPB_CUDA(cudaStreamSynchronize(s->st));
+  s->steps++;
+  // retire the jobs that reached their cycle count
+  std::vector<ServeJob *> still;
+  for (ServeJob *j : s->active) {
+    if (++j->cycles < j->d.ncycles) {
+      still.push_back(j);
+      continue;
+    }
+    const int rc = spb_sim_check(j->sim, s->st);
+    j->t[2] = seconds_since(s->t0);
+    if (rc) {
+      fail_job(s, j, rc);
+    } else {
+      j->state = SPB_JOB_DONE;
+    }
+  }
+  s->active.swap(still);
+  return (int)s->active.size();
+}
+
+extern "C" int spb_serve_status(const spb_serve *s, long id) {
+  const ServeJob *j = s ? find_job(s, id) : nullptr;
+  return j ? j->state : -1;
+}
+
+extern "C" int spb_serve_error(const spb_serve *s, long id) {
+  const ServeJob *j = s ? find_job(s, id) : nullptr;
+  return j ? j->error : SPB_ERR_INVALID;
+}
+
+extern "C" int spb_serve_result(spb_serve *s, long id, int species, float *x, float *y, float *z,
+                                float *u, float *v, float *w, float *q, double *moments,
+                                int on_device) {
+  ServeJob *j = s ? find_job(s, id) : nullptr;
+  if (!j || j->state != SPB_JOB_DONE)
+    return fail(SPB_ERR_INVALID, "spb_serve_result: no finished job with this id");
+  if (species < 0 || species >= j->d.ns)
+    return fail(SPB_ERR_INVALID, "spb_serve_result: bad species");
+  if (x && y && z && u && v && w)
+    if (int rc = spb_sim_particles(j->sim, species, x, y, z, u, v, w, q, on_device, s->st))
+      return rc;
+  if (moments)
+    if (int rc = spb_sim_moments(j->sim, species, moments, on_device, s->st)) return rc;
+  SPB_CUDA(cudaStreamSynchronize(s->st));
+  return SPB_OK;
+}
+
+extern "C" int spb_serve_times(const spb_serve *s, long id, double t[3]) {
+  const ServeJob *j = s ? find_job(s, id) : nullptr;
+  if (!j || !t) return fail(SPB_ERR_INVALID, "spb_serve_times: unknown job");
+  for (int i = 0; i < 3; ++i) t[i] = j->t[i];
+  return SPB_OK;
+}
+
+extern "C" int spb_serve_release(spb_serve *s, long id) {
+  ServeJob *j = s ? find_job(s, id) : nullptr;
+  if (!j || (j->state != SPB_JOB_DONE && j->state != SPB_JOB_FAILED))
+    return fail(SPB_ERR_INVALID, "spb_serve_release: no finished job with this id");
+  if (j->state == SPB_JOB_DONE) s->used -= j->bytes;
+  s->jobs.erase(id);
+  return SPB_OK;
+}
+
+extern "C" int spb_serve_counts(const spb_serve *s, int *pending, int *active, int *done,
+                                long long *bytes_held, long long *budget) {
+  if (!s) return fail(SPB_ERR_INVALID, "spb_serve_counts: null engine");
+  int nd = 0;
+  for (const auto &kv : s->jobs)
+    if (kv.second->state == SPB_JOB_DONE || kv.second->state == SPB_JOB_FAILED) ++nd;
+  if (pending) *pending = (int)s->pending.size();
+  if (active) *active = (int)s->active.size();
+  if (done) *done = nd;
+  if (bytes_held) *bytes_held = s->used;
+  if (budget) *budget = s->budget;
+  return SPB_OK;
+}

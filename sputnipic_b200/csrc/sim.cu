@@ -25,10 +25,12 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "grid_ctx.h"
 #include "kernels.h"
+#include "sim_host.h"
 #include "sim_kernels.cuh"
 #include "warp_sum.cuh"
 
@@ -401,175 +403,159 @@ __device__ __forceinline__ void issue_slot(const SpeciesDev &S, Pending &p, floa
 
 constexpr int PCH = 32;    // records per bulk chunk of the push (1 KB)
 
-// The mover (mover_PC, src/Mover.cpp:4-162) for every species. Persistent
-// CTAs walk tiles of TX x TY x TZ cells; one thread stages the tile's E/B
-// nodes plus a one-cell halo into shared memory with a TMA tensor copy (two
-// stages: the next tile's copy overlaps this tile's work). Warps walk the
-// tile's cells, one particle per lane, with the cells' records streamed
-// through two shared-memory chunk buffers per warp by bulk copies; the
-// gathers of the NiterMover iterations read the staged tile (or L2 past the
-// halo), and every pushed particle is written into the bucket of its new
-// cell. Afterwards the CTAs push the overflow entries (gathers from L2).
-template <int TX, int TY, int TZ, int MINB>
-__global__ void __launch_bounds__(SIM_TPB, MINB)
-    k_push(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P) {
+// Independent jobs (own grid, fields, species and buckets; one tile shape)
+// processed by one launch: the launch walks the concatenation of the jobs'
+// tiles, and a CTA reads a tile's job from the prefix table.
+struct JobTable {
+  int njobs, total_tiles;
+  const int *tile_base;          // [njobs + 1] first launch-wide tile of each job
+  const CycleParams *params;     // [njobs]
+};
+
+// The jobs' field maps travel as a kernel parameter, like the single job's.
+struct JobMaps {
+  CUtensorMap m[SERVE_MAX_JOBS];
+};
+struct NoMaps {
+  int unused;
+};
+template <bool MULTI>
+using MapsOf = typename std::conditional<MULTI, JobMaps, NoMaps>::type;
+
+// The job of launch-wide tile t: the largest j with tile_base[j] <= t.
+__device__ __forceinline__ int job_of(const JobTable &J, int t) {
+  int lo = 0, hi = J.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (J.tile_base[mid] <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Copies one job's parameters into shared memory (all threads of the CTA call).
+__device__ __forceinline__ void load_params(CycleParams *dst, const CycleParams *src) {
+  static_assert(sizeof(CycleParams) % 8 == 0, "copied in 8-byte words");
+  const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(CycleParams) / 8); i += blockDim.x) d[i] = s[i];
+  __syncthreads();
+}
+
+// Per-warp state of the push that lives across tiles and jobs.
+struct PushWarp {
+  float4 *wrec;        // staged records of the pending slot
+  float4 *buf;         // two record chunk buffers
+  uint64_t *cbar;      // their barriers
+  unsigned phase = 0, inflight = 0;   // per buffer: next parity, copy issued
+  bool dead = false;   // a bounded wait for a record chunk ran out
+  int bad = 0, lost = 0;
+};
+
+// All species of one tile (tile-local index `tile` of the job P) on the
+// staged fields sF. All threads call.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const float *sF,
+                                          PushWarp &W) {
   using T = Tile<TX, TY, TZ>;
   constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
-  static_assert(T::TC % SIM_NW == 0 && NC <= 32, "cells per warp must fit a warp's lanes");
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
-  float4 *sRec = reinterpret_cast<float4 *>(sF0 + 2 * T::SF);       // NW x 64 staged records
-  float4 *sBuf = sRec + SIM_NW * 64;                                // NW x 2 x PCH records
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sBuf + SIM_NW * 2 * PCH * 2);  // 2 + 2 NW
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float4 *wrec = sRec + warp * 64;   // this warp's staged records
-  float4 *buf = sBuf + warp * 2 * PCH * 2;
-  uint64_t *cbar = bar + 2 + warp * 2;
-  if (smem_addr(sF0) & 127u) {   // TMA destinations need 128-byte alignment
-    if (tid == 0) atomicOr(P.err, ERRBIT_SMEM_ALIGN);
-    return;
-  }
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    mbar_init(bar + 1, 1);
-  }
-  if (lane == 0) {
-    mbar_init(cbar, 1);
-    mbar_init(cbar + 1, 1);
-  }
-  __syncthreads();
-
-  const int ntiles = P.ntx * P.nty * P.ntz;
-  const unsigned box_bytes = (unsigned)(T::BN * 8 * sizeof(float));
-  auto issue = [&](int t, int stage) {
-    const int z = t % P.ntz, y = (t / P.ntz) % P.nty, x = t / (P.ntz * P.nty);
-    fence_proxy_async();
-    mbar_expect_tx(bar + stage, box_bytes);
-    // box origin: node c0 on every axis (the lower node of halo cell c0-1)
-    tma_load_4d(sF0 + stage * T::SF, &fmap, 0, z * TZ, y * TY, x * TX, bar + stage);
-  };
-  if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
-  int bad = 0, lost = 0, it = 0;
-  unsigned phase = 0, inflight = 0;   // record chunks, per buffer: next parity, copy issued
-  bool dead = false;                  // a bounded wait for a record chunk ran out
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int stage = it & 1;
-    // prefetch the next tile's fields into the other stage (read by the
-    // previous tile, which every thread finished before the last barrier)
-    if (tid == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
-    const bool arrived = mbar_wait_bounded(bar + stage, (it >> 1) & 1);
-    if (__syncthreads_or(!arrived)) {
-      // the staged fields never arrived (for some thread): the whole CTA
-      // reports, waits once more for its copies in flight, and gives up
-      if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
-      mbar_wait_bounded(bar + stage, (it >> 1) & 1);
-      mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
-      return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
+  const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
+  for (int s = 0; s < P.ns; ++s) {
+    const SpeciesDev &S = P.sp[s];
+    // lane j < NC holds bucket start, capacity and particle count of the
+    // warp's j-th cell (tile-local cell warp + j * NW)
+    long long cb = 0;
+    int ccap = 0, cc = 0;
+    if (lane < NC) {
+      const int key = tile * T::TC + warp + lane * SIM_NW;
+      cb = S.base[key];
+      ccap = (int)(S.base[key + 1] - cb);
+      cc = min(S.cin[key], ccap);
     }
-    const float *sF = sF0 + stage * T::SF;
-    const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
-    const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
-
-    for (int s = 0; s < P.ns; ++s) {
-      const SpeciesDev &S = P.sp[s];
-      // lane j < NC holds bucket start, capacity and particle count of the
-      // warp's j-th cell (tile-local cell warp + j * NW)
-      long long cb = 0;
-      int ccap = 0, cc = 0;
-      if (lane < NC) {
-        const int key = tile * T::TC + warp + lane * SIM_NW;
-        cb = S.base[key];
-        ccap = (int)(S.base[key + 1] - cb);
-        cc = min(S.cin[key], ccap);
+    int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
+    auto issue_next = [&]() {         // all lanes call; lane 0 copies
+      while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
+        ++pj;
+        poff = 0;
       }
-      int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
-      auto issue_next = [&]() {         // all lanes call; lane 0 copies
-        while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
-          ++pj;
-          poff = 0;
+      if (pj < NC && !W.dead) {
+        const int len = min(PCH, __shfl_sync(FULL, cc, pj) - poff);
+        const long long b0 = __shfl_sync(FULL, cb, pj);
+        if (lane == 0) {
+          fence_proxy_async();
+          mbar_expect_tx(W.cbar + nbuf, (unsigned)len * 32u);
+          bulk_load(W.buf + nbuf * PCH * 2, S.rin + 2 * (b0 + poff), (unsigned)len * 32u,
+                    W.cbar + nbuf);
         }
-        if (pj < NC && !dead) {
-          const int len = min(PCH, __shfl_sync(FULL, cc, pj) - poff);
-          const long long b0 = __shfl_sync(FULL, cb, pj);
-          if (lane == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(cbar + nbuf, (unsigned)len * 32u);
-            bulk_load(buf + nbuf * PCH * 2, S.rin + 2 * (b0 + poff), (unsigned)len * 32u,
-                      cbar + nbuf);
-          }
-          inflight |= 1u << nbuf;
-          poff += len;
-          nbuf ^= 1;
-        }
-      };
-      Pending pend;
-      pend.valid = false;
-      pend.sbase0 = 0;
-      issue_next();
-      int cbuf = 0;
-      for (int j = 0; j < NC; ++j) {
-        const int cnt = __shfl_sync(FULL, cc, j);
-        if (cnt <= 0 || dead) continue;
-        const long long b0 = __shfl_sync(FULL, cb, j);
-        const long long b1 = b0 + __shfl_sync(FULL, ccap, j);
-        const int lc = warp + j * SIM_NW;
-        const int key = tile * T::TC + lc;
-        const int cx0 = c0x + lc / (TY * TZ), cy0 = c0y + (lc / TZ) % TY, cz0 = c0z + lc % TZ;
-#pragma unroll 1
-        for (int off = 0; off < cnt; off += PCH) {
-          issue_next();   // the following chunk streams in while this one is pushed
-          const bool ok = mbar_wait_bounded(cbar + cbuf, (phase >> cbuf) & 1u);
-          if (!__all_sync(FULL, ok)) {
-            dead = true;
-            break;
-          }
-          phase ^= 1u << cbuf;
-          inflight &= ~(1u << cbuf);
-          const int len = min(PCH, cnt - off);
-          const float4 *rb = buf + cbuf * PCH * 2;
-#pragma unroll 1
-          for (int base = 0; base < len; base += 32) {
-            const int i = base + lane;
-            const bool valid = i < len;
-            // idle lanes of the last slot push a copy of the chunk's last
-            // particle (results discarded): one instruction stream per warp
-            const int ii = valid ? i : len - 1;
-            const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
-            int cx = cx0, cy = cy0, cz = cz0;
-            float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
-            int pbad = 0;
-            push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
-                             pbad);
-            bad |= valid ? pbad : 0;
-            const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
-            flush(S, pend, wrec, lane, lost);   // the previous slot's counters are back
-            __syncwarp();
-            issue_slot(S, pend, wrec, key, b0, b1, nkey, valid, make_float4(ox, oy, oz, a.w),
-                       make_float4(u, v, w, 0.f), lane);
-          }
-          __syncwarp();   // every lane is done with this buffer before it is refilled
-          cbuf ^= 1;
-        }
+        W.inflight |= 1u << nbuf;
+        poff += len;
+        nbuf ^= 1;
       }
-      flush(S, pend, wrec, lane, lost);
-      __syncwarp();
+    };
+    Pending pend;
+    pend.valid = false;
+    pend.sbase0 = 0;
+    issue_next();
+    int cbuf = 0;
+    for (int j = 0; j < NC; ++j) {
+      const int cnt = __shfl_sync(FULL, cc, j);
+      if (cnt <= 0 || W.dead) continue;
+      const long long b0 = __shfl_sync(FULL, cb, j);
+      const long long b1 = b0 + __shfl_sync(FULL, ccap, j);
+      const int lc = warp + j * SIM_NW;
+      const int key = tile * T::TC + lc;
+      const int cx0 = c0x + lc / (TY * TZ), cy0 = c0y + (lc / TZ) % TY, cz0 = c0z + lc % TZ;
+#pragma unroll 1
+      for (int off = 0; off < cnt; off += PCH) {
+        issue_next();   // the following chunk streams in while this one is pushed
+        const bool ok = mbar_wait_bounded(W.cbar + cbuf, (W.phase >> cbuf) & 1u);
+        if (!__all_sync(FULL, ok)) {
+          W.dead = true;
+          break;
+        }
+        W.phase ^= 1u << cbuf;
+        W.inflight &= ~(1u << cbuf);
+        const int len = min(PCH, cnt - off);
+        const float4 *rb = W.buf + cbuf * PCH * 2;
+#pragma unroll 1
+        for (int base = 0; base < len; base += 32) {
+          const int i = base + lane;
+          const bool valid = i < len;
+          // idle lanes of the last slot push a copy of the chunk's last
+          // particle (results discarded): one instruction stream per warp
+          const int ii = valid ? i : len - 1;
+          const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
+          int cx = cx0, cy = cy0, cz = cz0;
+          float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
+          int pbad = 0;
+          push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
+                           pbad);
+          W.bad |= valid ? pbad : 0;
+          const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
+          flush(S, pend, W.wrec, lane, W.lost);   // the previous slot's counters are back
+          __syncwarp();
+          issue_slot(S, pend, W.wrec, key, b0, b1, nkey, valid, make_float4(ox, oy, oz, a.w),
+                     make_float4(u, v, w, 0.f), lane);
+        }
+        __syncwarp();   // every lane is done with this buffer before it is refilled
+        cbuf ^= 1;
+      }
     }
-    // every warp is done with this field stage before it is refilled
-    if (__syncthreads_or(dead)) {
-      // a record chunk never arrived: report, wait (bounded) for this warp's
-      // copies still in flight and for the prefetched field stage, give up
-      if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
-      for (int b = 0; b < 2; ++b)
-        if (inflight & (1u << b)) mbar_wait_bounded(cbar + b, (phase >> b) & 1u);
-      if (tile + (int)gridDim.x < ntiles)
-        mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
-      return;
-    }
+    flush(S, pend, W.wrec, lane, W.lost);
+    __syncwarp();
   }
+}
 
-  // overflow entries: pushed with gathers from L2 (the staged-tile origin is
-  // placed out of reach, so every gather takes the global path)
+// The overflow entries of every species of job P: pushed with gathers from
+// L2 (the staged-tile origin is placed out of reach, so every gather takes
+// the global path). sF is any valid staged buffer. All threads call.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ void push_overflow(const CycleParams &P, const float *sF, PushWarp &W) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
     const int on = min(*S.ocin, S.ocap);
@@ -585,18 +571,150 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
       float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
       int pbad = 0;
       constexpr int FAR = -(1 << 20);
-      push<TX, TY, TZ>(P, sF0, FAR, FAR, FAR, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
-      bad |= valid ? pbad : 0;
+      push<TX, TY, TZ>(P, sF, FAR, FAR, FAR, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
+      W.bad |= valid ? pbad : 0;
       const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
       if (valid) {
         const int slot = atomicAdd(S.cout + nkey, 1);
-        lost |= put_at(S, nkey, S.base[nkey], S.base[nkey + 1], slot,
-                       make_float4(ox, oy, oz, a.w), make_float4(u, v, w, 0.f));
+        W.lost |= put_at(S, nkey, S.base[nkey], S.base[nkey + 1], slot,
+                         make_float4(ox, oy, oz, a.w), make_float4(u, v, w, 0.f));
       }
     }
   }
-  if (bad) atomicOr(P.err, ERRBIT_OUT_OF_GRID);
-  if (lost) atomicOr(P.err, ERRBIT_LOST);
+}
+
+// Reports and clears a warp state's flags into job P's error word.
+__device__ __forceinline__ void report(const CycleParams &P, PushWarp &W) {
+  if (W.bad) atomicOr(P.err, ERRBIT_OUT_OF_GRID);
+  if (W.lost) atomicOr(P.err, ERRBIT_LOST);
+  W.bad = W.lost = 0;
+}
+
+// The mover (mover_PC, src/Mover.cpp:4-162) for every species. Persistent
+// CTAs walk tiles of TX x TY x TZ cells; one thread stages the tile's E/B
+// nodes plus a one-cell halo into shared memory with a TMA tensor copy (two
+// stages: the next tile's copy overlaps this tile's work). Warps walk the
+// tile's cells, one particle per lane, with the cells' records streamed
+// through two shared-memory chunk buffers per warp by bulk copies; the
+// gathers of the NiterMover iterations read the staged tile (or L2 past the
+// halo), and every pushed particle is written into the bucket of its new
+// cell. Afterwards the CTAs push the overflow entries (gathers from L2).
+// MULTI = false: one job, parameters P1 and field map fmap. MULTI = true: the
+// jobs of table J, each tile's job parameters staged in shared memory.
+template <int TX, int TY, int TZ, int MINB, bool MULTI>
+__global__ void __launch_bounds__(SIM_TPB, MINB)
+    k_push(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P1,
+           const __grid_constant__ JobTable J, const __grid_constant__ MapsOf<MULTI> M) {
+  using T = Tile<TX, TY, TZ>;
+  static_assert(T::TC % SIM_NW == 0 && T::TC / SIM_NW <= 32,
+                "cells per warp must fit a warp's lanes");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
+  float4 *sRec = reinterpret_cast<float4 *>(sF0 + 2 * T::SF);       // NW x 64 staged records
+  float4 *sBuf = sRec + SIM_NW * 64;                                // NW x 2 x PCH records
+  CycleParams *sP = reinterpret_cast<CycleParams *>(sBuf + SIM_NW * 2 * PCH * 2);  // MULTI
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sP + (MULTI ? 1 : 0));   // 2 + 2 NW
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  PushWarp W;
+  W.wrec = sRec + warp * 64;
+  W.buf = sBuf + warp * 2 * PCH * 2;
+  W.cbar = bar + 2 + warp * 2;
+  int *const err0 = MULTI ? J.params[0].err : P1.err;
+  if (smem_addr(sF0) & 127u) {   // TMA destinations need 128-byte alignment
+    if (tid == 0) atomicOr(err0, ERRBIT_SMEM_ALIGN);
+    return;
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+  }
+  if (lane == 0) {
+    mbar_init(W.cbar, 1);
+    mbar_init(W.cbar + 1, 1);
+  }
+  __syncthreads();
+
+  const int ntiles = MULTI ? J.total_tiles : P1.ntx * P1.nty * P1.ntz;
+  auto locate_tile = [&](int t, int &job, int &local) {
+    if constexpr (MULTI) {
+      job = job_of(J, t);
+      local = t - J.tile_base[job];
+    } else {
+      job = 0;
+      local = t;
+    }
+  };
+  const unsigned box_bytes = (unsigned)(T::BN * 8 * sizeof(float));
+  auto issue = [&](int t, int stage) {   // thread 0
+    int job, local;
+    locate_tile(t, job, local);
+    const int nty = MULTI ? J.params[job].nty : P1.nty;
+    const int ntz = MULTI ? J.params[job].ntz : P1.ntz;
+    const CUtensorMap *map;
+    if constexpr (MULTI)
+      map = &M.m[job];
+    else
+      map = &fmap;
+    const int z = local % ntz, y = (local / ntz) % nty, x = local / (ntz * nty);
+    fence_proxy_async();
+    mbar_expect_tx(bar + stage, box_bytes);
+    // box origin: node c0 on every axis (the lower node of halo cell c0-1)
+    tma_load_4d(sF0 + stage * T::SF, map, 0, z * TZ, y * TY, x * TX, bar + stage);
+  };
+  if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+  int it = 0, cur_job = -1;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int stage = it & 1;
+    // prefetch the next tile's fields into the other stage (read by the
+    // previous tile, which every thread finished before the last barrier)
+    if (tid == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
+    const bool arrived = mbar_wait_bounded(bar + stage, (it >> 1) & 1);
+    if (__syncthreads_or(!arrived)) {
+      // the staged fields never arrived (for some thread): the whole CTA
+      // reports, waits once more for its copies in flight, and gives up
+      if (tid == 0) atomicOr(err0, ERRBIT_TIMEOUT);
+      mbar_wait_bounded(bar + stage, (it >> 1) & 1);
+      mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
+      return;
+    }
+    const float *sF = sF0 + stage * T::SF;
+    int job, local;
+    locate_tile(tile, job, local);
+    if constexpr (MULTI) {
+      if (job != cur_job) {
+        load_params(sP, J.params + job);
+        cur_job = job;
+      }
+      push_tile<TX, TY, TZ>(*sP, local, sF, W);
+      report(*sP, W);
+    } else {
+      push_tile<TX, TY, TZ>(P1, local, sF, W);
+    }
+    // every warp is done with this field stage (and the staged parameters)
+    // before they are refilled
+    if (__syncthreads_or(W.dead)) {
+      // a record chunk never arrived: report, wait (bounded) for this warp's
+      // copies still in flight and for the prefetched field stage, give up
+      if (tid == 0) atomicOr(err0, ERRBIT_TIMEOUT);
+      for (int b = 0; b < 2; ++b)
+        if (W.inflight & (1u << b)) mbar_wait_bounded(W.cbar + b, (W.phase >> b) & 1u);
+      if (tile + (int)gridDim.x < ntiles)
+        mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
+      return;
+    }
+  }
+  if constexpr (MULTI) {
+    for (int job = 0; job < J.njobs; ++job) {
+      load_params(sP, J.params + job);
+      push_overflow<TX, TY, TZ>(*sP, sF0, W);
+      report(*sP, W);
+      __syncthreads();   // before the next job's parameters overwrite these
+    }
+  } else {
+    push_overflow<TX, TY, TZ>(P1, sF0, W);
+    report(P1, W);
+  }
 }
 
 // Deposit of one particle with FP64 global atomics (overflow entries; a rare
@@ -622,6 +740,138 @@ __device__ __noinline__ void deposit_global(const CycleParams &P, const SpeciesD
 
 constexpr int DCH = 128;   // records per bulk chunk of the deposit (4 KB)
 
+// Per-warp state of the deposit that lives across tiles and jobs.
+struct DepWarp {
+  float4 *buf;         // two record chunk buffers
+  uint64_t *bar;       // their barriers
+  unsigned phase = 0, inflight = 0;   // per buffer: next parity, copy issued
+  bool dead = false;   // a bounded wait ran out
+};
+
+// All species of one tile (tile-local index `tile` of job P). Returns false
+// when a chunk never arrived (every thread then gets false). All threads call.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ bool deposit_tile(const CycleParams &P, int tile, float *sCell,
+                                             DepWarp &W) {
+  using T = Tile<TX, TY, TZ>;
+  constexpr int NX = TX + 1, NY = TY + 1, NZ = TZ + 1, NB = NX * NY * NZ;
+  constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long nodes = (long)P.nxn * P.nyn * P.nzn;
+  // lane -> (corner, moments) of the warp totals (see warp_sum80)
+  const int corner = (lane >> 2) & 7, mbase = 5 * ((lane >> 1) & 1);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+  const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
+  const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
+  for (int s = 0; s < P.ns; ++s) {
+    const SpeciesDev &S = P.sp[s];
+    // lane j < NC holds bucket start and particle count of the warp's j-th
+    // cell (tile-local cell warp + j * NW)
+    long long cb = 0;
+    int cc = 0;
+    if (lane < NC) {
+      const int key = tile * T::TC + warp + lane * SIM_NW;
+      cb = S.base[key];
+      cc = (int)min((long long)S.cout[key], S.base[key + 1] - cb);
+    }
+    int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
+    auto issue_next = [&]() {         // all lanes call; lane 0 copies
+      while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
+        ++pj;
+        poff = 0;
+      }
+      if (pj < NC && !W.dead) {
+        const int len = min(DCH, __shfl_sync(FULL, cc, pj) - poff);
+        const long long b0 = __shfl_sync(FULL, cb, pj);
+        if (lane == 0) {
+          fence_proxy_async();
+          mbar_expect_tx(W.bar + nbuf, (unsigned)len * 32u);
+          bulk_load(W.buf + nbuf * DCH * 2, S.rout + 2 * (b0 + poff), (unsigned)len * 32u,
+                    W.bar + nbuf);
+        }
+        W.inflight |= 1u << nbuf;
+        poff += len;
+        nbuf ^= 1;
+      }
+    };
+    issue_next();
+    int cbuf = 0;
+    for (int j = 0; j < NC; ++j) {
+      const int cnt = __shfl_sync(FULL, cc, j);
+      float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+      if (cnt > 0 && !W.dead) {
+        float2 acc[40];
+#pragma unroll
+        for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
+#pragma unroll 1
+        for (int off = 0; off < cnt; off += DCH) {
+          issue_next();   // the following chunk streams in while this one is summed
+          const bool ok = mbar_wait_bounded(W.bar + cbuf, (W.phase >> cbuf) & 1u);
+          if (!__all_sync(FULL, ok)) {
+            W.dead = true;
+            break;
+          }
+          W.phase ^= 1u << cbuf;
+          W.inflight &= ~(1u << cbuf);
+          const int len = min(DCH, cnt - off);
+          const float4 *rb = W.buf + cbuf * DCH * 2;
+#pragma unroll 1
+          for (int base = 0; base < len; base += 32) {
+            const bool valid = base + lane < len;
+            const int ii = min(base + lane, len - 1);
+            const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
+            add_terms(acc, valid ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, lane);
+          }
+          __syncwarp();   // every lane is done with this buffer before it is refilled
+          cbuf ^= 1;
+        }
+        warp_sum80(acc, r, lane);
+      }
+      float *dst = sCell + (warp + j * SIM_NW) * 80 + corner * 10 + mbase;
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if (k >= lo && k < hi) dst[k] = r[k];
+    }
+    if (__syncthreads_or(W.dead)) return false;
+    for (int idx = tid; idx < 10 * NB; idx += SIM_TPB) {
+      const int m = idx / NB, nb = idx % NB;
+      const int bz = nb % NZ, by = (nb / NZ) % NY, bx = nb / (NZ * NY);
+      float sum = 0.0f;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int lx = bx - a, ly = by - b, lz = bz - c;
+            if (lx >= 0 && lx < TX && ly >= 0 && ly < TY && lz >= 0 && lz < TZ)
+              sum += sCell[((lx * TY + ly) * TZ + lz) * 80 + (a * 4 + b * 2 + c) * 10 + m];
+          }
+      if (sum != 0.0f) {
+        const long g = ((long)(c0x + bx + 1) * P.nyn + (c0y + by + 1)) * P.nzn + (c0z + bz + 1);
+        atomicAdd(S.mom + m * nodes + g, (double)sum * P.scale);
+      }
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// Overflow entries of every species of job P, one by one with FP64 atomics.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
+  for (int s = 0; s < P.ns; ++s) {
+    const SpeciesDev &S = P.sp[s];
+    const int on = min(*S.ocout, S.ocap);
+    for (long i = (long)blockIdx.x * SIM_TPB + threadIdx.x; i < on;
+         i += (long)gridDim.x * SIM_TPB) {
+      int cx, cy, cz;
+      key_cell<TX, TY, TZ>(S.okout[i], P.nty, P.ntz, cx, cy, cz);
+      deposit_global(P, S, cx, cy, cz, S.oout[2 * i], S.oout[2 * i + 1]);
+    }
+  }
+}
+
 // The deposit (interpP2G, src/Mover.cpp:385-572) for every species, from the
 // buckets the push wrote. One warp per cell. Each warp streams its cells'
 // buckets through two shared-memory chunk buffers with bulk copies (one chunk
@@ -631,140 +881,76 @@ constexpr int DCH = 128;   // records per bulk chunk of the deposit (4 KB)
 // shared memory. Each node of the tile then adds up the totals of its (up to
 // 8) cells in the tile and one FP64 atomic per node and moment adds the sum
 // into the moments. Overflow entries deposit one by one with FP64 atomics.
-template <int TX, int TY, int TZ>
-__global__ void __launch_bounds__(SIM_TPB, 2) k_deposit(const __grid_constant__ CycleParams P) {
+// MULTI as for k_push.
+template <int TX, int TY, int TZ, bool MULTI>
+__global__ void __launch_bounds__(SIM_TPB, 2)
+    k_deposit(const __grid_constant__ CycleParams P1, const __grid_constant__ JobTable J) {
   using T = Tile<TX, TY, TZ>;
-  constexpr int NX = TX + 1, NY = TY + 1, NZ = TZ + 1, NB = NX * NY * NZ;
-  constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
-  static_assert(T::TC % SIM_NW == 0 && NC <= 32, "cells per warp must fit a warp's lanes");
+  static_assert(T::TC % SIM_NW == 0 && T::TC / SIM_NW <= 32,
+                "cells per warp must fit a warp's lanes");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float4 *sBuf = reinterpret_cast<float4 *>(smem_raw);                 // NW x 2 x DCH records
   float *sCell = reinterpret_cast<float *>(sBuf + SIM_NW * 2 * DCH * 2);  // TC x 8 x 10
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sCell + T::TC * 80);     // NW x 2
+  CycleParams *sP = reinterpret_cast<CycleParams *>(sCell + T::TC * 80);   // MULTI
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sP + (MULTI ? 1 : 0));    // NW x 2
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float4 *buf = sBuf + warp * 2 * DCH * 2;
-  uint64_t *bar = bars + warp * 2;
+  DepWarp W;
+  W.buf = sBuf + warp * 2 * DCH * 2;
+  W.bar = bars + warp * 2;
   if (lane == 0) {
-    mbar_init(bar, 1);
-    mbar_init(bar + 1, 1);
+    mbar_init(W.bar, 1);
+    mbar_init(W.bar + 1, 1);
   }
   __syncthreads();
-  const int ntiles = P.ntx * P.nty * P.ntz;
-  const long nodes = (long)P.nxn * P.nyn * P.nzn;
-  // lane -> (corner, moments) of the warp totals (see warp_sum80)
-  const int corner = (lane >> 2) & 7, mbase = 5 * ((lane >> 1) & 1);
-  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
-  unsigned phase = 0, inflight = 0;   // per buffer: parity of the next wait, copy issued
-  bool dead = false;                  // a bounded wait ran out
+  int *const err0 = MULTI ? J.params[0].err : P1.err;
+  const int ntiles = MULTI ? J.total_tiles : P1.ntx * P1.nty * P1.ntz;
+  int cur_job = -1;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
-    const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
-    for (int s = 0; s < P.ns; ++s) {
-      const SpeciesDev &S = P.sp[s];
-      // lane j < NC holds bucket start and particle count of the warp's j-th
-      // cell (tile-local cell warp + j * NW)
-      long long cb = 0;
-      int cc = 0;
-      if (lane < NC) {
-        const int key = tile * T::TC + warp + lane * SIM_NW;
-        cb = S.base[key];
-        cc = (int)min((long long)S.cout[key], S.base[key + 1] - cb);
+    bool ok;
+    if constexpr (MULTI) {
+      const int job = job_of(J, tile);
+      if (job != cur_job) {
+        load_params(sP, J.params + job);
+        cur_job = job;
       }
-      int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
-      auto issue_next = [&]() {         // all lanes call; lane 0 copies
-        while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
-          ++pj;
-          poff = 0;
-        }
-        if (pj < NC && !dead) {
-          const int len = min(DCH, __shfl_sync(FULL, cc, pj) - poff);
-          const long long b0 = __shfl_sync(FULL, cb, pj);
-          if (lane == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(bar + nbuf, (unsigned)len * 32u);
-            bulk_load(buf + nbuf * DCH * 2, S.rout + 2 * (b0 + poff), (unsigned)len * 32u,
-                      bar + nbuf);
-          }
-          inflight |= 1u << nbuf;
-          poff += len;
-          nbuf ^= 1;
-        }
-      };
-      issue_next();
-      int cbuf = 0;
-      for (int j = 0; j < NC; ++j) {
-        const int cnt = __shfl_sync(FULL, cc, j);
-        float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-        if (cnt > 0 && !dead) {
-          float2 acc[40];
-#pragma unroll
-          for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
-#pragma unroll 1
-          for (int off = 0; off < cnt; off += DCH) {
-            issue_next();   // the following chunk streams in while this one is summed
-            const bool ok = mbar_wait_bounded(bar + cbuf, (phase >> cbuf) & 1u);
-            if (!__all_sync(FULL, ok)) {
-              dead = true;
-              break;
-            }
-            phase ^= 1u << cbuf;
-            inflight &= ~(1u << cbuf);
-            const int len = min(DCH, cnt - off);
-            const float4 *rb = buf + cbuf * DCH * 2;
-#pragma unroll 1
-            for (int base = 0; base < len; base += 32) {
-              const bool valid = base + lane < len;
-              const int ii = min(base + lane, len - 1);
-              const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
-              add_terms(acc, valid ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, lane);
-            }
-            __syncwarp();   // every lane is done with this buffer before it is refilled
-            cbuf ^= 1;
-          }
-          warp_sum80(acc, r, lane);
-        }
-        float *dst = sCell + (warp + j * SIM_NW) * 80 + corner * 10 + mbase;
-#pragma unroll
-        for (int k = 0; k < 5; ++k)
-          if (k >= lo && k < hi) dst[k] = r[k];
-      }
-      if (__syncthreads_or(dead)) {
-        // a chunk never arrived: report, wait (bounded) for the copies this
-        // warp still has in flight, and give up
-        if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
-        for (int b = 0; b < 2; ++b)
-          if (inflight & (1u << b)) mbar_wait_bounded(bar + b, (phase >> b) & 1u);
-        return;
-      }
-      for (int idx = tid; idx < 10 * NB; idx += SIM_TPB) {
-        const int m = idx / NB, nb = idx % NB;
-        const int bz = nb % NZ, by = (nb / NZ) % NY, bx = nb / (NZ * NY);
-        float sum = 0.0f;
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-          for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-              const int lx = bx - a, ly = by - b, lz = bz - c;
-              if (lx >= 0 && lx < TX && ly >= 0 && ly < TY && lz >= 0 && lz < TZ)
-                sum += sCell[((lx * TY + ly) * TZ + lz) * 80 + (a * 4 + b * 2 + c) * 10 + m];
-            }
-        if (sum != 0.0f) {
-          const long g = ((long)(c0x + bx + 1) * P.nyn + (c0y + by + 1)) * P.nzn + (c0z + bz + 1);
-          atomicAdd(S.mom + m * nodes + g, (double)sum * P.scale);
-        }
-      }
-      __syncthreads();
+      ok = deposit_tile<TX, TY, TZ>(*sP, tile - J.tile_base[job], sCell, W);
+    } else {
+      ok = deposit_tile<TX, TY, TZ>(P1, tile, sCell, W);
+    }
+    if (!ok) {
+      // a chunk never arrived: report, wait (bounded) for the copies this
+      // warp still has in flight, and give up
+      if (tid == 0) atomicOr(err0, ERRBIT_TIMEOUT);
+      for (int b = 0; b < 2; ++b)
+        if (W.inflight & (1u << b)) mbar_wait_bounded(W.bar + b, (W.phase >> b) & 1u);
+      return;
     }
   }
-  for (int s = 0; s < P.ns; ++s) {
-    const SpeciesDev &S = P.sp[s];
-    const int on = min(*S.ocout, S.ocap);
-    for (long i = (long)blockIdx.x * SIM_TPB + tid; i < on; i += (long)gridDim.x * SIM_TPB) {
-      int cx, cy, cz;
-      key_cell<TX, TY, TZ>(S.okout[i], P.nty, P.ntz, cx, cy, cz);
-      deposit_global(P, S, cx, cy, cz, S.oout[2 * i], S.oout[2 * i + 1]);
+  if constexpr (MULTI) {
+    for (int job = 0; job < J.njobs; ++job) {
+      __syncthreads();   // every thread is done with the staged parameters
+      load_params(sP, J.params + job);
+      deposit_overflow<TX, TY, TZ>(*sP);
+    }
+  } else {
+    deposit_overflow<TX, TY, TZ>(P1);
+  }
+}
+
+// Zeroes every job's write-side fill counters and overflow counter and its
+// moments before a multi-job cycle (one launch instead of three memsets per
+// job and species).
+__global__ void k_zero_jobs(const __grid_constant__ JobTable J) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  const long t0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  for (int j = 0; j < J.njobs; ++j) {
+    const CycleParams &P = J.params[j];
+    const long ncells = (long)P.nxc * P.nyc * P.nzc, nodes = (long)P.nxn * P.nyn * P.nzn;
+    for (int s = 0; s < P.ns; ++s) {
+      const SpeciesDev &S = P.sp[s];
+      for (long i = t0; i < ncells; i += stride) S.cout[i] = 0;
+      if (t0 == 0) *S.ocout = 0;
+      for (long i = t0; i < 10 * nodes; i += stride) S.mom[i] = 0.0;
     }
   }
 }
@@ -1093,66 +1279,6 @@ using namespace spb;
 // ---------------------------------------------------------------------------
 namespace {
 
-struct SimSpecies {
-  long n = 0;
-  double qom = 0;
-  int ocap = 0;                 // overflow entries
-  float4 *rec[2] = {};          // buckets, [slots[b]][2] each
-  long long slots[2] = {0, 0};  // allocated record slots per buffer set
-  int *cnt[2] = {};             // per-cell fill counters
-  float4 *orec[2] = {};         // overflow records, [ocap][2]
-  int *okey[2] = {};            // overflow cell keys
-  int *ocnt = nullptr;          // [2] overflow entry counters
-  long long *base = nullptr;    // [ncells + 1] bucket layout of both buffer sets
-  long long *base2 = nullptr;   // [ncells + 1] the next layout (re-layout)
-  long long total = 0;          // record slots of the layout
-  int cur = 0;                  // the buffer set holding the particles
-  double *mom = nullptr;        // [10][nodes]
-};
-
-using EvPair = std::pair<cudaEvent_t, cudaEvent_t>;
-struct EvCycle {
-  cudaEvent_t b, m, e;          // before push, between push and deposit, after deposit
-};
-
-}  // namespace
-
-struct spb_sim {
-  spb_sim_desc d{};
-  int device = 0;
-  int N[3] = {0, 0, 0};
-  int tile[3] = {8, 4, 4};
-  int nt[3] = {0, 0, 0};
-  long ncells = 0, nodes = 0;
-  int nxn = 0, nyn = 0, nzn = 0;
-  double dxyz[3] = {0, 0, 0};
-  float *fields8 = nullptr;
-  float *stage = nullptr;       // 6*nodes for host field uploads
-  int *d_err = nullptr;
-  long long *scan_tmp = nullptr;  // scan block sums + grand total
-  int *counts = nullptr;          // [ncells] particles per cell
-  long long *lcap = nullptr;      // [ncells] capacities / clamped counts
-  long long *offset = nullptr;    // [ncells + 1] readback offsets
-  CUtensorMap fmap{};
-  bool fields_set = false;
-  int cycles_since_check = 0;
-  // CUDA graphs of one cycle's launches, keyed by the species' buffer parities;
-  // captured and replayed on gstream, ordered after the caller's stream
-  std::map<unsigned, cudaGraphExec_t> graphs;
-  cudaStream_t gstream = nullptr;
-  cudaEvent_t gev[2] = {nullptr, nullptr};
-  long cycles_run = 0;
-  bool graph_failed = false;
-  std::vector<SimSpecies> sp;
-  long launches = 0;
-  // optional CUDA-event timing of the cycle kernels and of the relayouts
-  bool timing = false;
-  std::vector<EvCycle> ev_cycle;
-  std::vector<EvPair> ev_relayout;
-};
-
-namespace {
-
 cudaEvent_t record_event(spb_sim *s, cudaStream_t st) {
   cudaEvent_t e = nullptr;
   if (s->timing && cudaEventCreate(&e) == cudaSuccess) cudaEventRecord(e, st);
@@ -1183,17 +1309,24 @@ int encode_field_map(spb_sim *s) {
   return SPB_OK;
 }
 
+// Dynamic shared memory of the kernels; the multi-job kernels also stage one
+// job's parameters.
 template <int TX, int TY, int TZ>
-size_t push_smem() {
+size_t push_smem(bool multi = false) {
   return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + (size_t)SIM_NW * 64 * sizeof(float4) +
-         (size_t)SIM_NW * 2 * PCH * 2 * sizeof(float4) + (2 + 2 * SIM_NW) * sizeof(uint64_t);
+         (size_t)SIM_NW * 2 * PCH * 2 * sizeof(float4) + (multi ? sizeof(CycleParams) : 0) +
+         (2 + 2 * SIM_NW) * sizeof(uint64_t);
 }
 template <int TX, int TY, int TZ>
-size_t deposit_smem() {
+size_t deposit_smem(bool multi = false) {
   return (size_t)SIM_NW * 2 * DCH * 2 * sizeof(float4) +
-         (size_t)Tile<TX, TY, TZ>::TC * 80 * sizeof(float) + SIM_NW * 2 * sizeof(uint64_t);
+         (size_t)Tile<TX, TY, TZ>::TC * 80 * sizeof(float) + (multi ? sizeof(CycleParams) : 0) +
+         SIM_NW * 2 * sizeof(uint64_t);
 }
 
+}  // namespace
+
+namespace spb {
 // Kernel parameters for a cycle that reads buffer set `cur` and writes the other.
 CycleParams make_params(spb_sim *s) {
   CycleParams P{};
@@ -1237,6 +1370,9 @@ CycleParams make_params(spb_sim *s) {
   }
   return P;
 }
+}  // namespace spb
+
+namespace {
 
 // One cycle: zero the moments and the write-side counters, push, deposit.
 template <int TX, int TY, int TZ, int MINB>
@@ -1250,9 +1386,9 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   const size_t psm = push_smem<TX, TY, TZ>(), dsm = deposit_smem<TX, TY, TZ>();
   static bool attr = false;
   if (!attr) {
-    SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB>,
+    SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ>,
+    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
     attr = true;
   }
@@ -1260,9 +1396,11 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   const int ntiles = s->nt[0] * s->nt[1] * s->nt[2];
   static int pocc = 0, docc = 0;   // resident CTAs per SM
   if (!pocc) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB>, SIM_TPB,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, false>,
+                                                      SIM_TPB,
                                                       psm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ>, SIM_TPB,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, false>,
+                                                      SIM_TPB,
                                                       dsm) != cudaSuccess) {
       cudaGetLastError();
       pocc = MINB;
@@ -1274,10 +1412,11 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   const int pctas = std::min(ntiles, s->d.ctas > 0 ? s->d.ctas : pocc * num_sms());
   const int dctas = std::min(ntiles, docc * num_sms());
   EvCycle ev{record_event(s, st), nullptr, nullptr};
-  k_push<TX, TY, TZ, MINB><<<pctas, SIM_TPB, psm, st>>>(s->fmap, P);
+  k_push<TX, TY, TZ, MINB, false><<<pctas, SIM_TPB, psm, st>>>(s->fmap, P, JobTable{},
+                                                               NoMaps{});
   SPB_CUDA(cudaGetLastError());
   ev.m = record_event(s, st);
-  k_deposit<TX, TY, TZ><<<dctas, SIM_TPB, dsm, st>>>(P);
+  k_deposit<TX, TY, TZ, false><<<dctas, SIM_TPB, dsm, st>>>(P, JobTable{});
   SPB_CUDA(cudaGetLastError());
   ev.e = record_event(s, st);
   if (ev.b && ev.m && ev.e) s->ev_cycle.push_back(ev);
@@ -1490,16 +1629,119 @@ int unload(spb_sim *s, SimSpecies &q, float *const dst[7], cudaStream_t st) {
   return SPB_OK;
 }
 
+}  // namespace
+
+namespace spb {
+
+JobBuffers::~JobBuffers() {
+  if (ready) cudaEventDestroy(ready);
+  cudaFree(d_tile_base);
+  cudaFree(d_params);
+  cudaFreeHost(h_tile_base);
+  cudaFreeHost(h_params);
+}
+
+}  // namespace spb
+
+namespace {
+
+int ensure_job_buffers(JobBuffers &B, int n) {
+  if (!B.ready) SPB_CUDA(cudaEventCreateWithFlags(&B.ready, cudaEventDisableTiming));
+  // the pinned mirrors may still be read by the previous launch's copies
+  SPB_CUDA(cudaEventSynchronize(B.ready));
+  if (n <= B.cap) return SPB_OK;
+  const int cap = std::max(n, 2 * B.cap);
+  cudaFree(B.d_tile_base);
+  cudaFree(B.d_params);
+  cudaFreeHost(B.h_tile_base);
+  cudaFreeHost(B.h_params);
+  B.d_tile_base = B.h_tile_base = nullptr;
+  B.d_params = B.h_params = nullptr;
+  B.cap = 0;
+  if (cudaMalloc(&B.d_tile_base, (cap + 1) * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&B.d_params, cap * sizeof(CycleParams)) != cudaSuccess ||
+      cudaMallocHost(&B.h_tile_base, (cap + 1) * sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&B.h_params, cap * sizeof(CycleParams)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SPB_ERR_ALLOC, "job table allocation failed");
+  }
+  B.cap = cap;
+  return SPB_OK;
+}
+
+template <int TX, int TY, int TZ>
+int launch_jobs_t(spb_sim *const *sims, int n, JobBuffers &B, cudaStream_t st) {
+  constexpr int MINB = 2;
+  const size_t psm = push_smem<TX, TY, TZ>(true), dsm = deposit_smem<TX, TY, TZ>(true);
+  static int pocc = 0, docc = 0;
+  if (!pocc) {
+    SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, true>,
+                                                      SIM_TPB, psm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, true>,
+                                                      SIM_TPB, dsm) != cudaSuccess) {
+      cudaGetLastError();
+      pocc = MINB;
+      docc = 1;
+    }
+    pocc = std::max(pocc, 1);
+    docc = std::max(docc, 1);
+  }
+  if (n > SERVE_MAX_JOBS) return fail(SPB_ERR_CAPACITY, "at most 64 jobs per launch");
+  if (int rc = ensure_job_buffers(B, n)) return rc;
+  static JobMaps maps;   // 8 KB, passed by value as a kernel parameter
+  int total = 0;
+  for (int j = 0; j < n; ++j) {
+    spb_sim *s = sims[j];
+    B.h_tile_base[j] = total;
+    total += s->nt[0] * s->nt[1] * s->nt[2];
+    B.h_params[j] = make_params(s);
+    maps.m[j] = s->fmap;
+  }
+  B.h_tile_base[n] = total;
+  SPB_CUDA(cudaMemcpyAsync(B.d_tile_base, B.h_tile_base, (n + 1) * sizeof(int),
+                           cudaMemcpyHostToDevice, st));
+  SPB_CUDA(cudaMemcpyAsync(B.d_params, B.h_params, n * sizeof(CycleParams),
+                           cudaMemcpyHostToDevice, st));
+  SPB_CUDA(cudaEventRecord(B.ready, st));
+  const JobTable J{n, total, B.d_tile_base, B.d_params};
+  k_zero_jobs<<<2 * num_sms(), 256, 0, st>>>(J);
+  SPB_CUDA(cudaGetLastError());
+  const int pctas = std::min(total, pocc * num_sms());
+  const int dctas = std::min(total, docc * num_sms());
+  k_push<TX, TY, TZ, MINB, true><<<pctas, SIM_TPB, psm, st>>>(CUtensorMap{}, CycleParams{}, J,
+                                                              maps);
+  SPB_CUDA(cudaGetLastError());
+  k_deposit<TX, TY, TZ, true><<<dctas, SIM_TPB, dsm, st>>>(CycleParams{}, J);
+  SPB_CUDA(cudaGetLastError());
+  g_launches += 3;
+  for (int j = 0; j < n; ++j) {
+    sims[j]->launches += 2;
+    for (auto &q : sims[j]->sp) q.cur = 1 - q.cur;
+  }
+  return SPB_OK;
+}
+
+}  // namespace
+
+namespace {
+
 // Tile shapes the kernels are instantiated for.
 struct TileImpl {
   int t[3];
   int (*cycle)(spb_sim *, cudaStream_t);
+  int (*jobs)(spb_sim *const *, int, JobBuffers &, cudaStream_t);
   int (*build)(spb_sim *, SimSpecies &, const float *const *, long, cudaStream_t);
   int (*unload)(spb_sim *, SimSpecies &, float *const *, cudaStream_t);
 };
 
 #define SPB_TILE(X, Y, Z) \
-  TileImpl { {X, Y, Z}, launch_cycle<X, Y, Z>, build<X, Y, Z>, unload<X, Y, Z> }
+  TileImpl {                                                                   \
+    {X, Y, Z}, launch_cycle<X, Y, Z>, launch_jobs_t<X, Y, Z>, build<X, Y, Z>, unload<X, Y, Z> \
+  }
 const TileImpl kTiles[] = {SPB_TILE(8, 4, 4), SPB_TILE(4, 4, 4), SPB_TILE(2, 2, 2),
                            SPB_TILE(8, 8, 4)};
 #undef SPB_TILE
@@ -1509,6 +1751,28 @@ const TileImpl *find_tile(const int t[3]) {
     if (ti.t[0] == t[0] && ti.t[1] == t[1] && ti.t[2] == t[2]) return &ti;
   return nullptr;
 }
+
+}  // namespace
+
+namespace spb {
+
+int launch_jobs(spb_sim *const *sims, int n, JobBuffers &buf, cudaStream_t st) {
+  if (n <= 0) return SPB_OK;
+  for (int j = 0; j < n; ++j) {
+    const spb_sim *s = sims[j];
+    if (!s || !s->fields_set) return fail(SPB_ERR_INVALID, "launch_jobs: job without fields");
+    for (int a = 0; a < 3; ++a)
+      if (s->tile[a] != sims[0]->tile[a])
+        return fail(SPB_ERR_INVALID, "launch_jobs: jobs of one launch share the tile shape");
+    for (const auto &q : s->sp)
+      if (!q.rec[0]) return fail(SPB_ERR_INVALID, "launch_jobs: a species was never loaded");
+  }
+  return find_tile(sims[0]->tile)->jobs(sims, n, buf, st);
+}
+
+}  // namespace spb
+
+namespace {
 
 // Temporary flat reference-layout arrays (7 x n floats).
 struct Flat {

@@ -27,6 +27,7 @@
 namespace spb {
 
 constexpr int SIM_MAX_SPECIES = 8;
+constexpr int SERVE_MAX_JOBS = 64;   // jobs per multi-job launch
 
 __host__ __device__ __forceinline__ uint32_t pack_cell(int cx, int cy, int cz) {
   return (uint32_t)cz | ((uint32_t)cy << 11) | ((uint32_t)cx << 21);
