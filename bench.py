@@ -376,6 +376,13 @@ def run_ours(args, rank, world, local_rank):
     if host is not None:
         e2e = run_e2e(args, wl, host, host_f, world, dist)
 
+    serving = None
+    if not args.no_serving:
+        # independent replicas under torchrun; rank 0 reports its own
+        from sputnipic_b200.serve import measure_stream
+        serving = measure_stream(rate=args.serve_rate, njobs=args.serve_jobs)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, n, kind, cores = time_cpu(wl, args.cpu_slabs, 3, 1, min_seconds=10.0)
@@ -410,7 +417,7 @@ def run_ours(args, rank, world, local_rank):
             "plain": None if plain is None else {
                 "value": plain["value"], "unit": UNIT, "ms_per_step": plain["ms_per_step"],
                 "kernels": plain["kernels"], "speedup_of_precision_form": value / plain["value"]},
-            "e2e": e2e, "cpu_baseline": cpu,
+            "e2e": e2e, "cpu_baseline": cpu, "serving": serving,
         }
         print(json.dumps(line), flush=True)
 
@@ -489,6 +496,10 @@ def main():
                     help="pick the tile shape and push variant first (timed on this workload)")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each cycle directly instead of replaying a CUDA graph")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the serving stream (Poisson arrivals of mixed jobs)")
+    ap.add_argument("--serve-rate", type=float, default=10.0, help="serving arrivals, jobs/s")
+    ap.add_argument("--serve-jobs", type=int, default=100, help="jobs in the serving stream")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

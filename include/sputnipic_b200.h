@@ -340,6 +340,9 @@ int spb_serve_result(spb_serve *srv, long id, int species, float *x, float *y, f
 int spb_serve_times(const spb_serve *srv, long id, double t[3]);
 /* Frees a finished or failed job. */
 int spb_serve_release(spb_serve *srv, long id);
+/* Steps run, then host seconds spent in admitting jobs, overflow checks,
+ * the launches and their completion, and retiring jobs (5 values). */
+int spb_serve_stats(const spb_serve *srv, double out[5]);
 /* Jobs queued, admitted and finished (not yet released); bytes held by the
  * admitted and finished jobs, and the budget. */
 int spb_serve_counts(const spb_serve *srv, int *pending, int *active, int *done,

@@ -248,6 +248,7 @@ def load():
     _proto(lib, "spb_serve_result", c_int, [P, c_long, c_int] + [P] * 8 + [c_int])
     _proto(lib, "spb_serve_times", c_int, [P, c_long, P])
     _proto(lib, "spb_serve_release", c_int, [P, c_long])
+    _proto(lib, "spb_serve_stats", c_int, [P, P])
     _proto(lib, "spb_serve_counts", c_int,
            [P, R(c_int), R(c_int), R(c_int), R(ctypes.c_longlong), R(ctypes.c_longlong)])
     _lib = lib

@@ -76,6 +76,8 @@ struct spb_serve {
   long long budget = 0, used = 0;
   long next_id = 0;
   long steps = 0;
+  double phase_s[4] = {0, 0, 0, 0};   // admit, overflow checks, launch + wait, retire
+  int *h_ovf = nullptr;   // pinned: overflow counters of the admitted jobs' species
   Clock::time_point t0;
   std::deque<ServeJob *> pending;
   std::vector<ServeJob *> active;
@@ -151,6 +153,7 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
   s->d = d;
   SPB_CUDA(cudaGetDevice(&s->device));
   SPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  SPB_CUDA(cudaMallocHost(&s->h_ovf, (size_t)SERVE_MAX_JOBS * SPB_SIM_MAX_SPECIES * sizeof(int)));
   if (d.hbm_budget > 0) {
     s->budget = d.hbm_budget;
   } else {
@@ -168,6 +171,7 @@ extern "C" void spb_serve_destroy(spb_serve *s) {
   if (s->st) cudaStreamSynchronize(s->st);
   s->jobs.clear();
   if (s->st) cudaStreamDestroy(s->st);
+  cudaFreeHost(s->h_ovf);
   delete s;
 }
 
@@ -207,6 +211,12 @@ extern "C" long spb_serve_submit(spb_serve *s, const spb_job_desc *job,
 extern "C" int spb_serve_step(spb_serve *s) {
   if (!s) return -fail(SPB_ERR_INVALID, "spb_serve_step: null engine");
   SPB_CUDA(cudaSetDevice(s->device));
+  Clock::time_point tp = Clock::now();
+  auto lap = [&](int phase) {
+    const Clock::time_point t = Clock::now();
+    s->phase_s[phase] += std::chrono::duration<double>(t - tp).count();
+    tp = t;
+  };
   // admit in order of arrival while the head fits
   while (!s->pending.empty() && (int)s->active.size() < s->d.max_jobs) {
     ServeJob *j = s->pending.front();
@@ -226,21 +236,32 @@ extern "C" int spb_serve_step(spb_serve *s) {
     }
     s->active.push_back(j);
   }
+  lap(0);
   if (s->active.empty()) return 0;
-  // overflow lists in use: re-lay out those jobs (synchronises)
-  if (s->steps > 0 && s->steps % s->d.check_every == 0)
+  // overflow lists in use: re-lay out those jobs (one synchronisation for all)
+  if (s->steps > 0 && s->steps % s->d.check_every == 0) {
+    int k = 0;
     for (ServeJob *j : s->active)
-      for (int i = 0; i < j->d.ns; ++i)
-        if (spb_sim_overflow(j->sim, i, s->st) > 0) {
-          if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
-          break;
-        }
+      for (const SimSpecies &q : j->sim->sp)
+        SPB_CUDA(cudaMemcpyAsync(s->h_ovf + k++, q.ocnt + q.cur, sizeof(int),
+                                 cudaMemcpyDeviceToHost, s->st));
+    SPB_CUDA(cudaStreamSynchronize(s->st));
+    k = 0;
+    for (ServeJob *j : s->active) {
+      bool over = false;
+      for (size_t i = 0; i < j->sim->sp.size(); ++i) over |= s->h_ovf[k++] > 0;
+      if (over)
+        if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
+    }
+  }
+  lap(1);
   std::vector<spb_sim *> sims;
   sims.reserve(s->active.size());
   for (ServeJob *j : s->active) sims.push_back(j->sim);
   if (int rc = launch_jobs(sims.data(), (int)sims.size(), s->buf, s->st)) return -rc;
   SPB_CUDA(cudaStreamSynchronize(s->st));
   s->steps++;
+  lap(2);
   // retire the jobs that reached their cycle count
   std::vector<ServeJob *> still;
   for (ServeJob *j : s->active) {
@@ -257,7 +278,15 @@ extern "C" int spb_serve_step(spb_serve *s) {
     }
   }
   s->active.swap(still);
+  lap(3);
   return (int)s->active.size();
+}
+
+extern "C" int spb_serve_stats(const spb_serve *s, double out[5]) {
+  if (!s || !out) return fail(SPB_ERR_INVALID, "spb_serve_stats: null argument");
+  out[0] = (double)s->steps;
+  for (int i = 0; i < 4; ++i) out[1 + i] = s->phase_s[i];
+  return SPB_OK;
 }
 
 extern "C" int spb_serve_status(const spb_serve *s, long id) {

@@ -1279,6 +1279,47 @@ using namespace spb;
 // ---------------------------------------------------------------------------
 namespace {
 
+// Device memory of the precision form comes from the device's stream-ordered
+// pool (cudaMallocAsync), which keeps freed memory for reuse: creating and
+// destroying simulations (one per serving job) then maps and unmaps nothing.
+// dmalloc returns memory usable by every stream; dfree hands it back at once,
+// so its callers make sure no queued work still reads it.
+cudaStream_t pool_stream() {
+  static std::mutex mu;
+  static std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    st = nullptr;
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long keep = ~0ull;   // keep freed memory in the pool
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  streams[dev] = st;
+  return st;
+}
+
+template <typename T>
+cudaError_t dmalloc(T **p, size_t bytes) {
+  cudaStream_t st = pool_stream();
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(p), std::max<size_t>(bytes, 1), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) *p = nullptr;
+  return e;
+}
+
+void dfree(void *p) {
+  if (p) cudaFreeAsync(p, pool_stream());
+}
+
 cudaEvent_t record_event(spb_sim *s, cudaStream_t st) {
   cudaEvent_t e = nullptr;
   if (s->timing && cudaEventCreate(&e) == cudaSuccess) cudaEventRecord(e, st);
@@ -1450,7 +1491,7 @@ GridScalars scalars(const spb_sim *s) {
 }
 
 void free_set(SimSpecies &q, int b) {
-  cudaFree(q.rec[b]);
+  dfree(q.rec[b]);
   q.rec[b] = nullptr;
   q.slots[b] = 0;
 }
@@ -1458,15 +1499,15 @@ void free_set(SimSpecies &q, int b) {
 void free_buckets(SimSpecies &q) {
   for (int b = 0; b < 2; ++b) {
     free_set(q, b);
-    cudaFree(q.cnt[b]);
-    cudaFree(q.orec[b]);
-    cudaFree(q.okey[b]);
+    dfree(q.cnt[b]);
+    dfree(q.orec[b]);
+    dfree(q.okey[b]);
     q.orec[b] = nullptr;
     q.cnt[b] = q.okey[b] = nullptr;
   }
-  cudaFree(q.ocnt);
-  cudaFree(q.base);
-  cudaFree(q.base2);
+  dfree(q.ocnt);
+  dfree(q.base);
+  dfree(q.base2);
   q.ocnt = nullptr;
   q.base = q.base2 = nullptr;
   q.ocap = 0;
@@ -1476,14 +1517,15 @@ void free_buckets(SimSpecies &q) {
 // Per-species arrays whose size does not depend on the layout.
 int alloc_fixed(spb_sim *s, SimSpecies &q, int ocap) {
   if (q.base && q.ocap == ocap) return SPB_OK;
+  if (q.base) SPB_CUDA(cudaDeviceSynchronize());   // queued work may still read the old arrays
   free_buckets(q);
-  bool ok = cudaMalloc(&q.ocnt, 2 * sizeof(int)) == cudaSuccess &&
-            cudaMalloc(&q.base, (s->ncells + 1) * sizeof(long long)) == cudaSuccess &&
-            cudaMalloc(&q.base2, (s->ncells + 1) * sizeof(long long)) == cudaSuccess;
+  bool ok = dmalloc(&q.ocnt, 2 * sizeof(int)) == cudaSuccess &&
+            dmalloc(&q.base, (s->ncells + 1) * sizeof(long long)) == cudaSuccess &&
+            dmalloc(&q.base2, (s->ncells + 1) * sizeof(long long)) == cudaSuccess;
   for (int b = 0; b < 2 && ok; ++b)
-    ok = cudaMalloc(&q.cnt[b], s->ncells * sizeof(int)) == cudaSuccess &&
-         cudaMalloc(&q.orec[b], (size_t)ocap * 2 * sizeof(float4)) == cudaSuccess &&
-         cudaMalloc(&q.okey[b], (size_t)ocap * sizeof(int)) == cudaSuccess;
+    ok = dmalloc(&q.cnt[b], s->ncells * sizeof(int)) == cudaSuccess &&
+         dmalloc(&q.orec[b], (size_t)ocap * 2 * sizeof(float4)) == cudaSuccess &&
+         dmalloc(&q.okey[b], (size_t)ocap * sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     free_buckets(q);
@@ -1499,7 +1541,7 @@ int ensure_set(SimSpecies &q, int b, long long slots, cudaStream_t st) {
   SPB_CUDA(cudaStreamSynchronize(st));
   free_set(q, b);
   const long long want = std::max<long long>(slots + slots / 16, 32);
-  if (cudaMalloc(&q.rec[b], (size_t)want * 2 * sizeof(float4)) != cudaSuccess) {
+  if (dmalloc(&q.rec[b], (size_t)want * 2 * sizeof(float4)) != cudaSuccess) {
     cudaGetLastError();
     return fail(SPB_ERR_ALLOC, "bucket allocation failed (64 bytes per record slot)");
   }
@@ -1779,7 +1821,7 @@ struct Flat {
   float *buf = nullptr;
   float *p[7] = {};
   int alloc(long n) {
-    if (cudaMalloc(&buf, 7 * std::max<long>(n, 1) * sizeof(float)) != cudaSuccess) {
+    if (dmalloc(&buf, 7 * std::max<long>(n, 1) * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       return fail(SPB_ERR_ALLOC, "temporary particle arrays: allocation failed");
     }
@@ -1789,7 +1831,7 @@ struct Flat {
   void release(cudaStream_t st) {
     if (buf) {
       cudaStreamSynchronize(st);
-      cudaFree(buf);
+      dfree(buf);
       buf = nullptr;
     }
   }
@@ -1852,12 +1894,12 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
     return rc;
   };
   const long nb = ceil_div(s->ncells, SCAN_B);
-  if (cudaMalloc(&s->fields8, s->nodes * 8 * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&s->scan_tmp, (nb + 1) * sizeof(long long)) != cudaSuccess ||
-      cudaMalloc(&s->counts, s->ncells * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&s->lcap, s->ncells * sizeof(long long)) != cudaSuccess ||
-      cudaMalloc(&s->offset, (s->ncells + 1) * sizeof(long long)) != cudaSuccess) {
+  if (dmalloc(&s->fields8, s->nodes * 8 * sizeof(float)) != cudaSuccess ||
+      dmalloc(&s->d_err, sizeof(int)) != cudaSuccess ||
+      dmalloc(&s->scan_tmp, (nb + 1) * sizeof(long long)) != cudaSuccess ||
+      dmalloc(&s->counts, s->ncells * sizeof(int)) != cudaSuccess ||
+      dmalloc(&s->lcap, s->ncells * sizeof(long long)) != cudaSuccess ||
+      dmalloc(&s->offset, (s->ncells + 1) * sizeof(long long)) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(SPB_ERR_ALLOC, "spb_sim_create: device allocation failed"));
   }
@@ -1869,7 +1911,7 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
   for (int i = 0; i < d->ns; ++i) {
     SimSpecies &q = s->sp[i];
     q.qom = d->qom[i];
-    if (cudaMalloc(&q.mom, 10 * s->nodes * sizeof(double)) != cudaSuccess) {
+    if (dmalloc(&q.mom, 10 * s->nodes * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
       return bail(fail(SPB_ERR_ALLOC, "spb_sim_create: device allocation failed"));
     }
@@ -2011,17 +2053,18 @@ extern "C" void spb_sim_destroy(spb_sim *s) {
   for (cudaEvent_t e : s->gev)
     if (e) cudaEventDestroy(e);
   drain(s, nullptr, nullptr, nullptr, nullptr, nullptr);
+  cudaDeviceSynchronize();   // no queued work may still read the memory returned below
   for (auto &q : s->sp) {
     free_buckets(q);
-    cudaFree(q.mom);
+    dfree(q.mom);
   }
-  cudaFree(s->fields8);
-  cudaFree(s->stage);
-  cudaFree(s->d_err);
-  cudaFree(s->scan_tmp);
-  cudaFree(s->counts);
-  cudaFree(s->lcap);
-  cudaFree(s->offset);
+  dfree(s->fields8);
+  dfree(s->stage);
+  dfree(s->d_err);
+  dfree(s->scan_tmp);
+  dfree(s->counts);
+  dfree(s->lcap);
+  dfree(s->offset);
   delete s;
 }
 
@@ -2061,7 +2104,7 @@ extern "C" int spb_sim_set_fields(spb_sim *s, const float *const fields[6], int 
   if (on_device) {
     for (int f = 0; f < 6; ++f) src[f] = fields[f];
   } else {
-    if (!s->stage && cudaMalloc(&s->stage, 6 * s->nodes * sizeof(float)) != cudaSuccess) {
+    if (!s->stage && dmalloc(&s->stage, 6 * s->nodes * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       return fail(SPB_ERR_ALLOC, "spb_sim_set_fields: staging allocation failed");
     }

@@ -59,6 +59,7 @@ class Server:
         _lib.check(self.lib.spb_serve_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h
         self._inputs = {}   # id -> (job, pointer arrays): kept alive until admitted
+        self.release_s = 0.0   # host seconds spent releasing finished jobs
 
     def close(self):
         if self.h:
@@ -137,7 +138,16 @@ class Server:
         return out
 
     def release(self, jid: int):
+        t = time.perf_counter()
         _lib.check(self.lib.spb_serve_release(self.h, jid))
+        self.release_s += time.perf_counter() - t
+
+    def stats(self) -> dict:
+        """Steps run and host seconds per phase of the steps."""
+        t = (ctypes.c_double * 5)()
+        _lib.check(self.lib.spb_serve_stats(self.h, t))
+        return {"steps": int(t[0]), "admit_s": t[1], "check_s": t[2], "run_s": t[3],
+                "retire_s": t[4]}
 
 
 def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
@@ -170,3 +180,94 @@ def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
             server.release(jid)
             del live[jid]
     return done, time.perf_counter() - t0
+
+
+SERVING_GRIDS = ((16, 8, 8), (32, 16, 16), (64, 32, 32), (128, 64, 64))
+SERVING_GRID_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
+SERVING_PPC = (8, 27, 64, 125)
+
+
+def job_mix(n_configs=12, seed=0, max_particles_per_species=5_000_000, max_cycles=50):
+    """Seeded mix of job configurations: grid, particles per cell, 2 or 4
+    species, 1..max_cycles cycles. Particles per cell are lowered where a
+    species would exceed the cap. Returns (workload, ncycles, species) tuples."""
+    import numpy as np
+
+    from . import workload as W
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_configs):
+        g = SERVING_GRIDS[rng.choice(len(SERVING_GRIDS), p=SERVING_GRID_WEIGHTS)]
+        cells = g[0] * g[1] * g[2]
+        ppcs = [p for p in SERVING_PPC if p * cells <= max_particles_per_species] or [1]
+        ppc = int(rng.choice(ppcs))
+        ns = int(rng.choice((2, 4)))
+        wl = W.small_gem(nxc=g[0], nyc=g[1], nzc=g[2], E_amp=1e-3, seed=int(rng.integers(1 << 30)),
+                         species=W.gem_species((ppc,) * 4))
+        out.append((wl, int(rng.integers(1, max_cycles + 1)), list(range(ns))))
+    return out
+
+
+def device_jobs(configs):
+    """Jobs with inputs generated on the device (one set per configuration;
+    jobs of the same configuration share them: the engine copies inputs at
+    admission)."""
+    from .device import gen_fields, gen_particles
+    jobs = []
+    for wl, nc, species in configs:
+        fields = gen_fields(wl)
+        parts = [gen_particles(wl, s) for s in species]
+        jobs.append(Job(wl=wl, fields=fields, parts=parts, ncycles=nc, species=list(species)))
+    return jobs
+
+
+def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4)):
+    """Poisson stream of `njobs` jobs at `rate` jobs/s drawn from a seeded mix
+    of configurations. Every configuration is also run alone (its single-job
+    latency). Returns latency percentiles, slowdowns against running alone and
+    the aggregate throughput in particle-cycles per second."""
+    import numpy as np
+    configs = job_mix(n_configs, seed)
+    pool = device_jobs(configs)
+    alone = []
+    for job in pool:
+        srv = Server(tile=tile)
+        done, _ = run_stream(srv, [job], [0.0])
+        srv.close()
+        assert done[0].status == DONE
+        alone.append(done[0].latency)
+    # warm-up burst: every configuration at once, so the device memory pool has
+    # grown to a mix's footprint before the timed stream
+    srv = Server(tile=tile)
+    run_stream(srv, pool, [0.0] * len(pool))
+    srv.close()
+    rng = np.random.default_rng(seed + 1)
+    pick = rng.integers(0, len(pool), size=njobs)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=njobs))
+    arrivals -= arrivals[0]
+    jobs = [pool[i] for i in pick]
+    srv = Server(tile=tile)
+    done, wall = run_stream(srv, jobs, list(arrivals))
+    stats = srv.stats()
+    stats["release_s"] = srv.release_s
+    srv.close()
+    index = {id(j): k for k, j in enumerate(pool)}
+    ok = [d for d in done if d.status == DONE]
+    lat = np.array([d.latency for d in ok])
+    slow = np.array([d.latency / alone[index[id(d.job)]] for d in ok])
+    work = sum(d.job.particles() * d.job.ncycles for d in ok)
+    return {
+        "jobs": njobs, "completed": len(ok), "rate_jobs_per_s": rate,
+        "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
+                       "p99": 1e3 * float(np.percentile(lat, 99))},
+        "single_job_latency_ms": {"p50": 1e3 * float(np.percentile(alone, 50)),
+                                  "p99": 1e3 * float(np.percentile(alone, 99))},
+        "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
+                              "p99": float(np.percentile(slow, 99))},
+        "throughput_particle_cycles_per_s": work / wall,
+        "wall_s": wall, "engine": stats,
+        "mix": f"{n_configs} configurations: grids {list(SERVING_GRIDS)} "
+               f"(weights {list(SERVING_GRID_WEIGHTS)}), ppc from {list(SERVING_PPC)} "
+               "(capped at 5M particles per species), 2 or 4 species, 1-50 cycles, "
+               "frozen GEM fields; Poisson arrivals",
+    }
