@@ -102,6 +102,19 @@ int spb_mover_interp(struct particles *part, struct EMfield *field,
                      struct interpDensSpecies *ids, struct grid *grd,
                      struct parameters *param);
 
+/* The reference driver's moment section in one call (no single reference
+ * function: it replaces src/sputniPIC_CPU.cpp:247-259): setZeroDensities
+ * (src/InterpDensNet.cpp:113-117), interpP2G of species 0..param->ns-1 into
+ * zeroed device moments, applyBCids per species (src/BC.cpp:362-615) and
+ * sumOverSpecies (src/InterpDensNet.cpp:120-146) on the device; the species'
+ * and net host arrays are written once (rhoc of both zeroed, as
+ * setZeroDensities does). applyBCids and sumOverSpecies are bit-identical to
+ * the reference on the same deposit; the deposit is interpP2G's. */
+struct interpDensNet;
+int spb_interp_all_species(struct particles *part, struct interpDensSpecies *ids,
+                           struct interpDensNet *idn, struct grid *grd,
+                           struct parameters *param);
+
 /* Host coherence of the drop-in. COPY (default): particles are uploaded and
  * downloaded on every call, so the host arrays are always current. DEVICE:
  * particles stay in HBM between calls; the host arrays are refreshed only by

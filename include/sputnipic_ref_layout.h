@@ -13,6 +13,7 @@
  *   struct EMfield            include/EMfield.h:8-25
  *   struct grid               include/Grid.h:11-63
  *   struct interpDensSpecies  include/InterpDensSpecies.h:9-40
+ *   struct interpDensNet      include/InterpDensNet.h:9-39
  *   struct parameters         include/Parameters.h:10-235
  *
  * Precision: the reference's default PrecisionTypes (include/PrecisionTypes.h:
@@ -116,6 +117,32 @@ struct grid {
 
 struct interpDensSpecies {
   int species_ID;
+  spb_FPinterp ***rhon;
+  spb_FPinterp *rhon_flat;
+  spb_FPinterp ***rhoc;
+  spb_FPinterp *rhoc_flat;
+  spb_FPinterp ***Jx;
+  spb_FPinterp *Jx_flat;
+  spb_FPinterp ***Jy;
+  spb_FPinterp *Jy_flat;
+  spb_FPinterp ***Jz;
+  spb_FPinterp *Jz_flat;
+  spb_FPinterp ***pxx;
+  spb_FPinterp *pxx_flat;
+  spb_FPinterp ***pxy;
+  spb_FPinterp *pxy_flat;
+  spb_FPinterp ***pxz;
+  spb_FPinterp *pxz_flat;
+  spb_FPinterp ***pyy;
+  spb_FPinterp *pyy_flat;
+  spb_FPinterp ***pyz;
+  spb_FPinterp *pyz_flat;
+  spb_FPinterp ***pzz;
+  spb_FPinterp *pzz_flat;
+};
+
+/* Net densities, the sum over species (include/InterpDensNet.h). */
+struct interpDensNet {
   spb_FPinterp ***rhon;
   spb_FPinterp *rhon_flat;
   spb_FPinterp ***rhoc;

@@ -1,7 +1,7 @@
 /*
  * Prints, as JSON, the offset of every member of the boundary structs as the
  * REFERENCE's headers lay them out (include/Particles.h, EMfield.h, Grid.h,
- * InterpDensSpecies.h, Parameters.h). TEST INFRASTRUCTURE ONLY: run by
+ * InterpDensSpecies.h, InterpDensNet.h, Parameters.h). TEST INFRASTRUCTURE ONLY: run by
  * tests/golden/make_golden.py to produce tests/golden/abi_layout.json.
  */
 #include <cstddef>
@@ -10,6 +10,7 @@
 
 #include "EMfield.h"
 #include "Grid.h"
+#include "InterpDensNet.h"
 #include "InterpDensSpecies.h"
 #include "Parameters.h"
 #include "Particles.h"

@@ -69,6 +69,10 @@ class InterpDensSpecies(ctypes.Structure):
                 + [(n, P) for f in ("rhon", "rhoc") + MOMENT_NAMES[1:] for n in (f, f + "_flat")])
 
 
+class InterpDensNet(ctypes.Structure):
+    _fields_ = [(n, P) for f in ("rhon", "rhoc") + MOMENT_NAMES[1:] for n in (f, f + "_flat")]
+
+
 def _ints(*names):
     return [(n, c_int) for n in names]
 
@@ -106,7 +110,8 @@ class Parameters(ctypes.Structure):
 
 
 STRUCTS = {"particles": Particles, "EMfield": EMfield, "grid": Grid,
-           "interpDensSpecies": InterpDensSpecies, "parameters": Parameters}
+           "interpDensSpecies": InterpDensSpecies, "interpDensNet": InterpDensNet,
+           "parameters": Parameters}
 
 
 class SpbPush(ctypes.Structure):
@@ -239,6 +244,8 @@ def load():
            [P, R(c_double), R(c_double), R(c_int), R(c_double), R(c_int)])
     _proto(lib, "spb_sim_bucket_slots", c_long, [P, c_int])
     _proto(lib, "spb_sim_overflow", c_long, [P, c_int, P])
+    _proto(lib, "spb_interp_all_species", c_int,
+           [R(Particles), R(InterpDensSpecies), R(InterpDensNet), R(Grid), R(Parameters)])
     _proto(lib, "spb_serve_create", c_int, [R(ServeDesc), R(P)])
     _proto(lib, "spb_serve_destroy", None, [P])
     _proto(lib, "spb_serve_submit", c_long, [P, R(JobDesc), P, P, P, c_int])

@@ -79,11 +79,22 @@
   X(parameters, DiagnosticsOutputCycle) X(parameters, inputfile)                 \
   X(parameters, SaveDirName) X(parameters, RestartDirName) X(parameters, WaveFile)
 
+#define SPB_LAYOUT_IDN(X)                                                        \
+  X(interpDensNet, rhon) X(interpDensNet, rhon_flat) X(interpDensNet, rhoc)      \
+  X(interpDensNet, rhoc_flat) X(interpDensNet, Jx) X(interpDensNet, Jx_flat)     \
+  X(interpDensNet, Jy) X(interpDensNet, Jy_flat) X(interpDensNet, Jz)            \
+  X(interpDensNet, Jz_flat) X(interpDensNet, pxx) X(interpDensNet, pxx_flat)     \
+  X(interpDensNet, pxy) X(interpDensNet, pxy_flat) X(interpDensNet, pxz)         \
+  X(interpDensNet, pxz_flat) X(interpDensNet, pyy) X(interpDensNet, pyy_flat)    \
+  X(interpDensNet, pyz) X(interpDensNet, pyz_flat) X(interpDensNet, pzz)         \
+  X(interpDensNet, pzz_flat)
+
 #define SPB_LAYOUT_ALL(X)                                                        \
   SPB_LAYOUT_PARTICLES(X) SPB_LAYOUT_EMFIELD(X) SPB_LAYOUT_GRID(X)               \
-  SPB_LAYOUT_IDS(X) SPB_LAYOUT_PARAMETERS(X)
+  SPB_LAYOUT_IDS(X) SPB_LAYOUT_IDN(X) SPB_LAYOUT_PARAMETERS(X)
 
-#define SPB_LAYOUT_STRUCTS(S) S(particles) S(EMfield) S(grid) S(interpDensSpecies) S(parameters)
+#define SPB_LAYOUT_STRUCTS(S)                                                    \
+  S(particles) S(EMfield) S(grid) S(interpDensSpecies) S(interpDensNet) S(parameters)
 
 /* Appends `"struct.member": offset,` pairs and `"struct": sizeof` to a
  * std::string; used by both expansions. */

@@ -270,6 +270,23 @@ enum class Op { Mover, MoverV, Interp, Fused };
 // mover is per particle and the deposit adds into the same moments.
 constexpr long PIPE_CHUNK = 1L << 22;
 
+// The moment buffer of a deposit: the host arrays' values uploaded (the
+// drop-ins add into them), or zeros that stay on the device (dev_mom).
+int upload_moments(Species *sp, struct interpDensSpecies *ids, long nodes, bool dev_mom,
+                   float *hm[10], float *dm[10]) {
+  if (int rc = ensure_moments(sp, nodes)) return rc;
+  if (!dev_mom) host_moment_arrays(ids, hm);
+  for (int m = 0; m < 10; ++m) {
+    dm[m] = sp->d_mom + m * nodes;
+    if (dev_mom) continue;
+    if (!hm[m]) return fail(SPB_ERR_INVALID, "moment array is null");
+    SPB_CUDA(cudaMemcpyAsync(dm[m], hm[m], nodes * sizeof(float), cudaMemcpyHostToDevice,
+                             sp->stream));
+  }
+  if (dev_mom) SPB_CUDA(cudaMemsetAsync(sp->d_mom, 0, 10 * nodes * sizeof(float), sp->stream));
+  return SPB_OK;
+}
+
 int ensure_pipe(Species *sp) {
   for (int j = 0; j < 2; ++j) {
     if (!sp->pipe[j]) SPB_CUDA(cudaStreamCreateWithFlags(&sp->pipe[j], cudaStreamNonBlocking));
@@ -282,7 +299,7 @@ int ensure_pipe(Species *sp) {
 
 int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfield *field,
                        struct interpDensSpecies *ids, spb_grid_ctx *ctx,
-                       struct parameters *param, long n) {
+                       struct parameters *param, long n, bool dev_mom) {
   const bool moves = op != Op::Interp;
   const bool deposits = op == Op::Interp || op == Op::Fused;
   if (int rc = ensure_pipe(sp)) return rc;
@@ -305,16 +322,8 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
       if (!f[a]) return fail(SPB_ERR_INVALID, "field array is null");
     if (int rc = spb_grid_set_fields(ctx, f, 0, sp->stream)) return rc;
   }
-  if (deposits) {
-    host_moment_arrays(ids, hm);
-    if (int rc = ensure_moments(sp, nodes)) return rc;
-    for (int m = 0; m < 10; ++m) {
-      if (!hm[m]) return fail(SPB_ERR_INVALID, "moment array is null");
-      dm[m] = sp->d_mom + m * nodes;
-      SPB_CUDA(cudaMemcpyAsync(dm[m], hm[m], nodes * sizeof(float), cudaMemcpyHostToDevice,
-                               sp->stream));
-    }
-  }
+  if (deposits)
+    if (int rc = upload_moments(sp, ids, nodes, dev_mom, hm, dm)) return rc;
   SPB_CUDA(cudaEventRecord(sp->ev_in, sp->stream));
   for (int j = 0; j < 2; ++j) SPB_CUDA(cudaStreamWaitEvent(sp->pipe[j], sp->ev_in, 0));
   const PushDev p = moves ? make_push(push_of(part, param)) : PushDev{};
@@ -348,7 +357,7 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
     SPB_CUDA(cudaEventRecord(sp->ev_done[j], sp->pipe[j]));
     SPB_CUDA(cudaStreamWaitEvent(sp->stream, sp->ev_done[j], 0));
   }
-  if (deposits)
+  if (deposits && !dev_mom)
     for (int m = 0; m < 10; ++m)
       SPB_CUDA(cudaMemcpyAsync(hm[m], dm[m], nodes * sizeof(float), cudaMemcpyDeviceToHost,
                                sp->stream));
@@ -362,7 +371,7 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
 
 // The common body of the four drop-ins.
 int run(Op op, struct particles *part, struct EMfield *field, struct interpDensSpecies *ids,
-        struct grid *grd, struct parameters *param) {
+        struct grid *grd, struct parameters *param, bool dev_mom = false) {
   if (!part || !grd) return fail(SPB_ERR_INVALID, "null particles or grid");
   const bool moves = op != Op::Interp;
   const bool deposits = op == Op::Interp || op == Op::Fused;
@@ -385,7 +394,7 @@ int run(Op op, struct particles *part, struct EMfield *field, struct interpDensS
   if (int rc = ensure_capacity(sp, n)) return rc;
   const bool device_mode = S().residency == SPB_RESIDENCY_DEVICE;
   if (!device_mode && n > PIPE_CHUNK)
-    return run_copy_pipelined(op, sp, part, field, ids, ctx, param, n);
+    return run_copy_pipelined(op, sp, part, field, ids, ctx, param, n, dev_mom);
   // particles: upload unless the device copy is known to be current
   if (!device_mode || !sp->dev_current || sp->nop != n) {
     if (int rc = copy_particles(sp, part, 0, 6, true)) return rc;
@@ -400,16 +409,8 @@ int run(Op op, struct particles *part, struct EMfield *field, struct interpDensS
   const long nodes = spb_grid_nodes(ctx);
   float *hm[10] = {};
   float *dm[10] = {};
-  if (deposits) {
-    host_moment_arrays(ids, hm);
-    if (int rc = ensure_moments(sp, nodes)) return rc;
-    for (int m = 0; m < 10; ++m) {
-      if (!hm[m]) return fail(SPB_ERR_INVALID, "moment array is null");
-      dm[m] = sp->d_mom + m * nodes;
-      SPB_CUDA(cudaMemcpyAsync(dm[m], hm[m], nodes * sizeof(float), cudaMemcpyHostToDevice,
-                               sp->stream));
-    }
-  }
+  if (deposits)
+    if (int rc = upload_moments(sp, ids, nodes, dev_mom, hm, dm)) return rc;
   int rc = SPB_OK;
   if (moves) {
     // fields are shared by all species: upload, launch and completion of the
@@ -438,7 +439,7 @@ int run(Op op, struct particles *part, struct EMfield *field, struct interpDensS
     ctx->launches++;
   }
   // results back to the host
-  if (deposits)
+  if (deposits && !dev_mom)
     for (int m = 0; m < 10; ++m)
       SPB_CUDA(cudaMemcpyAsync(hm[m], dm[m], nodes * sizeof(float), cudaMemcpyDeviceToHost,
                                sp->stream));
@@ -478,6 +479,85 @@ extern "C" int spb_mover_interp(struct particles *part, struct EMfield *field,
                                 struct interpDensSpecies *ids, struct grid *grd,
                                 struct parameters *param) {
   return run(Op::Fused, part, field, ids, grd, param);
+}
+
+// The driver's moment section (src/sputniPIC_CPU.cpp:247-259) in one call:
+// setZeroDensities, interpP2G of every species into zeroed device moments,
+// applyBCids per species and sumOverSpecies on the device, then the species'
+// and net host arrays written once. Species run one after another (each on
+// its own stream, as in the drop-in interpP2G); the epilogue runs on the
+// first species' stream after all of them finished.
+extern "C" int spb_interp_all_species(struct particles *part, struct interpDensSpecies *ids,
+                                      struct interpDensNet *idn, struct grid *grd,
+                                      struct parameters *param) {
+  if (!part || !ids || !idn || !grd || !param)
+    return fail(SPB_ERR_INVALID, "spb_interp_all_species: null argument");
+  const int ns = param->ns;
+  if (ns < 1 || ns > 32) return fail(SPB_ERR_UNSUPPORTED, "spb_interp_all_species: 1..32 species");
+  if (int rc = use_device()) return rc;
+  spb_grid_ctx *ctx = nullptr;
+  if (int rc = get_grid(grd, &ctx)) return rc;
+  const long nodes = spb_grid_nodes(ctx);
+  std::vector<const float *> bases;
+  std::vector<Species *> sps(ns, nullptr);
+  for (int s = 0; s < ns; ++s) {
+    if (part[s].nop <= 0) continue;   // no particles: zero moments
+    if (int rc = run(Op::Interp, &part[s], nullptr, &ids[s], grd, param, true)) return rc;
+    if (int rc = get_species(&part[s], &sps[s])) return rc;
+    bases.push_back(sps[s]->d_mom);
+  }
+  cudaStream_t st = nullptr;
+  for (Species *sp : sps)
+    if (sp && !st) st = sp->stream;
+  const int periodic[3] = {param->PERIODICX, param->PERIODICY, param->PERIODICZ};
+  if (!ctx->d_net && cudaMalloc(&ctx->d_net, 10 * nodes * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->d_net = nullptr;
+    return fail(SPB_ERR_ALLOC, "net density allocation failed");
+  }
+  long launches = 0;
+  for (Species *sp : sps) {
+    if (!sp) continue;
+    float *dm[10];
+    for (int m = 0; m < 10; ++m) dm[m] = sp->d_mom + m * nodes;
+    if (int rc = launch_apply_bc_ids(ctx->nxn, ctx->nyn, ctx->nzn, periodic, dm, st, &launches))
+      return rc;
+  }
+  if (bases.empty()) {
+    SPB_CUDA(cudaMemsetAsync(ctx->d_net, 0, 10 * nodes * sizeof(float), st));
+  } else if (int rc = launch_sum_species(bases.data(), (int)bases.size(), nodes, ctx->d_net,
+                                         st)) {
+    return rc;
+  }
+  // host arrays: species moments, net moments, and the zeroed cell-centred rhoc
+  const size_t nb = nodes * sizeof(float);
+  const size_t cells = (size_t)grd->nxc * grd->nyc * grd->nzc;
+  float *hn[10];
+  const float *const hnet[10] = {idn->rhon_flat, idn->Jx_flat, idn->Jy_flat, idn->Jz_flat,
+                                 idn->pxx_flat, idn->pxy_flat, idn->pxz_flat, idn->pyy_flat,
+                                 idn->pyz_flat, idn->pzz_flat};
+  for (int m = 0; m < 10; ++m) {
+    hn[m] = const_cast<float *>(hnet[m]);
+    if (!hn[m]) return fail(SPB_ERR_INVALID, "net moment array is null");
+    SPB_CUDA(cudaMemcpyAsync(hn[m], ctx->d_net + m * nodes, nb, cudaMemcpyDeviceToHost, st));
+  }
+  for (int s = 0; s < ns; ++s) {
+    float *hm[10];
+    host_moment_arrays(&ids[s], hm);
+    for (int m = 0; m < 10; ++m) {
+      if (!hm[m]) return fail(SPB_ERR_INVALID, "moment array is null");
+      if (sps[s])
+        SPB_CUDA(cudaMemcpyAsync(hm[m], sps[s]->d_mom + m * nodes, nb, cudaMemcpyDeviceToHost,
+                                 st));
+      else
+        std::memset(hm[m], 0, nb);
+    }
+    if (ids[s].rhoc_flat) std::memset(ids[s].rhoc_flat, 0, cells * sizeof(float));
+  }
+  if (idn->rhoc_flat) std::memset(idn->rhoc_flat, 0, cells * sizeof(float));
+  if (st) SPB_CUDA(cudaStreamSynchronize(st));
+  ctx->launches += launches;
+  return SPB_OK;
 }
 
 // C++-linkage drop-ins: the symbols an object compiled against the

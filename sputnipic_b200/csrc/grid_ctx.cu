@@ -213,6 +213,7 @@ extern "C" void spb_grid_destroy(spb_grid_ctx *c) {
   cudaFree(c->d_eb2);
   cudaFree(c->d_stage);
   cudaFree(c->d_mom_tmp);
+  cudaFree(c->d_net);
   cudaFree(c->d_err);
   delete c;
 }

@@ -14,6 +14,9 @@ int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F
 // Whether mom[0..9] are equally spaced, as launch_plain_p2g and
 // launch_plain_mover_interp require.
 bool moments_strided(float *const mom[10]);
+// net[m*nodes + i] = sum over species s (in order) of bases[s][m*nodes + i].
+int launch_sum_species(const float *const *bases, int ns, long nodes, float *net,
+                       cudaStream_t s);
 // mom[m][i] += src[m * nodes + i].
 int launch_add_moments(const float *src, long nodes, float *const mom[10], cudaStream_t s);
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,

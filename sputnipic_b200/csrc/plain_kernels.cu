@@ -368,6 +368,25 @@ __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
 // the reference holds: periodic folds X, Y, Z, then non-periodic doubling X,
 // Y, Z. Thread t handles one (row, col) pair of the boundary planes of all
 // ten moments.
+// sumOverSpecies (src/InterpDensNet.cpp:120-146) on the device: net moment m
+// of node i = the species' values added in species order, from zero, as the
+// reference's loop does (so the float sums are bit-identical).
+constexpr int SUM_MAX_SPECIES = 32;
+struct SpeciesBases {
+  const float *b[SUM_MAX_SPECIES];   // [10][nodes] moments of each species
+};
+
+__global__ void __launch_bounds__(TPB) k_sum_species(SpeciesBases S, int ns, long nodes,
+                                                     float *__restrict__ net) {
+  const long total = 10 * nodes;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    float acc = 0.0f;
+    for (int s = 0; s < ns; ++s) acc += S.b[s][i];
+    net[i] = acc;
+  }
+}
+
 // mom[m][i] += src[m * nodes + i] (moments deposited into a contiguous buffer)
 __global__ void __launch_bounds__(TPB) k_add_moments(const float *__restrict__ src, long nodes,
                                                      Moments10 M) {
@@ -456,6 +475,18 @@ int launch_add_moments(const float *src, long nodes, float *const mom[10], cudaS
   for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
   k_add_moments<<<(unsigned)std::min<long>(ceil_div(nodes, TPB), 4096), TPB, 0, s>>>(src, nodes,
                                                                                      M);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
+int launch_sum_species(const float *const *bases, int ns, long nodes, float *net,
+                       cudaStream_t s) {
+  if (ns < 1 || ns > SUM_MAX_SPECIES) return fail(SPB_ERR_UNSUPPORTED, "1..32 species");
+  SpeciesBases S{};
+  for (int i = 0; i < ns; ++i) S.b[i] = bases[i];
+  k_sum_species<<<(unsigned)std::min<long>(ceil_div(10 * nodes, TPB), 4096), TPB, 0, s>>>(
+      S, ns, nodes, net);
   SPB_CUDA(cudaGetLastError());
   g_launches++;
   return SPB_OK;

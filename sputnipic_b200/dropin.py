@@ -146,6 +146,16 @@ def moments(ids: InterpDensSpecies) -> list:
     return [ids._arrays[n] for n in MOMENT_NAMES]
 
 
+def interp_dens_net_allocate(grd: Grid) -> "_lib.InterpDensNet":
+    """src/InterpDensNet.cpp (interp_dens_net_allocate): 10 node moments plus
+    rhoc on centres, the sums over species."""
+    idn = _lib.InterpDensNet()
+    for name in MOMENT_NAMES:
+        setattr(idn, name + "_flat", _keep(idn, name, np.zeros(nodes(grd), np.float32)))
+    idn.rhoc_flat = _keep(idn, "rhoc", np.zeros(grd.nxc * grd.nyc * grd.nzc, np.float32))
+    return idn
+
+
 def setZeroSpeciesDensities(ids: InterpDensSpecies) -> None:
     """src/InterpDensNet.cpp:40-75 for one species."""
     for a in ids._arrays.values():
@@ -180,6 +190,20 @@ def interpP2G(part: Particles, ids: InterpDensSpecies, grd: Grid,
     lib.spb_interpP2G(ctypes.byref(part), ctypes.byref(ids), ctypes.byref(grd))
     if raise_on_error:
         _lib.check(lib.spb_last_error())
+
+
+def interp_all_species(parts: list, ids: list, idn, grd: Grid, param: Parameters,
+                       raise_on_error: bool = False) -> int:
+    """The driver's moment section (src/sputniPIC_CPU.cpp:247-259) in one call:
+    zero, interpP2G every species, applyBCids per species, sumOverSpecies,
+    all on the device. param.ns must equal len(parts)."""
+    lib = _lib.load()
+    ns = len(parts)
+    assert param.ns == ns == len(ids)
+    parr = (Particles * ns)(*parts)      # copies share the caller's arrays
+    iarr = (InterpDensSpecies * ns)(*ids)
+    return _ret(lib.spb_interp_all_species(parr, iarr, ctypes.byref(idn), ctypes.byref(grd),
+                                           ctypes.byref(param)), raise_on_error)
 
 
 def mover_interp(part: Particles, field: EMfield, ids: InterpDensSpecies, grd: Grid,

@@ -354,3 +354,47 @@ def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64):
     got = np.stack([m.cpu().numpy() for m in mom]).astype(np.float64) - 0.25
     check_moments(got, np.stack(m32), absm + 0.25)
     ctx.close()
+
+
+@pytest.mark.parametrize("residency", ["copy", "device"])
+def test_interp_all_species_matches_driver_section(orc32, orc64, residency):
+    """spb_interp_all_species against the reference driver's moment section
+    (zero, interpP2G per species, applyBCids per species, sumOverSpecies) run
+    with the oracle: species moments within the reordering bound (the bound's
+    sums of |terms| go through the same linear applyBCids), net moments
+    bit-identical to the float sum of the returned species moments in species
+    order, rhoc zeroed."""
+    wl = W.small_gem(E_amp=1e-3)
+    fields = W.gem_fields(wl)
+    parts = [W.gem_particles(wl, s) for s in range(4)]
+    param, grd, field, P = build(wl, fields, [{k: p[k].copy() for k in "xyzuvwq"} for p in parts])
+    if residency == "device":
+        assert dropin.set_residency(True) == 0
+    # one mover step first, so the deposit sees moved particles
+    for s in range(4):
+        assert dropin.mover_PC(P[s], field, grd, param) == 0
+    ids = [dropin.interp_dens_species_allocate(grd, s) for s in range(4)]
+    idn = dropin.interp_dens_net_allocate(grd)
+    for i in ids:
+        i._arrays["rhoc"][...] = 7.0
+    idn._arrays["rhoc"][...] = 7.0
+    assert dropin.interp_all_species(P, ids, idn, grd, param) == 0
+    if residency == "device":
+        for s in range(4):
+            assert dropin.sync_particles_to_host(P[s]) == 0
+    setup = oracle.setup_from(wl)
+    net = np.zeros((10, wl.nodes), np.float32)
+    for s in range(4):
+        moved = dropin.particle_arrays(P[s])
+        ref = [np.zeros(wl.nodes, np.float32) for _ in range(10)]
+        orc32.interp_p2g(setup, moved, ref)
+        orc32.apply_bc_ids(setup, ref)
+        absm = list(abs_moments(orc64, setup, wl, moved))
+        orc64.apply_bc_ids(setup, absm)
+        got = np.stack(dropin.moments(ids[s]))
+        check_moments(got, np.stack(ref), np.stack(absm))
+        net = net + got
+        assert not ids[s]._arrays["rhoc"].any()
+    assert np.array_equal(np.stack(dropin.moments(idn)), net)
+    assert not idn._arrays["rhoc"].any()
+    dropin.set_residency(False)
