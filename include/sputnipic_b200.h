@@ -115,6 +115,14 @@ int spb_interp_all_species(struct particles *part, struct interpDensSpecies *ids
                            struct interpDensNet *idn, struct grid *grd,
                            struct parameters *param);
 
+/* particle_sort (src/Particles.cpp:72-234; declared in include/Particles.h)
+ * on the device: particles ordered by bin of param->sort_cps cells per axis,
+ * stably, particles outside every bin last, over all part->npmax entries, with
+ * the reference's float arithmetic for the bins (bit-identical order). Named
+ * spb_particle_sort, not particle_sort, because src/Particles.cpp, which the
+ * driver keeps, defines that symbol. */
+int spb_particle_sort(struct parameters *param, struct particles *part, struct grid *grd);
+
 /* Host coherence of the drop-in. COPY (default): particles are uploaded and
  * downloaded on every call, so the host arrays are always current. DEVICE:
  * particles stay in HBM between calls; the host arrays are refreshed only by

@@ -104,6 +104,9 @@ class CpuOracle:
         lib.orc_interp_p2g.argtypes = [ctypes.POINTER(OrcSetup)] + [_P] * 7 + [ctypes.c_long, _P]
         lib.orc_apply_bc_ids.restype = None
         lib.orc_apply_bc_ids.argtypes = [ctypes.POINTER(OrcSetup), _P]
+        lib.orc_particle_sort.restype = ctypes.c_int
+        lib.orc_particle_sort.argtypes = ([ctypes.POINTER(OrcSetup), ctypes.c_int] + [_P] * 7
+                                          + [ctypes.c_long])
         lib.orc_mover_interp.restype = ctypes.c_int
         lib.orc_mover_interp.argtypes = ([ctypes.POINTER(OrcSetup), _P] + [_P] * 7
                                          + [ctypes.c_long, ctypes.c_double, _P])
@@ -151,6 +154,12 @@ class CpuOracle:
     def apply_bc_ids(self, setup: OrcSetup, mom) -> None:
         m, keep = self._arr(mom)
         self.lib.orc_apply_bc_ids(ctypes.byref(setup), m)
+
+    def particle_sort(self, setup: OrcSetup, sort_cps: int, part: dict) -> int:
+        """particle_sort (src/Particles.cpp:72-234) in place on x..q."""
+        p = [self._chk(part[k]) for k in "xyzuvwq"]
+        return self.lib.orc_particle_sort(ctypes.byref(setup), int(sort_cps),
+                                          *[_ptr(a) for a in p], len(p[0]))
 
     def mover_interp(self, setup: OrcSetup, fields, part: dict, qom: float, mom) -> int:
         f, keepf = self._arr(fields)

@@ -424,3 +424,50 @@ int orc_num_threads(void) {
 }
 
 int orc_fp_bytes(void) { return (int)sizeof(fpp); }
+
+/* particle_sort, binned branch (src/Particles.cpp:153-233): bin counts from the
+ * grid's cell counts with guard cells (grd->nxc), bin width L / (FPpart)n_bin
+ * rounded to FPpart, bin floor(x / width) in FPpart arithmetic, index
+ * z + y*nbz + x*nbz*nby (src/Particles.cpp:67-69), particles outside every bin
+ * in a last bin; a bin keeps the particles' original order. */
+int orc_particle_sort(const orc_setup *s, int sort_cps, void *xv, void *yv, void *zv, void *uv,
+                      void *vv, void *wv, void *qv, long n) {
+  if (n <= 0) return 0;
+  if (sort_cps < 1) return -1;
+  const long ncx = s->nxc + 2, ncy = s->nyc + 2, ncz = s->nzc + 2;   /* grd->nxc */
+  const long nbx = 1 + ((ncx - 1) / sort_cps);
+  const long nby = 1 + ((ncy - 1) / sort_cps);
+  const long nbz = 1 + ((ncz - 1) / sort_cps);
+  const fpp dx = (fpp)(s->Lx / (fpp)nbx), dy = (fpp)(s->Ly / (fpp)nby),
+            dz = (fpp)(s->Lz / (fpp)nbz);
+  const long bins = nbx * nby * nbz + 1;
+  fpp *arr[6] = {(fpp *)xv, (fpp *)yv, (fpp *)zv, (fpp *)uv, (fpp *)vv, (fpp *)wv};
+  fpi *q = (fpi *)qv;
+  long *key = (long *)malloc(sizeof(long) * n);
+  long *start = (long *)calloc(bins + 1, sizeof(long));
+  fpp *tmp = (fpp *)malloc(sizeof(fpp) * n);
+  fpi *tmpq = (fpi *)malloc(sizeof(fpi) * n);
+  long *dst = (long *)malloc(sizeof(long) * n);
+  if (!key || !start || !tmp || !tmpq || !dst) {
+    free(key); free(start); free(tmp); free(tmpq); free(dst);
+    return -1;
+  }
+  for (long i = 0; i < n; i++) {
+    const fpp fx = (fpp)floor(arr[0][i] / dx), fy = (fpp)floor(arr[1][i] / dy),
+              fz = (fpp)floor(arr[2][i] / dz);
+    const int in = fx >= 0 && fx < (fpp)nbx && fy >= 0 && fy < (fpp)nby && fz >= 0 &&
+                   fz < (fpp)nbz;
+    key[i] = in ? (long)fz + (long)fy * nbz + (long)fx * nbz * nby : bins - 1;
+    start[key[i] + 1]++;
+  }
+  for (long b = 0; b < bins; b++) start[b + 1] += start[b];
+  for (long i = 0; i < n; i++) dst[i] = start[key[i]]++;   /* in index order: stable */
+  for (int a = 0; a < 6; a++) {
+    for (long i = 0; i < n; i++) tmp[dst[i]] = arr[a][i];
+    memcpy(arr[a], tmp, sizeof(fpp) * n);
+  }
+  for (long i = 0; i < n; i++) tmpq[dst[i]] = q[i];
+  memcpy(q, tmpq, sizeof(fpi) * n);
+  free(key); free(start); free(tmp); free(tmpq); free(dst);
+  return 0;
+}

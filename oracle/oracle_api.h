@@ -57,6 +57,11 @@ void orc_interp_p2g(const orc_setup *s, const void *x, const void *y,
 
 /* applyBCids on one species' moments (src/BC.cpp:362-615). */
 void orc_apply_bc_ids(const orc_setup *s, void *const mom[10]);
+/* particle_sort (src/Particles.cpp:72-234, the binned branch) over n
+ * particles: bins of sort_cps cells per axis, stable within a bin, particles
+ * outside the bins last. Returns 0, or -1 when out of memory. */
+int orc_particle_sort(const orc_setup *s, int sort_cps, void *x, void *y, void *z, void *u,
+                      void *v, void *w, void *q, long n);
 
 /* mover_interp (src/Mover.cpp:575-862): mover then deposit, per particle. */
 int orc_mover_interp(const orc_setup *s, const void *const fld[6], void *x,

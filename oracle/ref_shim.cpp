@@ -21,6 +21,7 @@
 #include "BC.h"
 #include "InterpDensNet.h"
 #include "Mover.h"
+#include "Particles.h"
 #include "oracle_api.h"
 
 namespace {
@@ -215,5 +216,17 @@ int orc_cycle(const orc_setup *s, const void *const fld[6], int ns,
 int orc_num_threads(void) { return omp_get_max_threads(); }
 
 int orc_fp_bytes(void) { return (int)sizeof(FPpart); }
+
+int orc_particle_sort(const orc_setup *s, int sort_cps, void *x, void *y, void *z, void *u,
+                      void *v, void *w, void *q, long n) {
+  if (n <= 0) return 0;
+  if (sort_cps < 1) return -1;
+  RefWorld W(s);
+  W.param.sort_cps = sort_cps;
+  particles p;
+  wrap_particles(&p, s, x, y, z, u, v, w, q, n, 0.0);
+  particle_sort(&W.param, &p, &W.grd);   // src/Particles.cpp:72-234
+  return 0;
+}
 
 }  // extern "C"

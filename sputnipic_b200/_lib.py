@@ -246,6 +246,7 @@ def load():
     _proto(lib, "spb_sim_overflow", c_long, [P, c_int, P])
     _proto(lib, "spb_interp_all_species", c_int,
            [R(Particles), R(InterpDensSpecies), R(InterpDensNet), R(Grid), R(Parameters)])
+    _proto(lib, "spb_particle_sort", c_int, [R(Parameters), R(Particles), R(Grid)])
     _proto(lib, "spb_serve_create", c_int, [R(ServeDesc), R(P)])
     _proto(lib, "spb_serve_destroy", None, [P])
     _proto(lib, "spb_serve_submit", c_long, [P, R(JobDesc), P, P, P, c_int])

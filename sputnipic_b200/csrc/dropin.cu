@@ -50,6 +50,7 @@ struct Species {
   bool dev_current = false;   // the device holds the newest particle data
   bool host_stale = false;    // the host arrays are older than the device copy
   bool q_current = false;
+  bool host_q_stale = false;  // a device-side sort permuted q too
   long nop = 0;
   std::mutex mu;
 
@@ -217,10 +218,11 @@ float *const *host_moment_arrays(const struct interpDensSpecies *ids, float *out
 }
 
 // Copies arrays [first, last) of x..q between host and device.
-int copy_particles(Species *sp, const struct particles *p, int first, int last, bool to_device) {
+int copy_particles(Species *sp, const struct particles *p, int first, int last, bool to_device,
+                   long count = -1) {
   float *h[7];
   host_particle_arrays(p, h);
-  const size_t bytes = (size_t)p->nop * sizeof(float);
+  const size_t bytes = (size_t)(count < 0 ? p->nop : count) * sizeof(float);
   for (int a = first; a < last; ++a) {
     if (!h[a]) return fail(SPB_ERR_INVALID, "particle array is null");
     if (to_device)
@@ -560,6 +562,69 @@ extern "C" int spb_interp_all_species(struct particles *part, struct interpDensS
   return SPB_OK;
 }
 
+// particle_sort (src/Particles.cpp:72-234) on the device, over all npmax
+// entries like the reference. COPY: the host arrays are uploaded, sorted and
+// downloaded. A device-resident species with npmax == nop is sorted where it
+// lies and its host arrays stay stale; otherwise its host arrays are brought
+// up to date first.
+extern "C" int spb_particle_sort(struct parameters *param, struct particles *part,
+                                 struct grid *grd) {
+  if (!param || !part || !grd) return fail(SPB_ERR_INVALID, "spb_particle_sort: null argument");
+  if (param->sort_cps < 1) return fail(SPB_ERR_INVALID, "spb_particle_sort: sort_cps < 1");
+  const long n = part->npmax;
+  if (n <= 0) return SPB_OK;
+  if (!part->x) return fail(SPB_ERR_INVALID, "particle array is null");
+  if (int rc = use_device()) return rc;
+  SortBins B;
+  const long nc[3] = {grd->nxc, grd->nyc, grd->nzc};
+  const double L[3] = {grd->Lx, grd->Ly, grd->Lz};
+  for (int a = 0; a < 3; ++a) {
+    const long nb = 1 + ((nc[a] - 1) / param->sort_cps);
+    B.nb[a] = (int)nb;
+    B.dist[a] = (float)(L[a] / (double)(float)nb);   // FPpart dist = Lx / (FPpart)n_bin
+  }
+  Species *sp = nullptr;
+  if (int rc = get_species(part, &sp)) return rc;
+  std::lock_guard<std::mutex> lk(sp->mu);
+  const bool in_place = S().residency == SPB_RESIDENCY_DEVICE && sp->host_stale &&
+                        sp->q_current && part->nop == n && sp->nop == n;
+  if (!in_place && sp->host_stale) {   // the device holds the newest particles
+    float *h[7];
+    host_particle_arrays(part, h);
+    for (int a = 0; a < (sp->host_q_stale ? 7 : 6); ++a)
+      SPB_CUDA(cudaMemcpyAsync(h[a], sp->d[a], sp->nop * sizeof(float), cudaMemcpyDeviceToHost,
+                               sp->stream));
+    SPB_CUDA(cudaStreamSynchronize(sp->stream));
+    sp->host_stale = false;
+    sp->host_q_stale = false;
+  }
+  if (int rc = ensure_capacity(sp, n)) return rc;
+  // seven temporary arrays and the sort's scratch in one allocation
+  void *block = nullptr;
+  const size_t tmp_bytes = 7 * (size_t)n * sizeof(float);
+  const size_t bytes = tmp_bytes + particle_sort_scratch_bytes(n) + 256;
+  if (cudaMalloc(&block, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SPB_ERR_ALLOC, "spb_particle_sort: scratch allocation failed");
+  }
+  float *tmp[7];
+  for (int a = 0; a < 7; ++a) tmp[a] = static_cast<float *>(block) + a * n;
+  void *scratch = static_cast<unsigned char *>(block) + ((tmp_bytes + 255) & ~size_t(255));
+  int rc = SPB_OK;
+  if (!in_place) rc = copy_particles(sp, part, 0, 7, true, n);
+  if (!rc) rc = device_particle_sort(sp->d, tmp, n, B, scratch, sp->stream);
+  if (!rc && !in_place) rc = copy_particles(sp, part, 0, 7, false, n);
+  if (!rc) SPB_CUDA(cudaStreamSynchronize(sp->stream));
+  cudaFree(block);
+  if (rc) return rc;
+  // the device copy now equals the (sorted) host arrays, or is the newest copy
+  sp->dev_current = true;
+  sp->q_current = true;
+  sp->nop = part->nop;
+  if (in_place) sp->host_q_stale = true;
+  return SPB_OK;
+}
+
 // C++-linkage drop-ins: the symbols an object compiled against the
 // reference's include/Mover.h references.
 int mover_PC(struct particles *part, struct EMfield *field, struct grid *grd,
@@ -625,9 +690,10 @@ extern "C" int spb_sync_particles_to_host(struct particles *part) {
   if (int rc = use_device()) return rc;
   if (part->nop != sp->nop)
     return fail(SPB_ERR_INVALID, "particle count changed while the device copy was newer");
-  if (int rc = copy_particles(sp, part, 0, 6, false)) return rc;
+  if (int rc = copy_particles(sp, part, 0, sp->host_q_stale ? 7 : 6, false)) return rc;
   SPB_CUDA(cudaStreamSynchronize(sp->stream));
   sp->host_stale = false;
+  sp->host_q_stale = false;
   return SPB_OK;
 }
 
@@ -639,6 +705,7 @@ extern "C" int spb_invalidate_particles(struct particles *part) {
   sp->dev_current = false;
   sp->q_current = false;
   sp->host_stale = false;
+  sp->host_q_stale = false;
   return SPB_OK;
 }
 

@@ -11,6 +11,17 @@ int launch_pack_fields(const float *const f[6], float4 *eb4, float2 *eb2, long n
 int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F, float *x,
                        float *y, float *z, float *u, float *v, float *w, long n, int *err,
                        cudaStream_t s, int bc_variant = 0);
+// particle_sort.cu: particle_sort's bins (src/Particles.cpp:158-163).
+struct SortBins {
+  int nb[3];       // bins per axis
+  float dist[3];   // bin widths, rounded to float as the reference does
+};
+size_t particle_sort_scratch_bytes(long n);
+// Sorts arr[0..6] (x, y, z, u, v, w, q; n each) by bin, stably; tmp: seven
+// arrays of n floats; scratch: particle_sort_scratch_bytes(n). Synchronises.
+int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const SortBins &B,
+                         void *scratch, cudaStream_t st);
+
 // Whether mom[0..9] are equally spaced, as launch_plain_p2g and
 // launch_plain_mover_interp require.
 bool moments_strided(float *const mom[10]);

@@ -206,6 +206,15 @@ def interp_all_species(parts: list, ids: list, idn, grd: Grid, param: Parameters
                                            ctypes.byref(param)), raise_on_error)
 
 
+def particle_sort(param: Parameters, part: Particles, grd: Grid,
+                  raise_on_error: bool = False) -> int:
+    """particle_sort (src/Particles.cpp:72-234) on the device, over npmax
+    entries, with param.sort_cps cells per bin and axis."""
+    lib = _lib.load()
+    return _ret(lib.spb_particle_sort(ctypes.byref(param), ctypes.byref(part), ctypes.byref(grd)),
+                raise_on_error)
+
+
 def mover_interp(part: Particles, field: EMfield, ids: InterpDensSpecies, grd: Grid,
                  param: Parameters, raise_on_error: bool = False) -> int:
     lib = _lib.load()

@@ -160,3 +160,28 @@ def test_restated_matches_reference_build_small_gem_cycle():
             assert np.array_equal(res[0][0][s][k], res[1][0][s][k])
     for a, b in zip(res[0][1], res[1][1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not oracle.reference_available(32) or not oracle.reference_available(64),
+                    reason="the reference build (oracle/_ref) exists where the reference tree does")
+@pytest.mark.parametrize("fp", [32, 64])
+@pytest.mark.parametrize("sort_cps", [1, 3, 8])
+def test_particle_sort_restated_equals_reference(fp, sort_cps):
+    """particle_sort restated against the reference's own, on shuffled GEM
+    particles with some outside every bin (the last bin)."""
+    wl = W.small_gem(E_amp=1e-3)
+    setup = oracle.setup_from(wl)
+    p0 = W.gem_particles(wl, 0)
+    perm = np.random.default_rng(sort_cps).permutation(len(p0["x"]))
+    p = {k: np.ascontiguousarray(p0[k][perm]) for k in "xyzuvwq"}
+    p["x"][:5] = np.float32(-1.0)
+    p["y"][5:7] = np.float32(11.0)
+    if fp == 64:
+        p = {k: v.astype(np.float64) for k, v in p.items()}
+    a = {k: v.copy() for k, v in p.items()}
+    b = {k: v.copy() for k, v in p.items()}
+    assert oracle.CpuOracle("restated", fp).particle_sort(setup, sort_cps, a) == 0
+    assert oracle.CpuOracle("reference", fp).particle_sort(setup, sort_cps, b) == 0
+    for k in "xyzuvwq":
+        assert np.array_equal(a[k], b[k]), k
+    assert not np.array_equal(a["x"], p["x"])

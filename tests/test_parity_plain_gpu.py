@@ -398,3 +398,38 @@ def test_interp_all_species_matches_driver_section(orc32, orc64, residency):
     assert np.array_equal(np.stack(dropin.moments(idn)), net)
     assert not idn._arrays["rhoc"].any()
     dropin.set_residency(False)
+
+
+@pytest.mark.parametrize("residency", ["copy", "device"])
+@pytest.mark.parametrize("sort_cps", [1, 2, 5])
+def test_particle_sort_bitexact(orc32, residency, sort_cps):
+    """spb_particle_sort against particle_sort (the oracle, itself pinned to the
+    reference's own): shuffled GEM particles, a few outside every bin,
+    identical arrays after the sort (order within a bin included). DEVICE
+    residency sorts the resident copy and syncs on request."""
+    wl = W.small_gem(E_amp=1e-3)
+    fields = W.gem_fields(wl)
+    p0 = W.gem_particles(wl, 1)
+    perm = np.random.default_rng(sort_cps).permutation(len(p0["x"]))
+    part = {k: np.ascontiguousarray(p0[k][perm]) for k in "xyzuvwq"}
+    if residency == "copy":   # outside every bin (the mover would flag them)
+        part["x"][:3] = np.float32(-0.5)
+        part["z"][3:9] = np.float32(wl.Lz + 1.0)
+    param, grd, field, P = build(wl, fields, [{k: part[k].copy() for k in "xyzuvwq"}])
+    param.sort_cps = sort_cps
+    if residency == "device":
+        # the device copy is the newest and holds q: the sort runs where it lies
+        assert dropin.set_residency(True) == 0
+        assert dropin.mover_PC(P[0], field, grd, param) == 0
+        dropin.interpP2G(P[0], dropin.interp_dens_species_allocate(grd, 1), grd,
+                         raise_on_error=True)
+        orc32.mover_pc(oracle.setup_from(wl), fields, part, wl.species[0].qom)   # allocated as species 0
+    assert dropin.particle_sort(param, P[0], grd) == 0
+    if residency == "device":
+        assert dropin.sync_particles_to_host(P[0]) == 0
+    ref = {k: part[k].copy() for k in "xyzuvwq"}
+    assert orc32.particle_sort(oracle.setup_from(wl), sort_cps, ref) == 0
+    got = dropin.particle_arrays(P[0])
+    for k in "xyzuvwq":
+        assert np.array_equal(got[k], ref[k]), k
+    dropin.set_residency(False)
