@@ -61,6 +61,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
                : "memory");
 }
 
+// Raises the barrier's expected transaction bytes without arriving: several
+// copies can be armed one by one and the phase closed by one mbar_arrive.
+__device__ __forceinline__ void mbar_expect_tx_only(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
   unsigned ok;
   asm volatile(
@@ -191,76 +203,91 @@ struct Tile {
   static_assert((SF * 4) % 128 == 0, "field stages must stay 128-byte aligned");
 };
 
-// Trilinear gather of E and B at (cell g, fraction f) per axis from the staged
-// tile. Every lane reads the tile (indices clamped into it); lanes whose 8
-// nodes lie outside the tile then re-gather from HBM/L2, a warp-uniform branch
-// that is skipped when no lane needs it. All 32 lanes must call.
-template <int TX, int TY, int TZ>
-__device__ __forceinline__ Field6 gather(const CycleParams &P, const float *__restrict__ sF,
-                                         int c0x, int c0y, int c0z, int gx, int gy, int gz,
-                                         float fx, float fy, float fz) {
-  using T = Tile<TX, TY, TZ>;
+// Trilinear gather of E and B from the node array in HBM/L2, for a particle
+// whose nodes lie outside the staged tile (rare: kept out of line, so the
+// staged gather's registers and code stay those of the common case).
+__device__ __noinline__ Field6 gather_global(const float *__restrict__ fields8, int nxc, int nyc,
+                                             int nzc, int nyn, int nzn, int gx, int gy, int gz,
+                                             float fx, float fy, float fz) {
   const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
   Field6 F = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-  const int bx = gx + 1 - c0x, by = gy + 1 - c0y, bz = gz + 1 - c0z;
-  const bool inbox = ((unsigned)bx <= (unsigned)(TX + 1)) & ((unsigned)by <= (unsigned)(TY + 1)) &
-                     ((unsigned)bz <= (unsigned)(TZ + 1));
-  {
-    const int n0 = (min(max(bx, 0), TX + 1) * T::BY + min(max(by, 0), TY + 1)) * T::BZ +
-                   min(max(bz, 0), TZ + 1);
+  const long sy = nzn, sx = (long)nyn * nzn;
+  const int hx = min(max(gx, -1), nxc), hy = min(max(gy, -1), nyc), hz = min(max(gz, -1), nzc);
+  const long n0 = (long)(hx + 1) * sx + (long)(hy + 1) * sy + (hz + 1);
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const float wab = wx[a] * wy[b];
+    for (int b = 0; b < 2; ++b) {
+      const float wab = wx[a] * wy[b];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const int n = n0 + (a * T::BY + b) * T::BZ + c;
-          const float4 A = *reinterpret_cast<const float4 *>(sF + 8 * n);
-          const float2 B = *reinterpret_cast<const float2 *>(sF + 8 * n + 4);
-          acc_node(F, wab * wz[c], A, B);
-        }
+      for (int c = 0; c < 2; ++c) {
+        const long n = n0 + a * sx + b * sy + c;
+        const float4 A = __ldg(reinterpret_cast<const float4 *>(fields8 + 8 * n));
+        const float2 B = __ldg(reinterpret_cast<const float2 *>(fields8 + 8 * n + 4));
+        acc_node(F, wab * wz[c], A, B);
       }
-  }
-  if (__any_sync(0xffffffffu, !inbox)) {
-    if (!inbox) {
-      F = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
-      const int hx = min(max(gx, -1), P.nxc), hy = min(max(gy, -1), P.nyc),
-                hz = min(max(gz, -1), P.nzc);
-      const long n0 = (long)(hx + 1) * sx + (long)(hy + 1) * sy + (hz + 1);
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          const float wab = wx[a] * wy[b];
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const long n = n0 + a * sx + b * sy + c;
-            const float4 A = __ldg(reinterpret_cast<const float4 *>(P.fields8 + 8 * n));
-            const float2 B = __ldg(reinterpret_cast<const float2 *>(P.fields8 + 8 * n + 4));
-            acc_node(F, wab * wz[c], A, B);
-          }
-        }
     }
-  }
   return F;
 }
 
-// mover_PC for one particle in cell units (src/Mover.cpp:33-157). All 32 lanes
-// of the warp must call (the gather votes).
+// Trilinear gather of E and B at fraction f per axis from the staged tile,
+// node n0 the lower corner of the particle's cell (tile node index). The two
+// x layers accumulate separately (shorter dependency chains).
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ Field6 gather(const float *__restrict__ sF, int n0, float fx, float fy,
+                                         float fz) {
+  using T = Tile<TX, TY, TZ>;
+  const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+  Field6 F[2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    F[a] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const float wab = wx[a] * wy[b];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int n = n0 + (a * T::BY + b) * T::BZ + c;
+        const float4 A = *reinterpret_cast<const float4 *>(sF + 8 * n);
+        const float2 B = *reinterpret_cast<const float2 *>(sF + 8 * n + 4);
+        acc_node(F[a], wab * wz[c], A, B);
+      }
+    }
+  }
+  return {__fadd2_rn(F[0].exy, F[1].exy), __fadd2_rn(F[0].ezbx, F[1].ezbx),
+          __fadd2_rn(F[0].byz, F[1].byz)};
+}
+
+// Tile node index of the lower corner of cell g (tile origin c0), and whether
+// all 8 nodes of the cell are staged; 0 (a valid node) when they are not.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ int tile_node(int c0x, int c0y, int c0z, int gx, int gy, int gz,
+                                         bool &inbox) {
+  using T = Tile<TX, TY, TZ>;
+  const int bx = gx + 1 - c0x, by = gy + 1 - c0y, bz = gz + 1 - c0z;
+  inbox = ((unsigned)bx <= (unsigned)(TX + 1)) & ((unsigned)by <= (unsigned)(TY + 1)) &
+          ((unsigned)bz <= (unsigned)(TZ + 1));
+  return inbox ? (bx * T::BY + by) * T::BZ + bz : 0;
+}
+
+// mover_PC for one particle in cell units (src/Mover.cpp:33-157). n0c is the
+// tile node of the particle's start cell (the first gather is there, at the
+// stored offsets), or -1 when the start cell is not known to be staged. All 32 lanes of the warp must call (the gathers vote:
+// lanes whose cell lies past the staged halo re-gather from HBM/L2).
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ void push(const CycleParams &P, const float *__restrict__ sF, int c0x,
-                                     int c0y, int c0z, float qomdt2, int &cx, int &cy, int &cz,
-                                     float &ox, float &oy, float &oz, float &u, float &v, float &w,
-                                     int &bad) {
+                                     int c0y, int c0z, int n0c, float qomdt2, int &cx, int &cy,
+                                     int &cz, float &ox, float &oy, float &oz, float &u, float &v,
+                                     float &w, int &bad) {
   float dx = 0.f, dy = 0.f, dz = 0.f;   // predicted displacement in cells
   float up = 0.f, vp = 0.f, wp = 0.f;
 #pragma unroll 1
   for (int it = 0; it < P.niter; ++it) {
     int gx = cx, gy = cy, gz = cz;
     float fx = ox, fy = oy, fz = oz;
-    if (it > 0) {   // the first gather is at the start position: (c, o) as stored
+    int n0 = n0c;
+    bool inbox = true;
+    if (it > 0) {
       locate(ox + dx, cx, P.nxc, gx, fx);
       locate(oy + dy, cy, P.nyc, gy, fy);
       locate(oz + dz, cz, P.nzc, gz, fz);
@@ -270,7 +297,12 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
         truncate_below(gz, fz);
       }
     }
-    const Field6 F = gather<TX, TY, TZ>(P, sF, c0x, c0y, c0z, gx, gy, gz, fx, fy, fz);
+    if (it > 0 || n0c < 0) n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, gx, gy, gz, inbox);
+    Field6 F = gather<TX, TY, TZ>(sF, n0, fx, fy, fz);
+    if (__any_sync(0xffffffffu, !inbox)) {
+      if (!inbox)
+        F = gather_global(P.fields8, P.nxc, P.nyc, P.nzc, P.nyn, P.nzn, gx, gy, gz, fx, fy, fz);
+    }
     const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
     const float bx = F.ezbx.y, by = F.byz.x, bz = F.byz.y;
     const float omdtsq = qomdt2 * qomdt2 * (bx * bx + by * by + bz * bz);
@@ -357,51 +389,44 @@ __device__ __forceinline__ int put_at(const SpeciesDev &S, int key, long long db
 
 // A pushed slot of 32 particles whose stores wait for their counter updates:
 // the updates are issued right after the push and consumed one slot later,
-// so their round trip overlaps the next slot's push. The records wait in a
-// per-warp shared-memory staging area (two float4 per lane).
+// so their round trip overlaps the next slot's push. The lanes are grouped by
+// destination cell; each group's lowest lane reserves the group's slots with
+// one atomic. The records wait in a per-warp shared-memory staging area (two
+// float4 per lane).
 struct Pending {
   long long dbase, dend;  // destination bucket
   int key;                // destination cell
-  int mslot;              // slot from this lane's own counter update (a particle that moved)
-  int sbase0;             // lane 0: first slot of the warp's particles that stayed
-  unsigned sm;            // lanes whose particle stayed in the bucket's cell
-  bool valid, stay;
+  int slot0;              // group leader: first slot reserved for its group
+  int leader, rank;       // this lane's group leader and rank in the group
+  bool valid;
 };
 
 // Completes a pending slot. All 32 lanes call.
 __device__ __forceinline__ void flush(const SpeciesDev &S, const Pending &p, const float4 *stage,
                                       int lane, int &lost) {
-  const int sbase = __shfl_sync(FULL, p.sbase0, 0);
-  if (p.valid) {
-    const int slot = p.stay ? sbase + __popc(p.sm & ((1u << lane) - 1u)) : p.mslot;
-    lost |= put_at(S, p.key, p.dbase, p.dend, slot, stage[lane], stage[32 + lane]);
-  }
+  const int s0 = __shfl_sync(FULL, p.slot0, p.leader);
+  if (p.valid)
+    lost |= put_at(S, p.key, p.dbase, p.dend, s0 + p.rank, stage[lane], stage[32 + lane]);
 }
 
 // Issues the counter updates of a pushed slot and stages its records. All 32
 // lanes call, after the previous slot's flush.
 __device__ __forceinline__ void issue_slot(const SpeciesDev &S, Pending &p, float4 *stage,
-                                          int key, long long b0, long long b1, int nkey,
-                                          bool valid, float4 a, float4 b, int lane) {
-  p.stay = valid & (nkey == key);
-  p.sm = __ballot_sync(FULL, p.stay);
-  p.sbase0 = 0;
-  if (lane == 0 && p.sm) p.sbase0 = atomicAdd(S.cout + key, __popc(p.sm));
-  p.mslot = 0;
+                                          int nkey, bool valid, float4 a, float4 b, int lane) {
+  const unsigned peers = __match_any_sync(FULL, valid ? nkey : -1);
+  p.leader = __ffs(peers) - 1;
+  p.rank = __popc(peers & ((1u << lane) - 1u));
+  p.slot0 = 0;
+  if (valid && lane == p.leader) p.slot0 = atomicAdd(S.cout + nkey, __popc(peers));
   p.key = nkey;
-  p.dbase = b0;
-  p.dend = b1;
-  if (valid & !p.stay) {
-    p.mslot = atomicAdd(S.cout + nkey, 1);
-    p.dbase = S.base[nkey];
-    p.dend = S.base[nkey + 1];
-  }
   p.valid = valid;
+  p.dbase = valid ? __ldg(S.base + nkey) : 0;
+  p.dend = valid ? __ldg(S.base + nkey + 1) : 0;
   stage[lane] = a;
   stage[32 + lane] = b;
 }
 
-constexpr int PCH = 32;    // records per bulk chunk of the push (1 KB)
+constexpr int RH = 128;    // records per half of a warp's record ring (4 KB)
 
 // Independent jobs (own grid, fields, species and buckets; one tile shape)
 // processed by one launch: the launch walks the concatenation of the jobs'
@@ -447,102 +472,129 @@ __device__ __forceinline__ void load_params(CycleParams *dst, const CycleParams 
 // Per-warp state of the push that lives across tiles and jobs.
 struct PushWarp {
   float4 *wrec;        // staged records of the pending slot
-  float4 *buf;         // two record chunk buffers
-  uint64_t *cbar;      // their barriers
-  unsigned phase = 0, inflight = 0;   // per buffer: next parity, copy issued
-  bool dead = false;   // a bounded wait for a record chunk ran out
+  float4 *ring;        // record ring: two halves of RH records
+  uint64_t *cbar;      // the halves' barriers
+  unsigned phase = 0, inflight = 0;   // per half: next parity, copies armed
+  bool dead = false;   // a bounded wait for records ran out
   int bad = 0, lost = 0;
 };
 
 // All species of one tile (tile-local index `tile` of the job P) on the
 // staged fields sF. All threads call.
+//
+// Each warp owns NC cells of the tile (tile-local warp + j * NW) and pushes
+// their records as one stream: slot k holds the stream's records 32k..32k+31
+// whatever their cells, so slots stay full however the counts fall. Lane 0
+// copies the cells' records into a two-half ring (bulk copies, one per cell
+// piece; a half's barrier closes after its last piece is armed); a half is
+// refilled as soon as its last slot has been read.
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const float *sF,
                                           PushWarp &W) {
   using T = Tile<TX, TY, TZ>;
   constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
+  static_assert(RH % 32 == 0, "slots must not straddle ring halves");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
   const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
-    // lane j < NC holds bucket start, capacity and particle count of the
-    // warp's j-th cell (tile-local cell warp + j * NW)
+    // lane j < NC: bucket start and particle count of the warp's j-th cell,
+    // and cp = the cell's first index in the warp's stream
     long long cb = 0;
-    int ccap = 0, cc = 0;
+    int cc = 0;
     if (lane < NC) {
       const int key = tile * T::TC + warp + lane * SIM_NW;
       cb = S.base[key];
-      ccap = (int)(S.base[key + 1] - cb);
-      cc = min(S.cin[key], ccap);
+      cc = min(S.cin[key], (int)(S.base[key + 1] - cb));
     }
-    int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
-    auto issue_next = [&]() {         // all lanes call; lane 0 copies
-      while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
-        ++pj;
-        poff = 0;
-      }
-      if (pj < NC && !W.dead) {
-        const int len = min(PCH, __shfl_sync(FULL, cc, pj) - poff);
+    int cp = cc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, cp, o);
+      if (lane >= o) cp += t;
+    }
+    const int total = __shfl_sync(FULL, cp, 31);
+    cp -= cc;
+    if (total == 0 || W.dead) continue;
+
+    int pj = 0, poff = 0, pv = 0;   // next record to copy: cell, offset, stream index
+    // Copies the next records (at most RH) into half h; all lanes call.
+    auto fill = [&](int h) {
+      const int end = min(pv + RH, total);
+      if (lane == 0) fence_proxy_async();   // the half's previous reads come first
+      while (pv < end) {
+        int cnt = __shfl_sync(FULL, cc, pj);
+        while (poff >= cnt && pj < NC - 1) {
+          ++pj;
+          poff = 0;
+          cnt = __shfl_sync(FULL, cc, pj);
+        }
+        const int n = min(cnt - poff, end - pv);
+        if (n <= 0) break;   // unreachable: the counts sum to total
         const long long b0 = __shfl_sync(FULL, cb, pj);
         if (lane == 0) {
-          fence_proxy_async();
-          mbar_expect_tx(W.cbar + nbuf, (unsigned)len * 32u);
-          bulk_load(W.buf + nbuf * PCH * 2, S.rin + 2 * (b0 + poff), (unsigned)len * 32u,
-                    W.cbar + nbuf);
+          mbar_expect_tx_only(W.cbar + h, (unsigned)n * 32u);
+          bulk_load(W.ring + 2 * (pv % (2 * RH)), S.rin + 2 * (b0 + poff), (unsigned)n * 32u,
+                    W.cbar + h);
         }
-        W.inflight |= 1u << nbuf;
-        poff += len;
-        nbuf ^= 1;
+        pv += n;
+        poff += n;
       }
+      if (lane == 0) mbar_arrive(W.cbar + h);
+      W.inflight |= 1u << h;
     };
+    fill(0);
+    if (pv < total) fill(1);
+
     Pending pend;
     pend.valid = false;
-    pend.sbase0 = 0;
-    issue_next();
-    int cbuf = 0;
-    for (int j = 0; j < NC; ++j) {
-      const int cnt = __shfl_sync(FULL, cc, j);
-      if (cnt <= 0 || W.dead) continue;
-      const long long b0 = __shfl_sync(FULL, cb, j);
-      const long long b1 = b0 + __shfl_sync(FULL, ccap, j);
-      const int lc = warp + j * SIM_NW;
-      const int key = tile * T::TC + lc;
-      const int cx0 = c0x + lc / (TY * TZ), cy0 = c0y + (lc / TZ) % TY, cz0 = c0z + lc % TZ;
+    pend.slot0 = pend.leader = pend.rank = 0;
 #pragma unroll 1
-      for (int off = 0; off < cnt; off += PCH) {
-        issue_next();   // the following chunk streams in while this one is pushed
-        const bool ok = mbar_wait_bounded(W.cbar + cbuf, (W.phase >> cbuf) & 1u);
+    for (int rv = 0; rv < total; rv += 32) {
+      const int h = (rv / RH) & 1;
+      if (rv % RH == 0) {   // first slot of half h: wait for its copies
+        const bool ok = mbar_wait_bounded(W.cbar + h, (W.phase >> h) & 1u);
         if (!__all_sync(FULL, ok)) {
           W.dead = true;
           break;
         }
-        W.phase ^= 1u << cbuf;
-        W.inflight &= ~(1u << cbuf);
-        const int len = min(PCH, cnt - off);
-        const float4 *rb = W.buf + cbuf * PCH * 2;
-#pragma unroll 1
-        for (int base = 0; base < len; base += 32) {
-          const int i = base + lane;
-          const bool valid = i < len;
-          // idle lanes of the last slot push a copy of the chunk's last
-          // particle (results discarded): one instruction stream per warp
-          const int ii = valid ? i : len - 1;
-          const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
-          int cx = cx0, cy = cy0, cz = cz0;
-          float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
-          int pbad = 0;
-          push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
-                           pbad);
-          W.bad |= valid ? pbad : 0;
-          const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
-          flush(S, pend, W.wrec, lane, W.lost);   // the previous slot's counters are back
-          __syncwarp();
-          issue_slot(S, pend, W.wrec, key, b0, b1, nkey, valid, make_float4(ox, oy, oz, a.w),
-                     make_float4(u, v, w, 0.f), lane);
-        }
-        __syncwarp();   // every lane is done with this buffer before it is refilled
-        cbuf ^= 1;
+        W.phase ^= 1u << h;
+        W.inflight &= ~(1u << h);
+      }
+      const int i = rv + lane;
+      const bool valid = i < total;
+      // idle lanes of the last slot push a copy of the stream's last particle
+      // (results discarded): one instruction stream per warp
+      const int ii = valid ? i : total - 1;
+      const float4 *rp = W.ring + 2 * (ii % (2 * RH));
+      const float4 a = rp[0], b = rp[1];
+      // the lane's cell: the last j with cp_j <= ii
+      int j = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1) {
+        const int cand = j + st;
+        const int pc = __shfl_sync(FULL, cp, cand & 31);
+        if (cand < NC && pc <= ii) j = cand;
+      }
+      const int lc = warp + j * SIM_NW;
+      const int lx = lc / (TY * TZ), ly = (lc / TZ) % TY, lz = lc % TZ;
+      const int n0c = ((lx + 1) * T::BY + (ly + 1)) * T::BZ + (lz + 1);
+      int cx = c0x + lx, cy = c0y + ly, cz = c0z + lz;
+      float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
+      int pbad = 0;
+      push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, n0c, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
+                       pbad);
+      W.bad |= valid ? pbad : 0;
+      const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
+      flush(S, pend, W.wrec, lane, W.lost);   // the previous slot's counters are back
+      __syncwarp();
+      issue_slot(S, pend, W.wrec, nkey, valid, make_float4(ox, oy, oz, a.w),
+                 make_float4(u, v, w, 0.f), lane);
+      // last slot of half h read by every lane: refill it
+      if ((rv + 32) % RH == 0 && pv < total) {
+        __syncwarp();
+        fill(h);
       }
     }
     flush(S, pend, W.wrec, lane, W.lost);
@@ -571,7 +623,8 @@ __device__ __forceinline__ void push_overflow(const CycleParams &P, const float 
       float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
       int pbad = 0;
       constexpr int FAR = -(1 << 20);
-      push<TX, TY, TZ>(P, sF, FAR, FAR, FAR, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w, pbad);
+      push<TX, TY, TZ>(P, sF, FAR, FAR, FAR, -1, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
+                       pbad);
       W.bad |= valid ? pbad : 0;
       const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
       if (valid) {
@@ -611,14 +664,14 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
   float4 *sRec = reinterpret_cast<float4 *>(sF0 + 2 * T::SF);       // NW x 64 staged records
-  float4 *sBuf = sRec + SIM_NW * 64;                                // NW x 2 x PCH records
-  CycleParams *sP = reinterpret_cast<CycleParams *>(sBuf + SIM_NW * 2 * PCH * 2);  // MULTI
+  float4 *sBuf = sRec + SIM_NW * 64;                                // NW x 2 x RH records
+  CycleParams *sP = reinterpret_cast<CycleParams *>(sBuf + SIM_NW * 2 * RH * 2);  // MULTI
   uint64_t *bar = reinterpret_cast<uint64_t *>(sP + (MULTI ? 1 : 0));   // 2 + 2 NW
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   PushWarp W;
   W.wrec = sRec + warp * 64;
-  W.buf = sBuf + warp * 2 * PCH * 2;
+  W.ring = sBuf + warp * 2 * RH * 2;
   W.cbar = bar + 2 + warp * 2;
   int *const err0 = MULTI ? J.params[0].err : P1.err;
   if (smem_addr(sF0) & 127u) {   // TMA destinations need 128-byte alignment
@@ -1355,7 +1408,7 @@ int encode_field_map(spb_sim *s) {
 template <int TX, int TY, int TZ>
 size_t push_smem(bool multi = false) {
   return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + (size_t)SIM_NW * 64 * sizeof(float4) +
-         (size_t)SIM_NW * 2 * PCH * 2 * sizeof(float4) + (multi ? sizeof(CycleParams) : 0) +
+         (size_t)SIM_NW * 2 * RH * 2 * sizeof(float4) + (multi ? sizeof(CycleParams) : 0) +
          (2 + 2 * SIM_NW) * sizeof(uint64_t);
 }
 template <int TX, int TY, int TZ>
