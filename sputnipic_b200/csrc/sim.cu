@@ -32,7 +32,6 @@
 #include "kernels.h"
 #include "sim_host.h"
 #include "sim_kernels.cuh"
-#include "warp_sum.cuh"
 
 namespace spb {
 namespace {
@@ -343,16 +342,15 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
 // Deposit terms of one particle added to 40 packed accumulators:
 // acc[node*5 + k] += W_node * (mf[k], mf[k+5]) with the moment factors
 // mf = 1, u, v, w, uu | uv, uw, vv, vw, ww, i.e. the pairs (1,uv) (u,uw)
-// (v,vv) (w,vw) (uu,ww). node = a*4 + b*2 + c, a/b/c = 1 the upper node on
-// that axis, XOR-permuted by lane bits 4/3/2 (see warp_sum80). q is folded
-// into the x weights; q = 0 adds nothing.
+// (v,vv) (w,vw) (uu,ww), in the reference order rhon, Jx, Jy, Jz, pxx | pxy,
+// pxz, pyy, pyz, pzz (src/Mover.cpp:466-570); node = a*4 + b*2 + c with
+// a/b/c = 1 the upper node on that axis. q is folded into the x weights;
+// q = 0 adds nothing.
 __device__ __forceinline__ void add_terms(float2 (&acc)[40], float q, float ox, float oy, float oz,
-                                          float u, float v, float w, int lane) {
-  const bool px = lane & 16, py = lane & 8, pz = lane & 4;
-  const float lox = 1.0f - ox, loy = 1.0f - oy, loz = 1.0f - oz;
-  const float wx0 = q * (px ? ox : lox), wx1 = q * (px ? lox : ox);
-  const float wy0 = py ? oy : loy, wy1 = py ? loy : oy;
-  const float wz0 = pz ? oz : loz, wz1 = pz ? loz : oz;
+                                          float u, float v, float w) {
+  const float wx0 = q * (1.0f - ox), wx1 = q * ox;
+  const float wy0 = 1.0f - oy, wy1 = oy;
+  const float wz0 = 1.0f - oz, wz1 = oz;
   const float2 mf[5] = {make_float2(1.0f, u * v), make_float2(u, u * w), make_float2(v, v * v),
                         make_float2(w, v * w), make_float2(u * u, w * w)};
   const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
@@ -791,102 +789,81 @@ __device__ __noinline__ void deposit_global(const CycleParams &P, const SpeciesD
   }
 }
 
-constexpr int DCH = 128;   // records per bulk chunk of the deposit (4 KB)
-
-// Per-warp state of the deposit that lives across tiles and jobs.
-struct DepWarp {
-  float4 *buf;         // two record chunk buffers
-  uint64_t *bar;       // their barriers
-  unsigned phase = 0, inflight = 0;   // per buffer: next parity, copy issued
-  bool dead = false;   // a bounded wait ran out
-};
-
-// All species of one tile (tile-local index `tile` of job P). Returns false
-// when a chunk never arrived (every thread then gets false). All threads call.
+// Threads of a deposit CTA: one per cell of the tile, in whole warps.
 template <int TX, int TY, int TZ>
-__device__ __forceinline__ bool deposit_tile(const CycleParams &P, int tile, float *sCell,
-                                             DepWarp &W) {
+__host__ __device__ constexpr int dep_tpb() {
+  return ((TX * TY * TZ + 31) / 32) * 32;
+}
+
+// Read-only 16-byte load that asks L2 to fetch the surrounding 256 bytes:
+// a lane walking its cell's bucket then finds the next records in L2.
+__device__ __forceinline__ float4 ld_rec(const float4 *p) {
+  float4 v;
+  asm("ld.global.nc.L2::256B.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p));
+  return v;
+}
+
+// All species of one tile (tile-local index `tile` of job P). Thread t owns
+// cell t of the tile: it walks the cell's bucket, accumulating the 80 terms
+// of every particle in packed FP32 registers (no cross-lane reduction), and
+// stores the cell's totals in shared memory, term-major (sCell[j * TC + t]).
+// Each node of the tile then adds up the totals of its (up to 8) cells in the
+// tile and one FP64 atomic per node and moment adds the sum into the moments.
+// All threads call.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, float *sCell) {
   using T = Tile<TX, TY, TZ>;
   constexpr int NX = TX + 1, NY = TY + 1, NZ = TZ + 1, NB = NX * NY * NZ;
-  constexpr int NC = T::TC / SIM_NW;   // cells per warp and tile
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int TC = T::TC, NT = dep_tpb<TX, TY, TZ>();
+  const int tid = threadIdx.x;
+  const bool own = tid < TC;
   const long nodes = (long)P.nxn * P.nyn * P.nzn;
-  // lane -> (corner, moments) of the warp totals (see warp_sum80)
-  const int corner = (lane >> 2) & 7, mbase = 5 * ((lane >> 1) & 1);
-  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
   const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
   const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
-    // lane j < NC holds bucket start and particle count of the warp's j-th
-    // cell (tile-local cell warp + j * NW)
-    long long cb = 0;
-    int cc = 0;
-    if (lane < NC) {
-      const int key = tile * T::TC + warp + lane * SIM_NW;
-      cb = S.base[key];
-      cc = (int)min((long long)S.cout[key], S.base[key + 1] - cb);
+    const float4 *rec = S.rout;
+    int cnt = 0;
+    if (own) {
+      const int key = tile * TC + tid;
+      const long long b0 = S.base[key];
+      cnt = (int)min((long long)S.cout[key], S.base[key + 1] - b0);
+      rec += 2 * b0;
     }
-    int pj = 0, poff = 0, nbuf = 0;   // next chunk to copy: cell, offset, buffer
-    auto issue_next = [&]() {         // all lanes call; lane 0 copies
-      while (pj < NC && poff >= __shfl_sync(FULL, cc, pj)) {
-        ++pj;
-        poff = 0;
-      }
-      if (pj < NC && !W.dead) {
-        const int len = min(DCH, __shfl_sync(FULL, cc, pj) - poff);
-        const long long b0 = __shfl_sync(FULL, cb, pj);
-        if (lane == 0) {
-          fence_proxy_async();
-          mbar_expect_tx(W.bar + nbuf, (unsigned)len * 32u);
-          bulk_load(W.buf + nbuf * DCH * 2, S.rout + 2 * (b0 + poff), (unsigned)len * 32u,
-                    W.bar + nbuf);
-        }
-        W.inflight |= 1u << nbuf;
-        poff += len;
-        nbuf ^= 1;
-      }
-    };
-    issue_next();
-    int cbuf = 0;
-    for (int j = 0; j < NC; ++j) {
-      const int cnt = __shfl_sync(FULL, cc, j);
-      float r[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-      if (cnt > 0 && !W.dead) {
-        float2 acc[40];
+    const int trips = __reduce_max_sync(FULL, cnt);
+    float2 acc[40];
 #pragma unroll
-        for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
-#pragma unroll 1
-        for (int off = 0; off < cnt; off += DCH) {
-          issue_next();   // the following chunk streams in while this one is summed
-          const bool ok = mbar_wait_bounded(W.bar + cbuf, (W.phase >> cbuf) & 1u);
-          if (!__all_sync(FULL, ok)) {
-            W.dead = true;
-            break;
-          }
-          W.phase ^= 1u << cbuf;
-          W.inflight &= ~(1u << cbuf);
-          const int len = min(DCH, cnt - off);
-          const float4 *rb = W.buf + cbuf * DCH * 2;
-#pragma unroll 1
-          for (int base = 0; base < len; base += 32) {
-            const bool valid = base + lane < len;
-            const int ii = min(base + lane, len - 1);
-            const float4 a = rb[2 * ii], b = rb[2 * ii + 1];
-            add_terms(acc, valid ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, lane);
-          }
-          __syncwarp();   // every lane is done with this buffer before it is refilled
-          cbuf ^= 1;
-        }
-        warp_sum80(acc, r, lane);
-      }
-      float *dst = sCell + (warp + j * SIM_NW) * 80 + corner * 10 + mbase;
-#pragma unroll
-      for (int k = 0; k < 5; ++k)
-        if (k >= lo && k < hi) dst[k] = r[k];
+    for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+    if (cnt > 0) {
+      a = ld_rec(rec);
+      b = ld_rec(rec + 1);
     }
-    if (__syncthreads_or(W.dead)) return false;
-    for (int idx = tid; idx < 10 * NB; idx += SIM_TPB) {
+#pragma unroll 1
+    for (int k = 0; k < trips; ++k) {
+      // the next record loads while this one is summed; lanes past their
+      // count add zero terms
+      float4 na = a, nb = b;
+      if (k + 1 < cnt) {
+        na = ld_rec(rec + 2 * (k + 1));
+        nb = ld_rec(rec + 2 * (k + 1) + 1);
+      }
+      add_terms(acc, k < cnt ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z);
+      a = na;
+      b = nb;
+    }
+    if (own) {
+#pragma unroll
+      for (int i = 0; i < 40; ++i) {
+        const int node = i / 5, k = i % 5;
+        sCell[(node * 10 + k) * TC + tid] = acc[i].x;
+        sCell[(node * 10 + k + 5) * TC + tid] = acc[i].y;
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < 10 * NB; idx += NT) {
       const int m = idx / NB, nb = idx % NB;
       const int bz = nb % NZ, by = (nb / NZ) % NY, bx = nb / (NZ * NY);
       float sum = 0.0f;
@@ -898,7 +875,7 @@ __device__ __forceinline__ bool deposit_tile(const CycleParams &P, int tile, flo
           for (int c = 0; c < 2; ++c) {
             const int lx = bx - a, ly = by - b, lz = bz - c;
             if (lx >= 0 && lx < TX && ly >= 0 && ly < TY && lz >= 0 && lz < TZ)
-              sum += sCell[((lx * TY + ly) * TZ + lz) * 80 + (a * 4 + b * 2 + c) * 10 + m];
+              sum += sCell[((a * 4 + b * 2 + c) * 10 + m) * TC + (lx * TY + ly) * TZ + lz];
           }
       if (sum != 0.0f) {
         const long g = ((long)(c0x + bx + 1) * P.nyn + (c0y + by + 1)) * P.nzn + (c0z + bz + 1);
@@ -907,7 +884,6 @@ __device__ __forceinline__ bool deposit_tile(const CycleParams &P, int tile, flo
     }
     __syncthreads();
   }
-  return true;
 }
 
 // Overflow entries of every species of job P, one by one with FP64 atomics.
@@ -916,8 +892,8 @@ __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
     const int on = min(*S.ocout, S.ocap);
-    for (long i = (long)blockIdx.x * SIM_TPB + threadIdx.x; i < on;
-         i += (long)gridDim.x * SIM_TPB) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < on;
+         i += (long)gridDim.x * blockDim.x) {
       int cx, cy, cz;
       key_cell<TX, TY, TZ>(S.okout[i], P.nty, P.ntz, cx, cy, cz);
       deposit_global(P, S, cx, cy, cz, S.oout[2 * i], S.oout[2 * i + 1]);
@@ -926,57 +902,29 @@ __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
 }
 
 // The deposit (interpP2G, src/Mover.cpp:385-572) for every species, from the
-// buckets the push wrote. One warp per cell. Each warp streams its cells'
-// buckets through two shared-memory chunk buffers with bulk copies (one chunk
-// in flight while the previous one is summed); each lane accumulates the 80
-// terms (8 nodes x 10 moments) of its particles in packed FP32 registers,
-// the warp sums them by recursive halving, and the cell's 80 totals go to
-// shared memory. Each node of the tile then adds up the totals of its (up to
-// 8) cells in the tile and one FP64 atomic per node and moment adds the sum
-// into the moments. Overflow entries deposit one by one with FP64 atomics.
+// buckets the push wrote: persistent CTAs walk the tiles, one thread per cell
+// (deposit_tile). Overflow entries deposit one by one with FP64 atomics.
 // MULTI as for k_push.
 template <int TX, int TY, int TZ, bool MULTI>
-__global__ void __launch_bounds__(SIM_TPB, 2)
+__global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(), 512 / dep_tpb<TX, TY, TZ>())
     k_deposit(const __grid_constant__ CycleParams P1, const __grid_constant__ JobTable J) {
   using T = Tile<TX, TY, TZ>;
-  static_assert(T::TC % SIM_NW == 0 && T::TC / SIM_NW <= 32,
-                "cells per warp must fit a warp's lanes");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float4 *sBuf = reinterpret_cast<float4 *>(smem_raw);                 // NW x 2 x DCH records
-  float *sCell = reinterpret_cast<float *>(sBuf + SIM_NW * 2 * DCH * 2);  // TC x 8 x 10
+  float *sCell = reinterpret_cast<float *>(smem_raw);                       // 80 x TC
   CycleParams *sP = reinterpret_cast<CycleParams *>(sCell + T::TC * 80);   // MULTI
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sP + (MULTI ? 1 : 0));    // NW x 2
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  DepWarp W;
-  W.buf = sBuf + warp * 2 * DCH * 2;
-  W.bar = bars + warp * 2;
-  if (lane == 0) {
-    mbar_init(W.bar, 1);
-    mbar_init(W.bar + 1, 1);
-  }
-  __syncthreads();
-  int *const err0 = MULTI ? J.params[0].err : P1.err;
   const int ntiles = MULTI ? J.total_tiles : P1.ntx * P1.nty * P1.ntz;
   int cur_job = -1;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    bool ok;
     if constexpr (MULTI) {
       const int job = job_of(J, tile);
       if (job != cur_job) {
+        __syncthreads();   // every thread is done with the staged parameters
         load_params(sP, J.params + job);
         cur_job = job;
       }
-      ok = deposit_tile<TX, TY, TZ>(*sP, tile - J.tile_base[job], sCell, W);
+      deposit_tile<TX, TY, TZ>(*sP, tile - J.tile_base[job], sCell);
     } else {
-      ok = deposit_tile<TX, TY, TZ>(P1, tile, sCell, W);
-    }
-    if (!ok) {
-      // a chunk never arrived: report, wait (bounded) for the copies this
-      // warp still has in flight, and give up
-      if (tid == 0) atomicOr(err0, ERRBIT_TIMEOUT);
-      for (int b = 0; b < 2; ++b)
-        if (W.inflight & (1u << b)) mbar_wait_bounded(W.bar + b, (W.phase >> b) & 1u);
-      return;
+      deposit_tile<TX, TY, TZ>(P1, tile, sCell);
     }
   }
   if constexpr (MULTI) {
@@ -1413,9 +1361,7 @@ size_t push_smem(bool multi = false) {
 }
 template <int TX, int TY, int TZ>
 size_t deposit_smem(bool multi = false) {
-  return (size_t)SIM_NW * 2 * DCH * 2 * sizeof(float4) +
-         (size_t)Tile<TX, TY, TZ>::TC * 80 * sizeof(float) + (multi ? sizeof(CycleParams) : 0) +
-         SIM_NW * 2 * sizeof(uint64_t);
+  return (size_t)Tile<TX, TY, TZ>::TC * 80 * sizeof(float) + (multi ? sizeof(CycleParams) : 0);
 }
 
 }  // namespace
@@ -1494,7 +1440,7 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
                                                       SIM_TPB,
                                                       psm) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, false>,
-                                                      SIM_TPB,
+                                                      dep_tpb<TX, TY, TZ>(),
                                                       dsm) != cudaSuccess) {
       cudaGetLastError();
       pocc = MINB;
@@ -1510,7 +1456,7 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
                                                                NoMaps{});
   SPB_CUDA(cudaGetLastError());
   ev.m = record_event(s, st);
-  k_deposit<TX, TY, TZ, false><<<dctas, SIM_TPB, dsm, st>>>(P, JobTable{});
+  k_deposit<TX, TY, TZ, false><<<dctas, dep_tpb<TX, TY, TZ>(), dsm, st>>>(P, JobTable{});
   SPB_CUDA(cudaGetLastError());
   ev.e = record_event(s, st);
   if (ev.b && ev.m && ev.e) s->ev_cycle.push_back(ev);
@@ -1777,7 +1723,7 @@ int launch_jobs_t(spb_sim *const *sims, int n, JobBuffers &B, cudaStream_t st) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, true>,
                                                       SIM_TPB, psm) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, true>,
-                                                      SIM_TPB, dsm) != cudaSuccess) {
+                                                      dep_tpb<TX, TY, TZ>(), dsm) != cudaSuccess) {
       cudaGetLastError();
       pocc = MINB;
       docc = 1;
@@ -1810,7 +1756,7 @@ int launch_jobs_t(spb_sim *const *sims, int n, JobBuffers &B, cudaStream_t st) {
   k_push<TX, TY, TZ, MINB, true><<<pctas, SIM_TPB, psm, st>>>(CUtensorMap{}, CycleParams{}, J,
                                                               maps);
   SPB_CUDA(cudaGetLastError());
-  k_deposit<TX, TY, TZ, true><<<dctas, SIM_TPB, dsm, st>>>(CycleParams{}, J);
+  k_deposit<TX, TY, TZ, true><<<dctas, dep_tpb<TX, TY, TZ>(), dsm, st>>>(CycleParams{}, J);
   SPB_CUDA(cudaGetLastError());
   g_launches += 3;
   for (int j = 0; j < n; ++j) {
