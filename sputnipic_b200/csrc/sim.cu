@@ -366,21 +366,26 @@ __device__ __forceinline__ void add_terms(float2 (&acc)[40], float q, float ox, 
   }
 }
 
+// One 32-byte record store (one 256-bit access; p 32-byte aligned).
+__device__ __forceinline__ void st_rec(float4 *p, float4 a, float4 b) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x),
+               "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
 // Stores one pushed record in slot `slot` of the bucket [dbase, dend) of cell
 // `key`, or appends it to the overflow list when the bucket is full. Returns
 // 1 if the overflow list was full too (the particle is lost; reported).
+
 __device__ __forceinline__ int put_at(const SpeciesDev &S, int key, long long dbase,
                                       long long dend, int slot, float4 a, float4 b) {
   if (dbase + slot < dend) {
-    float4 *d = S.rout + 2 * (dbase + slot);
-    d[0] = a;
-    d[1] = b;
+    st_rec(S.rout + 2 * (dbase + slot), a, b);
     return 0;
   }
   const int o = atomicAdd(S.ocout, 1);
   if (o >= S.ocap) return 1;
-  S.oout[2 * (long)o] = a;
-  S.oout[2 * (long)o + 1] = b;
+  st_rec(S.oout + 2 * (long)o, a, b);
   S.okout[o] = key;
   return 0;
 }
@@ -795,14 +800,13 @@ __host__ __device__ constexpr int dep_tpb() {
   return ((TX * TY * TZ + 31) / 32) * 32;
 }
 
-// Read-only 16-byte load that asks L2 to fetch the surrounding 256 bytes:
-// a lane walking its cell's bucket then finds the next records in L2.
-__device__ __forceinline__ float4 ld_rec(const float4 *p) {
-  float4 v;
-  asm("ld.global.nc.L2::256B.v4.f32 {%0, %1, %2, %3}, [%4];"
-      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+// Read-only 32-byte load of one particle record (one 256-bit access) that asks
+// L2 to fetch the surrounding 256 bytes: a lane walking its cell's bucket then
+// finds the next records in L2.
+__device__ __forceinline__ void ld_rec(const float4 *p, float4 &a, float4 &b) {
+  asm("ld.global.nc.L2::256B.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
       : "l"(p));
-  return v;
 }
 
 // All species of one tile (tile-local index `tile` of job P). Thread t owns
@@ -837,19 +841,13 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
 #pragma unroll
     for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-    if (cnt > 0) {
-      a = ld_rec(rec);
-      b = ld_rec(rec + 1);
-    }
+    if (cnt > 0) ld_rec(rec, a, b);
 #pragma unroll 1
     for (int k = 0; k < trips; ++k) {
       // the next record loads while this one is summed; lanes past their
       // count add zero terms
       float4 na = a, nb = b;
-      if (k + 1 < cnt) {
-        na = ld_rec(rec + 2 * (k + 1));
-        nb = ld_rec(rec + 2 * (k + 1) + 1);
-      }
+      if (k + 1 < cnt) ld_rec(rec + 2 * (k + 1), na, nb);
       add_terms(acc, k < cnt ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z);
       a = na;
       b = nb;
@@ -1313,6 +1311,13 @@ cudaError_t dmalloc(T **p, size_t bytes) {
   cudaStream_t st = pool_stream();
   cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(p), std::max<size_t>(bytes, 1), st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  // the kernels move records with 32-byte accesses and bulk copies: every
+  // array must start on (at least) a 256-byte boundary, as device
+  // allocations do
+  if (e == cudaSuccess && (reinterpret_cast<uintptr_t>(*p) & 255u)) {
+    cudaFreeAsync(*p, st);
+    e = cudaErrorMisalignedAddress;
+  }
   if (e != cudaSuccess) *p = nullptr;
   return e;
 }
