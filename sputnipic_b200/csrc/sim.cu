@@ -32,6 +32,7 @@
 #include "kernels.h"
 #include "sim_host.h"
 #include "sim_kernels.cuh"
+#include "warp_sum.cuh"
 
 namespace spb {
 namespace {
@@ -344,13 +345,16 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
 // mf = 1, u, v, w, uu | uv, uw, vv, vw, ww, i.e. the pairs (1,uv) (u,uw)
 // (v,vv) (w,vw) (uu,ww), in the reference order rhon, Jx, Jy, Jz, pxx | pxy,
 // pxz, pyy, pyz, pzz (src/Mover.cpp:466-570); node = a*4 + b*2 + c with
-// a/b/c = 1 the upper node on that axis. q is folded into the x weights;
-// q = 0 adds nothing.
+// a/b/c = 1 the upper node on that axis, XOR-permuted by bits 4/3/2 of
+// `perm` (the lane for warp_sum80, 0 for the plain order). q is folded into
+// the x weights; q = 0 adds nothing.
 __device__ __forceinline__ void add_terms(float2 (&acc)[40], float q, float ox, float oy, float oz,
-                                          float u, float v, float w) {
-  const float wx0 = q * (1.0f - ox), wx1 = q * ox;
-  const float wy0 = 1.0f - oy, wy1 = oy;
-  const float wz0 = 1.0f - oz, wz1 = oz;
+                                          float u, float v, float w, int perm) {
+  const bool px = perm & 16, py = perm & 8, pz = perm & 4;
+  const float lox = 1.0f - ox, loy = 1.0f - oy, loz = 1.0f - oz;
+  const float wx0 = q * (px ? ox : lox), wx1 = q * (px ? lox : ox);
+  const float wy0 = py ? oy : loy, wy1 = py ? loy : oy;
+  const float wz0 = pz ? oz : loz, wz1 = pz ? loz : oz;
   const float2 mf[5] = {make_float2(1.0f, u * v), make_float2(u, u * w), make_float2(v, v * v),
                         make_float2(w, v * w), make_float2(u * u, w * w)};
   const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
@@ -809,6 +813,29 @@ __device__ __forceinline__ void ld_rec(const float4 *p, float4 &a, float4 &b) {
       : "l"(p));
 }
 
+// Per-warp quota of the deposit (all 32 lanes call with their cell's count):
+// lanes sum at most Q particles of their own cell, one particle per lane per
+// step; the excess of the cells above Q is summed by the whole warp, 32
+// particles per step plus one warp reduction per cell. Q minimises the
+// estimated issue slots, 60 per lane step and 65 per warp step + 160 per
+// excess cell, over the candidates Q = one of the lanes' counts; a warp whose
+// largest count is at most 1.25 x its mean keeps Q = its largest count.
+__device__ __forceinline__ int deposit_quota(int cnt) {
+  const int mx = __reduce_max_sync(FULL, cnt);
+  if (mx > (1 << 24)) return mx;   // keeps the cost sums below 2^32
+  const int sum = __reduce_add_sync(FULL, cnt);
+  if ((long long)mx * 32 * 4 <= (long long)sum * 5) return mx;   // max <= 1.25 x mean
+  unsigned cost = 60u * (unsigned)cnt;
+#pragma unroll 4
+  for (int i = 0; i < 32; ++i) {
+    const int c = __shfl_sync(FULL, cnt, i);
+    if (c > cnt) cost += 65u * (unsigned)((c - cnt + 31) >> 5) + 160u;
+  }
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned best = __reduce_min_sync(FULL, (min(cost, (1u << 26) - 1) << 5) | lane);
+  return __shfl_sync(FULL, cnt, (int)(best & 31u));
+}
+
 // All species of one tile (tile-local index `tile` of job P). Thread t owns
 // cell t of the tile: it walks the cell's bucket, accumulating the 80 terms
 // of every particle in packed FP32 registers (no cross-lane reduction), and
@@ -836,19 +863,23 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
       cnt = (int)min((long long)S.cout[key], S.base[key + 1] - b0);
       rec += 2 * b0;
     }
-    const int trips = __reduce_max_sync(FULL, cnt);
+    // quota: each lane sums at most Q particles of its own cell; the rest of
+    // the few cells above Q is summed by the whole warp afterwards
+    const int Q = deposit_quota(cnt);
+    const int n1 = min(cnt, Q);
+    const int trips = __reduce_max_sync(FULL, n1);
     float2 acc[40];
 #pragma unroll
     for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-    if (cnt > 0) ld_rec(rec, a, b);
+    if (n1 > 0) ld_rec(rec, a, b);
 #pragma unroll 1
     for (int k = 0; k < trips; ++k) {
       // the next record loads while this one is summed; lanes past their
       // count add zero terms
       float4 na = a, nb = b;
-      if (k + 1 < cnt) ld_rec(rec + 2 * (k + 1), na, nb);
-      add_terms(acc, k < cnt ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z);
+      if (k + 1 < n1) ld_rec(rec + 2 * (k + 1), na, nb);
+      add_terms(acc, k < n1 ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, 0);
       a = na;
       b = nb;
     }
@@ -858,6 +889,37 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
         const int node = i / 5, k = i % 5;
         sCell[(node * 10 + k) * TC + tid] = acc[i].x;
         sCell[(node * 10 + k + 5) * TC + tid] = acc[i].y;
+      }
+    }
+    // the cells above the quota: particles Q.. of each, one per lane, summed
+    // by the warp (warp_sum80) and added to the cell's totals
+    unsigned heavy = __ballot_sync(FULL, cnt > Q);
+    if (heavy) {
+      __syncwarp();
+      const int lane = tid & 31, wbase = tid & ~31;
+      const int corner = (lane >> 2) & 7, mbase = 5 * ((lane >> 1) & 1);
+      const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+      while (heavy) {
+        const int hl = __ffs(heavy) - 1;
+        heavy &= heavy - 1;
+        const int hc = __shfl_sync(FULL, cnt, hl);
+        const float4 *hrec = reinterpret_cast<const float4 *>(
+            __shfl_sync(FULL, reinterpret_cast<unsigned long long>(rec), hl));
+#pragma unroll
+        for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
+#pragma unroll 1
+        for (int o = Q; o < hc; o += 32) {
+          const int i = o + lane;
+          float4 ha = make_float4(0.f, 0.f, 0.f, 0.f), hb = ha;
+          if (i < hc) ld_rec(hrec + 2 * i, ha, hb);
+          add_terms(acc, i < hc ? ha.w : 0.0f, ha.x, ha.y, ha.z, hb.x, hb.y, hb.z, lane);
+        }
+        float r[5];
+        warp_sum80(acc, r, lane);
+        float *dst = sCell + (corner * 10 + mbase) * TC + wbase + hl;
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          if (k >= lo && k < hi) dst[k * TC] += r[k];
       }
     }
     __syncthreads();
