@@ -491,7 +491,7 @@ def main():
                     help="cycles between overflow checks (a species using its overflow "
                          "list is re-laid out)")
     ap.add_argument("--variant", type=int, default=0,
-                    help="push kernel residency: 0 two CTAs per SM, 1 three, 2 four")
+                    help="push kernel residency: 0 three CTAs per SM, 1 two, 2 four")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the tile shape and push variant first (timed on this workload)")
     ap.add_argument("--no-graph", action="store_true",

@@ -230,9 +230,10 @@ typedef struct spb_sim_desc {
   int resort_every;         /* cycles between overflow checks (>= 1): a species
                                whose overflow list is in use is re-laid out */
   int ctas;                 /* persistent CTAs of the push (0: per variant) */
-  int variant;              /* push kernel residency: 0 two CTAs per SM (up to
-                               128 registers), 1 three (up to 80), 2 four
-                               (up to 64) */
+  int variant;              /* push kernel residency: 0 three CTAs per SM (up
+                               to 80 registers, 2 KB record-ring halves),
+                               1 two (up to 128, 4 KB halves), 2 four (up to
+                               64, 2 KB halves) */
   int bucket_slots;         /* record slots of every cell's bucket (0: each
                                cell's count at the last layout + max(16,
                                count/4), rounded up to 4) */

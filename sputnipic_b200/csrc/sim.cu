@@ -122,13 +122,22 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
 // push in cell units
 // ---------------------------------------------------------------------------
 
+// floor(p) for |p| < 2^22 as a float (s) and an int, from one add rounded
+// toward -infinity against 1.5 * 2^23 (whose neighbours are the integers):
+// full-rate adds instead of a rounding instruction and a conversion.
+__device__ __forceinline__ int floor_split(float p, float &s) {
+  constexpr float M = 12582912.0f;   // 1.5 * 2^23
+  const float t = __fadd_rd(p, M);
+  s = t - M;
+  return __float_as_int(t) - __float_as_int(M);
+}
+
 // Gather cell and fraction of a predicted position p (cells, relative to the
-// particle's cell c), rounding down. Cells outside [-1, N] are left to the
-// gather's bounds handling.
-__device__ __forceinline__ void locate(float p, int c, int N, int &g, float &f) {
-  const float lim = (float)(N + 8);
-  const float s = fminf(fmaxf(floorf(p), -lim), lim);
-  g = c + __float2int_rz(s);
+// particle's cell c), rounding down; |p| is clamped to lim = N + 8. Cells
+// outside [-1, N] are left to the gather's bounds handling.
+__device__ __forceinline__ void locate(float p, int c, float lim, int &g, float &f) {
+  float s;
+  g = c + floor_split(fminf(fmaxf(p, -lim), lim), s);
   f = p - s;
 }
 
@@ -166,12 +175,12 @@ __device__ __forceinline__ void bc_cell(int &c, float &o, float &vel, int N, int
   o = top ? 1.0f : o;
 }
 
-// Final position update on one axis: p = o + displacement, new cell and offset.
-__device__ __forceinline__ void advance(int &c, float &o, float disp, int N) {
-  const float lim = (float)(N + 8);
+// Final position update on one axis: p = o + displacement, new cell and offset
+// (|p| clamped to lim = N + 8 for the cell).
+__device__ __forceinline__ void advance(int &c, float &o, float disp, float lim) {
   const float p = o + disp;
-  const float s = fminf(fmaxf(floorf(p), -lim), lim);
-  c += __float2int_rz(s);
+  float s;
+  c += floor_split(fminf(fmaxf(p, -lim), lim), s);
   o = p - s;
   const bool wrap = o >= 1.0f;
   c = wrap ? c + 1 : c;
@@ -288,9 +297,9 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
     int n0 = n0c;
     bool inbox = true;
     if (it > 0) {
-      locate(ox + dx, cx, P.nxc, gx, fx);
-      locate(oy + dy, cy, P.nyc, gy, fy);
-      locate(oz + dz, cz, P.nzc, gz, fz);
+      locate(ox + dx, cx, P.lim[0], gx, fx);
+      locate(oy + dy, cy, P.lim[1], gy, fy);
+      locate(oz + dz, cz, P.lim[2], gz, fz);
       if (__any_sync(0xffffffffu, (gx | gy | gz) < 0)) {   // some lane is below the domain
         truncate_below(gx, fx);
         truncate_below(gy, fy);
@@ -321,9 +330,9 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   u = 2.0f * up - u;
   v = 2.0f * vp - v;
   w = 2.0f * wp - w;
-  advance(cx, ox, up * P.fdt[0], P.nxc);
-  advance(cy, oy, vp * P.fdt[1], P.nyc);
-  advance(cz, oz, wp * P.fdt[2], P.nzc);
+  advance(cx, ox, up * P.fdt[0], P.lim[0]);
+  advance(cy, oy, vp * P.fdt[1], P.lim[1]);
+  advance(cz, oz, wp * P.fdt[2], P.lim[2]);
   // the particle BC, the range flag and the clamps change nothing for a
   // particle whose new cell is inside the domain: skipped unless some lane
   // needs them
@@ -433,7 +442,12 @@ __device__ __forceinline__ void issue_slot(const SpeciesDev &S, Pending &p, floa
   stage[32 + lane] = b;
 }
 
-constexpr int RH = 128;    // records per half of a warp's record ring (4 KB)
+// Records per half of a warp's record ring: 4 KB at two resident CTAs per SM,
+// 2 KB at three or more (so that three CTAs fit in shared memory).
+template <int MINB>
+__host__ __device__ constexpr int ring_half() {
+  return MINB >= 3 ? 64 : 128;
+}
 
 // Independent jobs (own grid, fields, species and buckets; one tile shape)
 // processed by one launch: the launch walks the concatenation of the jobs'
@@ -495,7 +509,7 @@ struct PushWarp {
 // copies the cells' records into a two-half ring (bulk copies, one per cell
 // piece; a half's barrier closes after its last piece is armed); a half is
 // refilled as soon as its last slot has been read.
-template <int TX, int TY, int TZ>
+template <int TX, int TY, int TZ, int RH>
 __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const float *sF,
                                           PushWarp &W) {
   using T = Tile<TX, TY, TZ>;
@@ -666,6 +680,7 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
     k_push(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P1,
            const __grid_constant__ JobTable J, const __grid_constant__ MapsOf<MULTI> M) {
   using T = Tile<TX, TY, TZ>;
+  constexpr int RH = ring_half<MINB>();
   static_assert(T::TC % SIM_NW == 0 && T::TC / SIM_NW <= 32,
                 "cells per warp must fit a warp's lanes");
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -746,10 +761,10 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
         load_params(sP, J.params + job);
         cur_job = job;
       }
-      push_tile<TX, TY, TZ>(*sP, local, sF, W);
+      push_tile<TX, TY, TZ, RH>(*sP, local, sF, W);
       report(*sP, W);
     } else {
-      push_tile<TX, TY, TZ>(P1, local, sF, W);
+      push_tile<TX, TY, TZ, RH>(P1, local, sF, W);
     }
     // every warp is done with this field stage (and the staged parameters)
     // before they are refilled
@@ -1420,10 +1435,11 @@ int encode_field_map(spb_sim *s) {
 
 // Dynamic shared memory of the kernels; the multi-job kernels also stage one
 // job's parameters.
-template <int TX, int TY, int TZ>
+template <int TX, int TY, int TZ, int MINB>
 size_t push_smem(bool multi = false) {
   return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + (size_t)SIM_NW * 64 * sizeof(float4) +
-         (size_t)SIM_NW * 2 * RH * 2 * sizeof(float4) + (multi ? sizeof(CycleParams) : 0) +
+         (size_t)SIM_NW * 2 * ring_half<MINB>() * 2 * sizeof(float4) +
+         (multi ? sizeof(CycleParams) : 0) +
          (2 + 2 * SIM_NW) * sizeof(uint64_t);
 }
 template <int TX, int TY, int TZ>
@@ -1451,6 +1467,7 @@ CycleParams make_params(spb_sim *s) {
     P.periodic[a] = s->d.periodic[a] ? 1 : 0;
     P.hdt[a] = (float)(0.5 * s->d.dt / s->dxyz[a]);
     P.fdt[a] = (float)(s->d.dt / s->dxyz[a]);
+    P.lim[a] = (float)(s->N[a] + 8);
   }
   P.scale = 1.0 / (s->dxyz[0] * s->dxyz[1] * s->dxyz[2]);
   P.fields8 = s->fields8;
@@ -1490,7 +1507,7 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
     SPB_CUDA(cudaMemsetAsync(q.cnt[1 - q.cur], 0, s->ncells * sizeof(int), st));
     SPB_CUDA(cudaMemsetAsync(q.ocnt + (1 - q.cur), 0, sizeof(int), st));
   }
-  const size_t psm = push_smem<TX, TY, TZ>(), dsm = deposit_smem<TX, TY, TZ>();
+  const size_t psm = push_smem<TX, TY, TZ, MINB>(), dsm = deposit_smem<TX, TY, TZ>();
   static bool attr = false;
   if (!attr) {
     SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, false>,
@@ -1536,9 +1553,9 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
 template <int TX, int TY, int TZ>
 int launch_cycle(spb_sim *s, cudaStream_t st) {
   switch (s->d.variant) {
-    case 1: return launch_cycle_v<TX, TY, TZ, 3>(s, st);
+    case 1: return launch_cycle_v<TX, TY, TZ, 2>(s, st);
     case 2: return launch_cycle_v<TX, TY, TZ, 4>(s, st);
-    default: return launch_cycle_v<TX, TY, TZ, 2>(s, st);
+    default: return launch_cycle_v<TX, TY, TZ, 3>(s, st);
   }
 }
 
@@ -1779,8 +1796,8 @@ int ensure_job_buffers(JobBuffers &B, int n) {
 
 template <int TX, int TY, int TZ>
 int launch_jobs_t(spb_sim *const *sims, int n, JobBuffers &B, cudaStream_t st) {
-  constexpr int MINB = 2;
-  const size_t psm = push_smem<TX, TY, TZ>(true), dsm = deposit_smem<TX, TY, TZ>(true);
+  constexpr int MINB = 3;
+  const size_t psm = push_smem<TX, TY, TZ, MINB>(true), dsm = deposit_smem<TX, TY, TZ>(true);
   static int pocc = 0, docc = 0;
   if (!pocc) {
     SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, true>,
