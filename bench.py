@@ -349,7 +349,13 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
     _lib.load()
-    wl = R.rank_workload(W.gem(), rank)
+    base = W.gem()
+    if tuple(args.grid) != (base.nxc, base.nyc, base.nzc):
+        # smaller profiling grid with the benchmark's cell size
+        g = args.grid
+        base = base.with_(nxc=g[0], nyc=g[1], nzc=g[2], Lx=base.Lx * g[0] / base.nxc,
+                          Ly=base.Ly * g[1] / base.nyc, Lz=base.Lz * g[2] / base.nzc)
+    wl = R.rank_workload(base, rank)
     if args.nspecies != 4 or args.ppc != 125:
         wl = wl.with_(lattice=5 if args.ppc == 125 else 0,
                       species=W.gem_species((args.ppc,) * 4)[:args.nspecies])
@@ -486,6 +492,9 @@ def main():
                     help="smaller profiling cases only; the benchmark uses all 4")
     ap.add_argument("--ppc", type=float, default=125,
                     help="smaller profiling cases only; the benchmark uses 125")
+    ap.add_argument("--grid", type=int, nargs=3, default=[128, 64, 64],
+                    help="smaller profiling cases only (same cell size); the benchmark "
+                         "uses 128 64 64")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--resort", type=int, default=4,
                     help="cycles between overflow checks (a species using its overflow "
