@@ -389,6 +389,10 @@ def run_ours(args, rank, world, local_rank):
         serving = measure_stream(rate=args.serve_rate, njobs=args.serve_jobs)
         torch.cuda.empty_cache()
 
+    hat = None
+    if not args.no_hat:
+        hat = measure_hat(torch, wl)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, n, kind, cores = time_cpu(wl, args.cpu_slabs, 3, 1, min_seconds=10.0)
@@ -423,9 +427,43 @@ def run_ours(args, rank, world, local_rank):
             "plain": None if plain is None else {
                 "value": plain["value"], "unit": UNIT, "ms_per_step": plain["ms_per_step"],
                 "kernels": plain["kernels"], "speedup_of_precision_form": value / plain["value"]},
-            "e2e": e2e, "cpu_baseline": cpu, "serving": serving,
+            "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "hat_densities": hat,
         }
         print(json.dumps(line), flush=True)
+
+
+def measure_hat(torch, wl, reps=10, warmup=3):
+    """calculateHatDensities (src/MaxwellSolver.cpp:465-603) on the workload's
+    grid in FP64 (the precision form's moment type), device arrays, timed with
+    CUDA events over `reps` calls after `warmup`. Algorithmic bytes: the
+    species' J and pressure arrays, B and rho_c read once, J hat and rho hat
+    written once."""
+    from sputnipic_b200.hat import hat_desc, hat_densities
+    ns = len(wl.species)
+    mom, fields, rhoc = W.hat_inputs(wl, seed=11, dtype=np.float64)
+    T = lambda a: torch.from_numpy(a).cuda()  # noqa: E731
+    dmom = [[T(a) for a in sp] for sp in mom]
+    dB = [T(f) for f in fields[3:]]
+    drho = T(rhoc)
+    desc = hat_desc(wl, 1.0, fp=64)
+    for _ in range(warmup):
+        hat_densities(desc, dmom, dB, drho)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(reps):
+        hat_densities(desc, dmom, dB, drho)
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / reps
+    cells = (wl.nxc + 2) * (wl.nyc + 2) * (wl.nzc + 2)
+    algo = 8 * ((9 * ns + 3 + 3) * wl.nodes + 2 * cells)
+    peak = peaks()[0]
+    achieved = algo / (ms * 1e-3) / 1e9
+    return {"ms": ms, "species": ns, "dtype": "f64", "algorithmic_bytes": algo,
+            "achieved_gbs": achieved, "frac": achieved / peak, "launches": 3 * ns + 3,
+            "note": "bit-identical to the reference's FP64 build; per species a divergence, "
+                    "a guard-cell fill and a node pass, then three launches for rho hat"}
 
 
 def run_e2e(args, wl, host_parts, host_f, world, dist):
@@ -510,6 +548,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=10.0, help="serving arrivals, jobs/s")
     ap.add_argument("--serve-jobs", type=int, default=100, help="jobs in the serving stream")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-hat", action="store_true",
+                    help="skip the calculateHatDensities measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

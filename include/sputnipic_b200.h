@@ -123,6 +123,43 @@ int spb_interp_all_species(struct particles *part, struct interpDensSpecies *ids
  * driver keeps, defines that symbol. */
 int spb_particle_sort(struct parameters *param, struct particles *part, struct grid *grd);
 
+/* calculateHatDensities (src/MaxwellSolver.cpp:465-603; declared in
+ * include/MaxwellSolver.h:37-40), the field solver's first consumer of the
+ * moments: J hat on the nodes (the divergence of each species' pressure tensor
+ * scaled by -dt/2 and interpolated to the nodes, plus its J, rotated with the
+ * species' qom dt B / 2c and summed over species; node guards filled as
+ * applyBCscalarDensN) and rho hat = rho_c - dt theta div(J hat) on the cell
+ * centres (guards filled as applyBCscalarDensC). Bit-identical to the
+ * reference's FP32 build (and, with double arrays, its FP64 build).
+ *
+ * spb_calculateHatDensities is the drop-in over the reference's host structs
+ * (reads ids[0..param->ns-1] J and pressures, field->B*n, idn->rhoc; writes
+ * id_aux->Jxh/Jyh/Jzh/rhoh); the C++-linkage calculateHatDensities below
+ * has the reference's signature. The spb_hat_densities_* entry points work
+ * on device arrays: mom holds ns*10 device pointers (species-major, the
+ * interpP2G moment order; entries 1..9 are read), B the three magnetic
+ * field node arrays, rhoc the centre array [nxc][nyc][nzc] (guards
+ * included); outputs as the drop-in's. Asynchronous on `stream`. */
+struct interpDens_aux;
+#define SPB_HAT_MAX_SPECIES 16
+typedef struct spb_hat_desc {
+  int nxc, nyc, nzc;           /* cells per axis, guard cells included (grid.nxc) */
+  double invdx, invdy, invdz;  /* the grid's inverse spacings (grid.invdx) */
+  int periodic[3];             /* param.PERIODICX/Y/Z */
+  double dt, c, th;            /* param.dt, param.c, param.th */
+  int ns;                      /* species, 1..SPB_HAT_MAX_SPECIES */
+  double qom[SPB_HAT_MAX_SPECIES];
+} spb_hat_desc;
+int spb_calculateHatDensities(struct interpDens_aux *id_aux, struct interpDensNet *idn,
+                              struct interpDensSpecies *ids, struct EMfield *field,
+                              struct grid *grd, struct parameters *param);
+int spb_hat_densities_f32(const spb_hat_desc *d, const float *const *mom,
+                          const float *const B[3], const float *rhoc, float *jxh, float *jyh,
+                          float *jzh, float *rhoh, void *stream);
+int spb_hat_densities_f64(const spb_hat_desc *d, const double *const *mom,
+                          const double *const B[3], const double *rhoc, double *jxh,
+                          double *jyh, double *jzh, double *rhoh, void *stream);
+
 /* Host coherence of the drop-in. COPY (default): particles are uploaded and
  * downloaded on every call, so the host arrays are always current. DEVICE:
  * particles stay in HBM between calls; the host arrays are refreshed only by
@@ -441,6 +478,9 @@ void interpP2G(struct particles *part, struct interpDensSpecies *ids,
 int mover_interp(struct particles *part, struct EMfield *field,
                  struct interpDensSpecies *ids, struct grid *grd,
                  struct parameters *param);
+void calculateHatDensities(struct interpDens_aux *id_aux, struct interpDensNet *idn,
+                           struct interpDensSpecies *ids, struct EMfield *field,
+                           struct grid *grd, struct parameters *param);
 #endif
 
 #endif /* SPUTNIPIC_B200_H */

@@ -167,6 +167,16 @@ struct interpDensNet {
   spb_FPinterp *pzz_flat;
 };
 
+/* Implicit-source densities of the field solver (include/InterpDens_aux.h:
+ * 6-13): rho hat on the cell centres, J hat on the nodes, each a 3-level
+ * pointer over one contiguous block (newArr3). */
+struct interpDens_aux {
+  spb_FPinterp ***rhoh;
+  spb_FPinterp ***Jxh;
+  spb_FPinterp ***Jyh;
+  spb_FPinterp ***Jzh;
+};
+
 struct parameters {
   double c;
   double fourpi;

@@ -114,6 +114,9 @@ class CpuOracle:
         lib.orc_cycle.argtypes = ([ctypes.POINTER(OrcSetup), _P, ctypes.c_int] + [_P] * 7
                                   + [_P, _P, _P, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_double)])
+        lib.orc_hat_densities.restype = ctypes.c_int
+        lib.orc_hat_densities.argtypes = ([ctypes.POINTER(OrcSetup), ctypes.c_double, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)] + [_P] * 7)
         lib.orc_num_threads.restype = ctypes.c_int
         lib.orc_fp_bytes.restype = ctypes.c_int
         assert lib.orc_fp_bytes() * 8 == fp
@@ -167,6 +170,25 @@ class CpuOracle:
         p = [self._chk(part[k]) for k in "xyzuvwq"]
         return self.lib.orc_mover_interp(ctypes.byref(setup), f, *[_ptr(a) for a in p],
                                          len(p[0]), float(qom), m)
+
+    def hat_densities(self, setup: OrcSetup, th: float, qom, mom, fields, rhoc):
+        """calculateHatDensities (src/MaxwellSolver.cpp:465-603). mom: list of
+        ns lists of 10 node arrays; fields: the six node arrays; rhoc: the
+        cell-centre net charge density (flat, guard cells included). Returns
+        (Jxh, Jyh, Jzh, rhoh) as new arrays."""
+        ns = len(mom)
+        m, keepm = self._arr([a for sp in mom for a in sp])
+        f, keepf = self._arr(fields)
+        rc = self._chk(rhoc)
+        nodes = len(fields[0])
+        out = [np.empty(nodes, dtype=self.dtype) for _ in range(3)]
+        out.append(np.empty(len(rc), dtype=self.dtype))
+        q = (ctypes.c_double * ns)(*[float(x) for x in qom])
+        r = self.lib.orc_hat_densities(ctypes.byref(setup), float(th), ns, q, m, f, _ptr(rc),
+                                       *[_ptr(a) for a in out])
+        if r != 0:
+            raise RuntimeError(f"orc_hat_densities failed: {r}")
+        return tuple(out)
 
     def cycle(self, setup: OrcSetup, fields, species: list, mom):
         """One driver cycle over ``species`` (list of particle dicts with a

@@ -11,6 +11,7 @@
 #include "EMfield.h"
 #include "Grid.h"
 #include "InterpDensNet.h"
+#include "InterpDens_aux.h"
 #include "InterpDensSpecies.h"
 #include "Parameters.h"
 #include "Particles.h"

@@ -471,3 +471,205 @@ int orc_particle_sort(const orc_setup *s, int sort_cps, void *xv, void *yv, void
   free(key); free(start); free(tmp); free(tmpq); free(dst);
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * calculateHatDensities (src/MaxwellSolver.cpp:465-603): the implicit
+ * sources J-hat (nodes) and rho-hat (cell centres) from the species moments.
+ * ---------------------------------------------------------------------- */
+
+/* Guard-cell fill of one scalar array of n0 x n1 x n2 points
+ * (applyBCscalarDensC, src/BC.cpp:623-727, and applyBCscalarDensN,
+ * src/BC.cpp:11-121). Phases in the reference order: periodic faces X, Y, Z;
+ * edges along X, Y, Z; corners; then non-periodic faces X, Y, Z, which copy
+ * the neighbouring plane. A periodic face copies from index n-1-s to 0 and
+ * from s to n-1, with s = 1 on centres and 2 on nodes. yhi is the end of the
+ * Y-edge loop (the centre version runs it to nyn - 1 = n1). */
+static void og_bc_scalar(fpi *a, int n0, int n1, int n2, const int per[3], int s, int yhi) {
+#define A3(i, j, k) a[((long)(i) * n1 + (j)) * n2 + (k)]
+  const int e0 = n0 - 1, e1 = n1 - 1, e2 = n2 - 1;      /* last index */
+  const int f0 = n0 - 1 - s, f1 = n1 - 1 - s, f2 = n2 - 1 - s;  /* periodic source */
+  if (per[0])
+    for (int j = 1; j < e1; j++)
+      for (int k = 1; k < e2; k++) {
+        A3(0, j, k) = A3(f0, j, k);
+        A3(e0, j, k) = A3(s, j, k);
+      }
+  if (per[1])
+    for (int i = 1; i < e0; i++)
+      for (int k = 1; k < e2; k++) {
+        A3(i, 0, k) = A3(i, f1, k);
+        A3(i, e1, k) = A3(i, s, k);
+      }
+  if (per[2])
+    for (int i = 1; i < e0; i++)
+      for (int j = 1; j < e1; j++) {
+        A3(i, j, 0) = A3(i, j, f2);
+        A3(i, j, e2) = A3(i, j, s);
+      }
+  if (per[1] || per[2])
+    for (int i = 1; i < e0; i++) {
+      A3(i, e1, e2) = A3(i, s, s);
+      A3(i, 0, 0) = A3(i, f1, f2);
+      A3(i, 0, e2) = A3(i, f1, s);
+      A3(i, e1, 0) = A3(i, s, f2);
+    }
+  if (per[0] || per[2])
+    for (int j = 1; j < yhi; j++) {
+      A3(e0, j, e2) = A3(s, j, s);
+      A3(0, j, 0) = A3(f0, j, f2);
+      A3(0, j, e2) = A3(f0, j, s);
+      A3(e0, j, 0) = A3(s, j, f2);
+    }
+  if (per[0] || per[1])
+    for (int k = 1; k < e2; k++) {
+      A3(e0, e1, k) = A3(s, s, k);
+      A3(0, 0, k) = A3(f0, f1, k);
+      A3(e0, 0, k) = A3(s, f1, k);
+      A3(0, e1, k) = A3(f0, s, k);
+    }
+  if (per[0] || per[1] || per[2]) {
+    A3(e0, e1, e2) = A3(s, s, s);
+    A3(0, e1, e2) = A3(f0, s, s);
+    A3(e0, 0, e2) = A3(s, f1, s);
+    A3(0, 0, e2) = A3(f0, f1, s);
+    A3(e0, e1, 0) = A3(s, s, f2);
+    A3(0, e1, 0) = A3(f0, s, f2);
+    A3(e0, 0, 0) = A3(s, f1, f2);
+    A3(0, 0, 0) = A3(f0, f1, f2);
+  }
+  if (!per[0])
+    for (int j = 0; j < n1; j++)
+      for (int k = 0; k < n2; k++) {
+        A3(0, j, k) = A3(1, j, k);
+        A3(e0, j, k) = A3(e0 - 1, j, k);
+      }
+  if (!per[1])
+    for (int i = 0; i < n0; i++)
+      for (int k = 0; k < n2; k++) {
+        A3(i, 0, k) = A3(i, 1, k);
+        A3(i, e1, k) = A3(i, e1 - 1, k);
+      }
+  if (!per[2])
+    for (int i = 0; i < n0; i++)
+      for (int j = 0; j < n1; j++) {
+        A3(i, j, 0) = A3(i, j, 1);
+        A3(i, j, e2) = A3(i, j, e2 - 1);
+      }
+#undef A3
+}
+
+/* Centre-difference stencil of a node array at cell (i, j, k) along `axis`:
+ * the four node differences across the cell's faces, each times .25 and the
+ * inverse spacing, summed in double in the reference order (src/Grid.cpp:
+ * 267-319 divN2C, 322-396 divSymmTensorN2C). The caller rounds. */
+static double og_d4(const og_grid *g, const fpi *a, int i, int j, int k, int axis, fpi inv) {
+  /* the two indices that run across the face, in the order the reference
+   * lists the four terms: x (j, k) with k fastest; y (i, k) with k fastest;
+   * z (i, j) with i fastest */
+  double sum = 0.0;
+  for (int t = 0; t < 4; t++) {
+    int i0 = i, j0 = j, k0 = k;
+    int hi = t >> 1, lo = t & 1;
+    if (axis == 0) { j0 += hi; k0 += lo; }
+    else if (axis == 1) { i0 += hi; k0 += lo; }
+    else { j0 += hi; i0 += lo; }
+    const long n0 = og_node(g, i0, j0, k0);
+    const long n1 = og_node(g, i0 + (axis == 0), j0 + (axis == 1), k0 + (axis == 2));
+    const double term = .25 * (fpi)(a[n1] - a[n0]) * inv;
+    sum = t ? sum + term : term;
+  }
+  return sum;
+}
+
+int orc_hat_densities(const orc_setup *s, double th, int ns, const double *qom,
+                      const void *const *mom, const void *const fld[6], const void *rhoc_v,
+                      void *jxh_v, void *jyh_v, void *jzh_v, void *rhoh_v) {
+  og_grid g;
+  if (og_make_grid(s, &g)) return -1;
+  const int nxc = g.nxc, nyc = g.nyc, nzc = g.nzc;
+  const int nxn = g.nxn, nyn = g.nyn, nzn = g.nzn;
+  const long nc = (long)nxc * nyc * nzc, nn = (long)nxn * nyn * nzn;
+  fpi *tc[3], *tn[3];
+  for (int a = 0; a < 3; a++) {
+    tc[a] = (fpi *)calloc(nc, sizeof(fpi));
+    tn[a] = (fpi *)calloc(nn, sizeof(fpi));
+  }
+  fpi *jh[3] = {(fpi *)jxh_v, (fpi *)jyh_v, (fpi *)jzh_v};
+  fpi *rhoh = (fpi *)rhoh_v;
+  const fpi *rhoc = (const fpi *)rhoc_v;
+  const fpf *Bn[3] = {(const fpf *)fld[3], (const fpf *)fld[4], (const fpf *)fld[5]};
+  const fpi inv[3] = {(fpi)g.invdx, (fpi)g.invdy, (fpi)g.invdz};
+#define CI(i, j, k) (((long)(i) * nyc + (j)) * nzc + (k))
+  for (long n = 0; n < nn; n++) jh[0][n] = jh[1][n] = jh[2][n] = 0;
+  for (long c = 0; c < nc; c++) rhoh[c] = 0;
+  const fpf alfa = (fpf)(-s->dt / 2.0);
+  for (int is = 0; is < ns; is++) {
+    const fpi *const *M = (const fpi *const *)mom + 10 * is;
+    /* divSymmTensorN2C: row r of the symmetric tensor, columns x, y, z
+     * (pxx pxy pxz / pxy pyy pyz / pxz pyz pzz), then scaled by -dt/2 */
+    const fpi *T[3][3] = {{M[4], M[5], M[6]}, {M[5], M[7], M[8]}, {M[6], M[8], M[9]}};
+    for (int i = 1; i < nxc - 1; i++)
+      for (int j = 1; j < nyc - 1; j++)
+        for (int k = 1; k < nzc - 1; k++) {
+          fpi comp[3][3]; /* [row][axis] */
+          for (int r = 0; r < 3; r++)
+            for (int ax = 0; ax < 3; ax++)
+              comp[r][ax] = (fpi)og_d4(&g, T[ax][r], i, j, k, ax, inv[ax]);
+          for (int r = 0; r < 3; r++) tc[r][CI(i, j, k)] = comp[r][0] + comp[r][1] + comp[r][2];
+        }
+    for (int r = 0; r < 3; r++) {
+      for (long c = 0; c < nc; c++) tc[r][c] *= alfa;
+      og_bc_scalar(tc[r], nxc, nyc, nzc, s->periodic, 1, nyn - 1);
+    }
+    /* interpC2Ninterp on the inner nodes, then + J (src/Grid.cpp:122-139) */
+    for (int r = 0; r < 3; r++) {
+      const fpi *C = tc[r];
+      for (int i = 1; i < nxn - 1; i++)
+        for (int j = 1; j < nyn - 1; j++)
+          for (int k = 1; k < nzn - 1; k++) {
+            fpi sum8 = C[CI(i, j, k)] + C[CI(i - 1, j, k)];
+            sum8 = sum8 + C[CI(i, j - 1, k)];
+            sum8 = sum8 + C[CI(i, j, k - 1)];
+            sum8 = sum8 + C[CI(i - 1, j - 1, k)];
+            sum8 = sum8 + C[CI(i - 1, j, k - 1)];
+            sum8 = sum8 + C[CI(i, j - 1, k - 1)];
+            sum8 = sum8 + C[CI(i - 1, j - 1, k - 1)];
+            tn[r][og_node(&g, i, j, k)] = (fpi)(.125 * sum8);
+          }
+      const fpi *J = M[1 + r];
+      for (long n = 0; n < nn; n++) tn[r][n] += J[n];
+    }
+    /* PIdot: rotate with the species' omega_c dt / 2 and accumulate */
+    const fpf beta = (fpf)(.5 * qom[is] * s->dt / s->c);
+    for (long n = 0; n < nn; n++) {
+      const fpf ox = beta * Bn[0][n], oy = beta * Bn[1][n], oz = beta * Bn[2][n];
+      const fpi X = tn[0][n], Y = tn[1][n], Z = tn[2][n];
+      const fpf edotb = X * ox + Y * oy + Z * oz;
+      const fpf denom = (fpf)(1 / (1.0 + ox * ox + oy * oy + oz * oz));
+      jh[0][n] += (X + (Y * oz - Z * oy + edotb * ox)) * denom;
+      jh[1][n] += (Y + (Z * ox - X * oz + edotb * oy)) * denom;
+      jh[2][n] += (Z + (X * oy - Y * ox + edotb * oz)) * denom;
+    }
+  }
+  for (int r = 0; r < 3; r++) og_bc_scalar(jh[r], nxn, nyn, nzn, s->periodic, 2, nyn - 1);
+  /* rho hat = rho_c - dt theta div(J hat) (divN2C on the inner cells) */
+  fpi *dv = tc[0];
+  for (long c = 0; c < nc; c++) dv[c] = 0;
+  for (int i = 1; i < nxc - 1; i++)
+    for (int j = 1; j < nyc - 1; j++)
+      for (int k = 1; k < nzc - 1; k++) {
+        const fpf cx = (fpf)og_d4(&g, jh[0], i, j, k, 0, inv[0]);
+        const fpf cy = (fpf)og_d4(&g, jh[1], i, j, k, 1, inv[1]);
+        const fpf cz = (fpf)og_d4(&g, jh[2], i, j, k, 2, inv[2]);
+        dv[CI(i, j, k)] = cx + cy + cz;
+      }
+  for (long c = 0; c < nc; c++) rhoh[c] = (fpi)(rhoc[c] - s->dt * th * dv[c]);
+  og_bc_scalar(rhoh, nxc, nyc, nzc, s->periodic, 1, nyn - 1);
+#undef CI
+  for (int a = 0; a < 3; a++) {
+    free(tc[a]);
+    free(tn[a]);
+  }
+  og_free_grid(&g);
+  return 0;
+}

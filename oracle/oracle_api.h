@@ -8,7 +8,10 @@
  *
  * Two libraries implement this header:
  *   - oracle/liboracle_{fp32,fp64}.so: oracle.c, a plain-C restatement of
- *     sputniPIC's src/Mover.cpp, src/Grid.cpp:5-62 and src/BC.cpp:362-615.
+ *     sputniPIC's src/Mover.cpp, src/Grid.cpp:5-62 and src/BC.cpp:362-615,
+ *     src/Particles.cpp:72-234 (particle_sort) and
+ *     src/MaxwellSolver.cpp:465-603 (calculateHatDensities) with the Grid.cpp
+ *     stencils and BC.cpp guard-cell fills it calls.
  *   - oracle/_ref/libref_{fp32,fp64}.so: ref_shim.cpp linked against the
  *     reference's own sources, compiled where they lie.
  * ORC_FP is float in the *_fp32 builds (the reference's PrecisionTypes.h)
@@ -77,6 +80,18 @@ int orc_cycle(const orc_setup *s, const void *const fld[6], int ns,
               void *const *v, void *const *w, void *const *q, const long *nop,
               const double *qom, void *const *mom, double *t_mover,
               double *t_interp);
+
+/* calculateHatDensities (src/MaxwellSolver.cpp:465-603) for ns species
+ * (ns <= 6, the reference's NS_MAX): mom holds ns*10 node arrays
+ * (species-major, interpP2G order; Jx..Jz and pxx..pzz are read), fld the
+ * six field node arrays (Bxn..Bzn are read), rhoc the net charge density on
+ * the cell centres, flat [nxc+2][nyc+2][nzc+2]; qom[ns] the species'
+ * charge-to-mass ratios, th the implicitness parameter theta. Writes the node
+ * arrays jxh, jyh, jzh and the centre array rhoh. Returns 0, -1 when out of
+ * memory. */
+int orc_hat_densities(const orc_setup *s, double th, int ns, const double *qom,
+                      const void *const *mom, const void *const fld[6], const void *rhoc,
+                      void *jxh, void *jyh, void *jzh, void *rhoh);
 
 /* Number of OpenMP threads the library will use. */
 int orc_num_threads(void);

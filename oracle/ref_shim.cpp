@@ -6,7 +6,9 @@
  * TEST INFRASTRUCTURE ONLY. Built by oracle/Makefile against the reference's
  * sources where they lie (src/Mover.cpp, src/Grid.cpp, src/BC.cpp,
  * src/EMfield.cpp, src/InterpDensSpecies.cpp, src/InterpDensNet.cpp,
- * src/Particles.cpp) into oracle/_ref/, which is never committed.
+ * src/Particles.cpp, src/MaxwellSolver.cpp with src/Basic.cpp and
+ * src/Solvers.cpp it links against) into oracle/_ref/, which is never
+ * committed.
  *
  * Each call builds the reference structs the way the CPU driver does
  * (src/sputniPIC_CPU.cpp:105-135: setGrid, field_allocate,
@@ -20,6 +22,7 @@
 
 #include "BC.h"
 #include "InterpDensNet.h"
+#include "MaxwellSolver.h"
 #include "Mover.h"
 #include "Particles.h"
 #include "oracle_api.h"
@@ -226,6 +229,44 @@ int orc_particle_sort(const orc_setup *s, int sort_cps, void *x, void *y, void *
   particles p;
   wrap_particles(&p, s, x, y, z, u, v, w, q, n, 0.0);
   particle_sort(&W.param, &p, &W.grd);   // src/Particles.cpp:72-234
+  return 0;
+}
+
+/* calculateHatDensities (src/MaxwellSolver.cpp:465-603) on the caller's
+ * arrays: the structs are built as the CPU driver builds them
+ * (src/sputniPIC_CPU.cpp:105-135), the moments and rhoc copied in, the hat
+ * densities copied out. */
+int orc_hat_densities(const orc_setup *s, double th, int ns, const double *qom,
+                      const void *const *mom, const void *const fld[6], const void *rhoc,
+                      void *jxh, void *jyh, void *jzh, void *rhoh) {
+  if (ns < 1 || ns > NS_MAX) return -1;
+  RefWorld W(s);
+  W.param.ns = ns;
+  W.param.th = th;
+  for (int is = 0; is < ns; is++) W.param.qom[is] = qom[is];
+  W.load_field(fld);
+  std::vector<interpDensSpecies> ids(ns);
+  for (int is = 0; is < ns; is++) {
+    interp_dens_species_allocate(&W.grd, &ids[is], is);
+    FPinterp *slot[10];
+    moment_slots(&ids[is], slot);
+    for (int m = 0; m < 10; m++)
+      std::memcpy(slot[m], ((const void *const *)mom)[10 * is + m], sizeof(FPinterp) * W.nodes());
+  }
+  interpDensNet idn;
+  interp_dens_net_allocate(&W.grd, &idn);
+  const long cells = (long)W.grd.nxc * W.grd.nyc * W.grd.nzc;
+  std::memcpy(idn.rhoc_flat, rhoc, sizeof(FPinterp) * cells);
+  interpDens_aux aux;
+  interp_dens_aux_allocate(&W.grd, &aux);
+  calculateHatDensities(&aux, &idn, ids.data(), &W.field, &W.grd, &W.param);
+  std::memcpy(jxh, &aux.Jxh[0][0][0], sizeof(FPinterp) * W.nodes());
+  std::memcpy(jyh, &aux.Jyh[0][0][0], sizeof(FPinterp) * W.nodes());
+  std::memcpy(jzh, &aux.Jzh[0][0][0], sizeof(FPinterp) * W.nodes());
+  std::memcpy(rhoh, &aux.rhoh[0][0][0], sizeof(FPinterp) * cells);
+  interp_dens_aux_deallocate(&W.grd, &aux);
+  interp_dens_net_deallocate(&W.grd, &idn);
+  for (int is = 0; is < ns; is++) interp_dens_species_deallocate(&W.grd, &ids[is]);
   return 0;
 }
 

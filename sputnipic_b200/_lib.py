@@ -73,6 +73,11 @@ class InterpDensNet(ctypes.Structure):
     _fields_ = [(n, P) for f in ("rhon", "rhoc") + MOMENT_NAMES[1:] for n in (f, f + "_flat")]
 
 
+class InterpDensAux(ctypes.Structure):
+    """Implicit-source densities of the field solver (include/InterpDens_aux.h:6-13)."""
+    _fields_ = [(n, P) for n in ("rhoh", "Jxh", "Jyh", "Jzh")]
+
+
 def _ints(*names):
     return [(n, c_int) for n in names]
 
@@ -111,7 +116,7 @@ class Parameters(ctypes.Structure):
 
 STRUCTS = {"particles": Particles, "EMfield": EMfield, "grid": Grid,
            "interpDensSpecies": InterpDensSpecies, "interpDensNet": InterpDensNet,
-           "parameters": Parameters}
+           "interpDens_aux": InterpDensAux, "parameters": Parameters}
 
 
 class SpbPush(ctypes.Structure):
@@ -142,6 +147,17 @@ class SimDesc(ctypes.Structure):
                 ("ns", c_int), ("qom", c_double * 8), ("capacity", c_long * 8),
                 ("tile", c_int * 3), ("resort_every", c_int), ("ctas", c_int),
                 ("variant", c_int), ("bucket_slots", c_int), ("graph", c_int)]
+
+
+HAT_MAX_SPECIES = 16
+
+
+class HatDesc(ctypes.Structure):
+    """spb_hat_desc (include/sputnipic_b200.h)."""
+    _fields_ = [("nxc", c_int), ("nyc", c_int), ("nzc", c_int),
+                ("invdx", c_double), ("invdy", c_double), ("invdz", c_double),
+                ("periodic", c_int * 3), ("dt", c_double), ("c", c_double), ("th", c_double),
+                ("ns", c_int), ("qom", c_double * HAT_MAX_SPECIES)]
 
 
 class ServeDesc(ctypes.Structure):
@@ -247,6 +263,11 @@ def load():
     _proto(lib, "spb_interp_all_species", c_int,
            [R(Particles), R(InterpDensSpecies), R(InterpDensNet), R(Grid), R(Parameters)])
     _proto(lib, "spb_particle_sort", c_int, [R(Parameters), R(Particles), R(Grid)])
+    _proto(lib, "spb_calculateHatDensities", c_int,
+           [R(InterpDensAux), R(InterpDensNet), R(InterpDensSpecies), R(EMfield), R(Grid),
+            R(Parameters)])
+    for fp in ("f32", "f64"):
+        _proto(lib, "spb_hat_densities_" + fp, c_int, [R(HatDesc), P, P, P, P, P, P, P, P])
     _proto(lib, "spb_serve_create", c_int, [R(ServeDesc), R(P)])
     _proto(lib, "spb_serve_destroy", None, [P])
     _proto(lib, "spb_serve_submit", c_long, [P, R(JobDesc), P, P, P, c_int])

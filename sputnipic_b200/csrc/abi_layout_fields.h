@@ -89,12 +89,17 @@
   X(interpDensNet, pyz) X(interpDensNet, pyz_flat) X(interpDensNet, pzz)         \
   X(interpDensNet, pzz_flat)
 
+#define SPB_LAYOUT_AUX(X)                                                        \
+  X(interpDens_aux, rhoh) X(interpDens_aux, Jxh) X(interpDens_aux, Jyh)          \
+  X(interpDens_aux, Jzh)
+
 #define SPB_LAYOUT_ALL(X)                                                        \
   SPB_LAYOUT_PARTICLES(X) SPB_LAYOUT_EMFIELD(X) SPB_LAYOUT_GRID(X)               \
-  SPB_LAYOUT_IDS(X) SPB_LAYOUT_IDN(X) SPB_LAYOUT_PARAMETERS(X)
+  SPB_LAYOUT_IDS(X) SPB_LAYOUT_IDN(X) SPB_LAYOUT_AUX(X) SPB_LAYOUT_PARAMETERS(X)
 
 #define SPB_LAYOUT_STRUCTS(S)                                                    \
-  S(particles) S(EMfield) S(grid) S(interpDensSpecies) S(interpDensNet) S(parameters)
+  S(particles) S(EMfield) S(grid) S(interpDensSpecies) S(interpDensNet)          \
+  S(interpDens_aux) S(parameters)
 
 /* Appends `"struct.member": offset,` pairs and `"struct": sizeof` to a
  * std::string; used by both expansions. */

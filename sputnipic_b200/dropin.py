@@ -8,8 +8,9 @@ Same names, argument meaning and results as sputniPIC's C++ functions:
   (src/InterpDensSpecies.cpp:4-42) build the reference structs over numpy
   arrays (the structs are ctypes mirrors with the reference's layout);
 * ``mover_PC``, ``mover_PC_V``, ``interpP2G``, ``mover_interp``
-  (include/Mover.h:11-26) call the CUDA library's drop-in entry points with
-  those structs, exactly as the reference's C++ driver would.
+  (include/Mover.h:11-26), ``calculateHatDensities``
+  (include/MaxwellSolver.h:37-40) call the CUDA library's drop-in entry
+  points with those structs, exactly as the reference's C++ driver would.
 
 mover_PC / mover_PC_V / mover_interp return the library status (0 = ok,
 as the reference's always-0 return); interpP2G returns None and leaves its
@@ -156,6 +157,32 @@ def interp_dens_net_allocate(grd: Grid) -> "_lib.InterpDensNet":
     return idn
 
 
+def _arr3(obj, name: str, n0: int, n1: int, n2: int) -> int:
+    """newArr3 (include/Alloc.h:52-60): one zeroed float block with a
+    row-pointer and a plane-pointer level over it; returns the top pointer."""
+    data = np.zeros(n0 * n1 * n2, np.float32)
+    rows = (data.ctypes.data + 4 * n2 * np.arange(n0 * n1, dtype=np.uint64)).astype(np.uint64)
+    planes = (rows.ctypes.data + 8 * n1 * np.arange(n0, dtype=np.uint64)).astype(np.uint64)
+    _keep(obj, name, data)
+    _keep(obj, name + "_rows", rows)
+    return _keep(obj, name + "_planes", planes)
+
+
+def interp_dens_aux_allocate(grd: Grid) -> "_lib.InterpDensAux":
+    """interp_dens_aux_allocate (include/InterpDens_aux.h:16-24): rho hat on
+    the cell centres, J hat on the nodes, each a 3-level array."""
+    aux = _lib.InterpDensAux()
+    aux.rhoh = _arr3(aux, "rhoh", grd.nxc, grd.nyc, grd.nzc)
+    for n in ("Jxh", "Jyh", "Jzh"):
+        setattr(aux, n, _arr3(aux, n, grd.nxn, grd.nyn, grd.nzn))
+    return aux
+
+
+def hat_arrays(aux) -> tuple:
+    """The flat (Jxh, Jyh, Jzh, rhoh) arrays of an interp_dens_aux_allocate."""
+    return tuple(aux._arrays[n] for n in ("Jxh", "Jyh", "Jzh", "rhoh"))
+
+
 def setZeroSpeciesDensities(ids: InterpDensSpecies) -> None:
     """src/InterpDensNet.cpp:40-75 for one species."""
     for a in ids._arrays.values():
@@ -204,6 +231,20 @@ def interp_all_species(parts: list, ids: list, idn, grd: Grid, param: Parameters
     iarr = (InterpDensSpecies * ns)(*ids)
     return _ret(lib.spb_interp_all_species(parr, iarr, ctypes.byref(idn), ctypes.byref(grd),
                                            ctypes.byref(param)), raise_on_error)
+
+
+def calculateHatDensities(aux, idn, ids: list, field: EMfield, grd: Grid, param: Parameters,
+                          raise_on_error: bool = False) -> int:
+    """calculateHatDensities (src/MaxwellSolver.cpp:465-603) on the device:
+    J hat and rho hat into ``aux`` from the species moments ``ids``
+    (param.ns of them), the magnetic field and ``idn``'s rhoc."""
+    lib = _lib.load()
+    ns = len(ids)
+    assert param.ns == ns
+    iarr = (InterpDensSpecies * ns)(*ids)
+    return _ret(lib.spb_calculateHatDensities(ctypes.byref(aux), ctypes.byref(idn), iarr,
+                                              ctypes.byref(field), ctypes.byref(grd),
+                                              ctypes.byref(param)), raise_on_error)
 
 
 def particle_sort(param: Parameters, part: Particles, grd: Grid,

@@ -276,3 +276,19 @@ def gem_particles(wl: GemWorkload, s: int, cell_lo: int = 0, cell_hi: int | None
 
 def zero_moments(wl: GemWorkload, dtype=np.float32):
     return [np.zeros(wl.nodes, dtype) for _ in range(10)]
+
+
+def hat_inputs(wl: GemWorkload, seed: int = 0, dtype=np.float32, ns: int | None = None):
+    """Seeded inputs of calculateHatDensities on wl's grid: per species the 10
+    node moments (rhon..pzz, magnitudes like a GEM deposit's: rho ~ 1, J ~
+    1e-2, pressures ~ 1e-3), the six node fields (E ~ 1e-3, B ~ 0.05) and the
+    net charge density on the cell centres (guard cells included)."""
+    rng = np.random.default_rng(seed)
+    ns = len(wl.species) if ns is None else ns
+    scale = (1.0,) + (1e-2,) * 3 + (1e-3,) * 6
+    mom = [[(rng.standard_normal(wl.nodes) * sc).astype(dtype) for sc in scale]
+           for _ in range(ns)]
+    fields = ([rng.uniform(-1e-3, 1e-3, wl.nodes).astype(dtype) for _ in range(3)]
+              + [rng.uniform(-0.05, 0.05, wl.nodes).astype(dtype) for _ in range(3)])
+    rhoc = rng.standard_normal((wl.nxc + 2) * (wl.nyc + 2) * (wl.nzc + 2)).astype(dtype)
+    return mom, fields, rhoc

@@ -21,6 +21,8 @@ CXX_DROPINS = [
     "mover_PC_V(particles*, EMfield*, grid*, parameters*)",
     "interpP2G(particles*, interpDensSpecies*, grid*)",
     "mover_interp(particles*, EMfield*, interpDensSpecies*, grid*, parameters*)",
+    "calculateHatDensities(interpDens_aux*, interpDensNet*, interpDensSpecies*, EMfield*, grid*, "
+    "parameters*)",
 ]
 
 

@@ -185,3 +185,27 @@ def test_particle_sort_restated_equals_reference(fp, sort_cps):
     for k in "xyzuvwq":
         assert np.array_equal(a[k], b[k]), k
     assert not np.array_equal(a["x"], p["x"])
+
+
+def hat_case(per):
+    """The grid, species qoms and theta of one hat-densities fixture case
+    (tests/golden/hat_densities.json)."""
+    wl = W.small_gem(nxc=8, nyc=6, nzc=5, periodic=tuple(bool(p) for p in per))
+    return wl, [sp.qom for sp in wl.species[:3]], 1.0
+
+
+@pytest.mark.parametrize("fp", [32, 64])
+@pytest.mark.parametrize("per", [(1, 0, 1), (1, 1, 1), (0, 0, 0), (0, 1, 0)])
+def test_hat_densities_restated_matches_reference_digests(fp, per):
+    """calculateHatDensities (src/MaxwellSolver.cpp:465-603): the restatement
+    reproduces the reference build's outputs bit for bit (SHA-256 of Jxh, Jyh,
+    Jzh, rhoh), for periodic, reflecting and mixed axes."""
+    with open(os.path.join(GOLDEN, "hat_densities.json")) as f:
+        doc = json.load(f)
+    wl, qom, th = hat_case(per)
+    dt = np.float32 if fp == 32 else np.float64
+    mom, fields, rhoc = W.hat_inputs(wl, seed=doc["seed"], dtype=dt, ns=doc["species"])
+    out = oracle.CpuOracle("restated", fp).hat_densities(oracle.setup_from(wl), th, qom, mom,
+                                                         fields, rhoc)
+    assert sha(out) == doc["cases"][f"{''.join(map(str, per))}_fp{fp}"]
+    assert all(np.isfinite(a).all() for a in out)
