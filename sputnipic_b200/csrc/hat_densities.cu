@@ -2,15 +2,16 @@
 // implicit sources of the field solver, J hat on the nodes and rho hat on the
 // cell centres, from the species moments, in the reference's arithmetic.
 //
-// Per species: the divergence of the pressure tensor on the inner cells
-// (divSymmTensorN2C, src/Grid.cpp:322-396) scaled by -dt/2, the centre guard
-// cells filled (applyBCscalarDensC, src/BC.cpp:623-727), then one node pass
-// that interpolates the centres to the inner nodes (interpC2Ninterp,
-// src/Grid.cpp:122-139), adds the species' J, rotates with the species'
-// omega_c dt/2 and accumulates J hat (the PIdot loop, MaxwellSolver.cpp:
-// 535-566). Afterwards the node guards of J hat (applyBCscalarDensN,
-// src/BC.cpp:11-121), one cell pass for rho hat = rho_c - dt theta div(J hat)
-// (divN2C, src/Grid.cpp:267-319) and the centre guards of rho hat.
+// Six launches for all species: the divergence of every species' pressure
+// tensor on the inner cells (divSymmTensorN2C, src/Grid.cpp:322-396) scaled by
+// -dt/2; the centre guard cells of all 3 ns temporaries (applyBCscalarDensC,
+// src/BC.cpp:623-727); one node pass that, species by species, interpolates
+// the centres to the inner nodes (interpC2Ninterp, src/Grid.cpp:122-139),
+// adds the species' J, rotates with its omega_c dt/2 and accumulates J hat
+// in registers (the PIdot loop, MaxwellSolver.cpp:535-566); the node guards
+// of J hat (applyBCscalarDensN, src/BC.cpp:11-121); one cell pass for
+// rho hat = rho_c - dt theta div(J hat) (divN2C, src/Grid.cpp:267-319); the
+// centre guards of rho hat.
 //
 // Arithmetic. This file is compiled with -fmad=false and follows the C
 // promotions of the reference expressions: the stencils' .25 * (a - b) * inv
@@ -77,36 +78,42 @@ __device__ __forceinline__ double d4(const HatGeom &g, const T *__restrict__ a, 
   return sum;
 }
 
-// Pressure-tensor rows (pxx pxy pxz / pxy pyy pyz / pxz pyz pzz): divergence
-// of each row on the inner cells, times alfa = (T)(-dt/2).
+constexpr int HAT_MAXS = SPB_HAT_MAX_SPECIES;
+
+// Every species' inputs: pressure tensors (pxx, pxy, pxz, pyy, pyz, pzz), J,
+// the centre temporaries (three per species) and beta = qom dt / 2c.
 template <typename T>
-struct Tensor6 {
-  const T *p[6];   // pxx, pxy, pxz, pyy, pyz, pzz
+struct Species6 {
+  const T *p[HAT_MAXS][6];
+  const T *j[HAT_MAXS][3];
+  T *tc[HAT_MAXS][3];
+  T beta[HAT_MAXS];
 };
 
+// Pressure-tensor rows (pxx pxy pxz / pxy pyy pyz / pxz pyz pzz): divergence
+// of each row on the inner cells, times alfa = (T)(-dt/2); species blockIdx.y.
 template <typename T>
-__global__ void k_hat_div_tensor(HatGeom g, Tensor6<T> P, T alfa, T *__restrict__ cx,
-                                 T *__restrict__ cy, T *__restrict__ cz) {
+__global__ void k_hat_div_tensor(HatGeom g, const __grid_constant__ Species6<T> S, T alfa) {
+  const int is = blockIdx.y;
   const int mx = g.nxc - 2, my = g.nyc - 2, mz = g.nzc - 2;
   const long inner = (long)mx * my * mz;
   // row r, column ax -> tensor component
   const int comp[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-  T *out[3] = {cx, cy, cz};
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < inner;
        t += (long)gridDim.x * blockDim.x) {
     const int k = 1 + (int)(t % mz), j = 1 + (int)((t / mz) % my), i = 1 + (int)(t / ((long)mz * my));
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      const T c0 = (T)d4(g, P.p[comp[r][0]], i, j, k, 0);
-      const T c1 = (T)d4(g, P.p[comp[r][1]], i, j, k, 1);
-      const T c2 = (T)d4(g, P.p[comp[r][2]], i, j, k, 2);
+      const T c0 = (T)d4(g, S.p[is][comp[r][0]], i, j, k, 0);
+      const T c1 = (T)d4(g, S.p[is][comp[r][1]], i, j, k, 1);
+      const T c2 = (T)d4(g, S.p[is][comp[r][2]], i, j, k, 2);
       const T div = c0 + c1 + c2;
-      out[r][cidx(g, i, j, k)] = div * alfa;
+      S.tc[is][r][cidx(g, i, j, k)] = div * alfa;
     }
   }
 }
 
-// Guard-cell fill of n0 x n1 x n2 scalar arrays, one CTA per array
+// Guard-cell fill of n0 x n1 x n2 scalar arrays, one CTA per array (A.a[blockIdx.x])
 // (applyBCscalarDensC with s = 1, applyBCscalarDensN with s = 2). Phases in
 // the reference order: periodic faces X, Y, Z; edges along X, Y, Z; corners;
 // non-periodic faces X, Y, Z. A periodic face copies from n-1-s to 0 and from
@@ -117,90 +124,117 @@ struct Fill {
 };
 
 template <typename T>
-__global__ void k_hat_fill(Fill f, T *a0, T *a1, T *a2) {
-  T *a = blockIdx.x == 0 ? a0 : (blockIdx.x == 1 ? a1 : a2);
-  if (!a) return;
-  const int n1 = f.n1, n2 = f.n2, s = f.s;
-  const int e0 = f.n0 - 1, e1 = n1 - 1, e2 = n2 - 1;
-  const int f0 = e0 - s, f1 = e1 - s, f2 = e2 - s;
-  auto at = [&](int i, int j, int k) -> T & { return a[((long)i * n1 + j) * n2 + k]; };
+struct Arrays {
+  T *a[3 * HAT_MAXS];
+};
+
+// One fill phase over N elements of C copies each (dst <- src, as linear
+// indices from idx(t, c, dst, src)): every thread loads the sources of U
+// elements before storing them, which no phase makes unsafe (a phase never
+// writes what it reads).
+template <typename T, int C, int U, typename Idx>
+__device__ __forceinline__ void fill_phase(T *a, int N, Idx idx) {
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (f.per[0])
-    for (int t = tid; t < (e1 - 1) * (e2 - 1); t += nt) {
-      const int j = 1 + t / (e2 - 1), k = 1 + t % (e2 - 1);
-      at(0, j, k) = at(f0, j, k);
-      at(e0, j, k) = at(s, j, k);
+  for (int t0 = tid; t0 < N; t0 += U * nt) {
+    T v[U][C];
+    long d[U][C];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * nt;
+      if (t < N) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          long sidx;
+          idx(t, c, d[u][c], sidx);
+          v[u][c] = a[sidx];
+        }
+      }
     }
-  __syncthreads();
-  if (f.per[1])
-    for (int t = tid; t < (e0 - 1) * (e2 - 1); t += nt) {
-      const int i = 1 + t / (e2 - 1), k = 1 + t % (e2 - 1);
-      at(i, 0, k) = at(i, f1, k);
-      at(i, e1, k) = at(i, s, k);
-    }
-  __syncthreads();
-  if (f.per[2])
-    for (int t = tid; t < (e0 - 1) * (e1 - 1); t += nt) {
-      const int i = 1 + t / (e1 - 1), j = 1 + t % (e1 - 1);
-      at(i, j, 0) = at(i, j, f2);
-      at(i, j, e2) = at(i, j, s);
-    }
-  __syncthreads();
-  if (f.per[1] || f.per[2])
-    for (int i = 1 + tid; i < e0; i += nt) {
-      at(i, e1, e2) = at(i, s, s);
-      at(i, 0, 0) = at(i, f1, f2);
-      at(i, 0, e2) = at(i, f1, s);
-      at(i, e1, 0) = at(i, s, f2);
-    }
-  __syncthreads();
-  if (f.per[0] || f.per[2])
-    for (int j = 1 + tid; j < f.yhi; j += nt) {
-      at(e0, j, e2) = at(s, j, s);
-      at(0, j, 0) = at(f0, j, f2);
-      at(0, j, e2) = at(f0, j, s);
-      at(e0, j, 0) = at(s, j, f2);
-    }
-  __syncthreads();
-  if (f.per[0] || f.per[1])
-    for (int k = 1 + tid; k < e2; k += nt) {
-      at(e0, e1, k) = at(s, s, k);
-      at(0, 0, k) = at(f0, f1, k);
-      at(e0, 0, k) = at(s, f1, k);
-      at(0, e1, k) = at(f0, s, k);
-    }
-  __syncthreads();
-  if ((f.per[0] || f.per[1] || f.per[2]) && tid == 0) {
-    at(e0, e1, e2) = at(s, s, s);
-    at(0, e1, e2) = at(f0, s, s);
-    at(e0, 0, e2) = at(s, f1, s);
-    at(0, 0, e2) = at(f0, f1, s);
-    at(e0, e1, 0) = at(s, s, f2);
-    at(0, e1, 0) = at(f0, s, f2);
-    at(e0, 0, 0) = at(s, f1, f2);
-    at(0, 0, 0) = at(f0, f1, f2);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (t0 + u * nt < N) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) a[d[u][c]] = v[u][c];
+      }
   }
   __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_hat_fill(Fill f, const __grid_constant__ Arrays<T> A) {
+  T *a = A.a[blockIdx.x];
+  const int n0 = f.n0, n1 = f.n1, n2 = f.n2, s = f.s;
+  const int e0 = n0 - 1, e1 = n1 - 1, e2 = n2 - 1;
+  const int f0 = e0 - s, f1 = e1 - s, f2 = e2 - s;
+  auto L = [=](int i, int j, int k) -> long { return ((long)i * n1 + j) * n2 + k; };
+  if (f.per[0])
+    fill_phase<T, 2, 4>(a, (e1 - 1) * (e2 - 1), [=](int t, int c, long &d, long &src) {
+      const int j = 1 + t / (e2 - 1), k = 1 + t % (e2 - 1);
+      d = c ? L(e0, j, k) : L(0, j, k);
+      src = c ? L(s, j, k) : L(f0, j, k);
+    });
+  if (f.per[1])
+    fill_phase<T, 2, 4>(a, (e0 - 1) * (e2 - 1), [=](int t, int c, long &d, long &src) {
+      const int i = 1 + t / (e2 - 1), k = 1 + t % (e2 - 1);
+      d = c ? L(i, e1, k) : L(i, 0, k);
+      src = c ? L(i, s, k) : L(i, f1, k);
+    });
+  if (f.per[2])
+    fill_phase<T, 2, 4>(a, (e0 - 1) * (e1 - 1), [=](int t, int c, long &d, long &src) {
+      const int i = 1 + t / (e1 - 1), j = 1 + t % (e1 - 1);
+      d = c ? L(i, j, e2) : L(i, j, 0);
+      src = c ? L(i, j, s) : L(i, j, f2);
+    });
+  if (f.per[1] || f.per[2])
+    fill_phase<T, 4, 2>(a, e0 - 1, [=](int t, int c, long &d, long &src) {
+      const int i = 1 + t;
+      const int dj[4] = {e1, 0, 0, e1}, dk[4] = {e2, 0, e2, 0};
+      const int sj[4] = {s, f1, f1, s}, sk[4] = {s, f2, s, f2};
+      d = L(i, dj[c], dk[c]);
+      src = L(i, sj[c], sk[c]);
+    });
+  if (f.per[0] || f.per[2])
+    fill_phase<T, 4, 2>(a, f.yhi - 1, [=](int t, int c, long &d, long &src) {
+      const int j = 1 + t;
+      const int di[4] = {e0, 0, 0, e0}, dk[4] = {e2, 0, e2, 0};
+      const int si[4] = {s, f0, f0, s}, sk[4] = {s, f2, s, f2};
+      d = L(di[c], j, dk[c]);
+      src = L(si[c], j, sk[c]);
+    });
+  if (f.per[0] || f.per[1])
+    fill_phase<T, 4, 2>(a, e2 - 1, [=](int t, int c, long &d, long &src) {
+      const int k = 1 + t;
+      const int di[4] = {e0, 0, e0, 0}, dj[4] = {e1, 0, 0, e1};
+      const int si[4] = {s, f0, s, f0}, sj[4] = {s, f1, f1, s};
+      d = L(di[c], dj[c], k);
+      src = L(si[c], sj[c], k);
+    });
+  if (f.per[0] || f.per[1] || f.per[2])
+    fill_phase<T, 8, 1>(a, 1, [=](int, int c, long &d, long &src) {
+      // corners in the reference's order; (bit 2, bit 1, bit 0) of c pick
+      // the far (e) or near (0) face along (x, y, z), reversed
+      const int ci = (c & 1) ? 0 : 1, cj = (c & 2) ? 0 : 1, ck = (c & 4) ? 0 : 1;
+      d = L(ci ? e0 : 0, cj ? e1 : 0, ck ? e2 : 0);
+      src = L(ci ? s : f0, cj ? s : f1, ck ? s : f2);
+    });
   if (!f.per[0])
-    for (int t = tid; t < n1 * n2; t += nt) {
+    fill_phase<T, 2, 4>(a, n1 * n2, [=](int t, int c, long &d, long &src) {
       const int j = t / n2, k = t % n2;
-      at(0, j, k) = at(1, j, k);
-      at(e0, j, k) = at(e0 - 1, j, k);
-    }
-  __syncthreads();
+      d = c ? L(e0, j, k) : L(0, j, k);
+      src = c ? L(e0 - 1, j, k) : L(1, j, k);
+    });
   if (!f.per[1])
-    for (int t = tid; t < f.n0 * n2; t += nt) {
+    fill_phase<T, 2, 4>(a, n0 * n2, [=](int t, int c, long &d, long &src) {
       const int i = t / n2, k = t % n2;
-      at(i, 0, k) = at(i, 1, k);
-      at(i, e1, k) = at(i, e1 - 1, k);
-    }
-  __syncthreads();
+      d = c ? L(i, e1, k) : L(i, 0, k);
+      src = c ? L(i, e1 - 1, k) : L(i, 1, k);
+    });
   if (!f.per[2])
-    for (int t = tid; t < f.n0 * n1; t += nt) {
+    fill_phase<T, 2, 4>(a, n0 * n1, [=](int t, int c, long &d, long &src) {
       const int i = t / n1, j = t % n1;
-      at(i, j, 0) = at(i, j, 1);
-      at(i, j, e2) = at(i, j, e2 - 1);
-    }
+      d = c ? L(i, j, e2) : L(i, j, 0);
+      src = c ? L(i, j, e2 - 1) : L(i, j, 1);
+    });
 }
 
 template <typename T>
@@ -212,45 +246,50 @@ struct Out3 {
   T *v[3];
 };
 
-// One species on every node: the interpolated divergence (inner nodes) plus
-// J, rotated by the species' beta B and added into J hat (written fresh for
-// the first species).
+// Every node: per species in order, the interpolated divergence (inner
+// nodes) plus J, rotated by the species' beta B and added into J hat, which
+// starts at 0 (the reference's per-species accumulation, in registers).
 template <typename T>
-__global__ void k_hat_pidot(HatGeom g, Vec3<T> C, Vec3<T> J, Vec3<T> B, T beta, int first,
+__global__ void k_hat_pidot(HatGeom g, const __grid_constant__ Species6<T> S, int ns, Vec3<T> B,
                             Out3<T> JH) {
   const long nodes = (long)g.nxn * g.nyn * g.nzn;
   for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < nodes;
        n += (long)gridDim.x * blockDim.x) {
     const int k = (int)(n % g.nzn), j = (int)((n / g.nzn) % g.nyn), i = (int)(n / ((long)g.nzn * g.nyn));
     const bool inner = i >= 1 && i < g.nxn - 1 && j >= 1 && j < g.nyn - 1 && k >= 1 && k < g.nzn - 1;
-    T tn[3];
+    const T bx = B.v[0][n], by = B.v[1][n], bz = B.v[2][n];
+    T jh[3] = {(T)0, (T)0, (T)0};
+    for (int is = 0; is < ns; ++is) {
+      T tn[3];
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      T v = (T)0;
-      if (inner) {
-        const T *c = C.v[r];
-        T s8 = c[cidx(g, i, j, k)] + c[cidx(g, i - 1, j, k)];
-        s8 = s8 + c[cidx(g, i, j - 1, k)];
-        s8 = s8 + c[cidx(g, i, j, k - 1)];
-        s8 = s8 + c[cidx(g, i - 1, j - 1, k)];
-        s8 = s8 + c[cidx(g, i - 1, j, k - 1)];
-        s8 = s8 + c[cidx(g, i, j - 1, k - 1)];
-        s8 = s8 + c[cidx(g, i - 1, j - 1, k - 1)];
-        v = (T)(0.125 * (double)s8);
+      for (int r = 0; r < 3; ++r) {
+        T v = (T)0;
+        if (inner) {
+          const T *c = S.tc[is][r];
+          T s8 = c[cidx(g, i, j, k)] + c[cidx(g, i - 1, j, k)];
+          s8 = s8 + c[cidx(g, i, j - 1, k)];
+          s8 = s8 + c[cidx(g, i, j, k - 1)];
+          s8 = s8 + c[cidx(g, i - 1, j - 1, k)];
+          s8 = s8 + c[cidx(g, i - 1, j, k - 1)];
+          s8 = s8 + c[cidx(g, i, j - 1, k - 1)];
+          s8 = s8 + c[cidx(g, i - 1, j - 1, k - 1)];
+          v = (T)(0.125 * (double)s8);
+        }
+        tn[r] = v + S.j[is][r][n];
       }
-      tn[r] = v + J.v[r][n];
+      const T beta = S.beta[is];
+      const T ox = beta * bx, oy = beta * by, oz = beta * bz;
+      const T X = tn[0], Y = tn[1], Z = tn[2];
+      const T edotb = X * ox + Y * oy + Z * oz;
+      const T oxx = ox * ox, oyy = oy * oy, ozz = oz * oz;
+      const T denom = (T)(1 / (1.0 + (double)oxx + (double)oyy + (double)ozz));
+      jh[0] = jh[0] + (X + (Y * oz - Z * oy + edotb * ox)) * denom;
+      jh[1] = jh[1] + (Y + (Z * ox - X * oz + edotb * oy)) * denom;
+      jh[2] = jh[2] + (Z + (X * oy - Y * ox + edotb * oz)) * denom;
     }
-    const T ox = beta * B.v[0][n], oy = beta * B.v[1][n], oz = beta * B.v[2][n];
-    const T X = tn[0], Y = tn[1], Z = tn[2];
-    const T edotb = X * ox + Y * oy + Z * oz;
-    const T oxx = ox * ox, oyy = oy * oy, ozz = oz * oz;
-    const T denom = (T)(1 / (1.0 + (double)oxx + (double)oyy + (double)ozz));
-    const T rx = (X + (Y * oz - Z * oy + edotb * ox)) * denom;
-    const T ry = (Y + (Z * ox - X * oz + edotb * oy)) * denom;
-    const T rz = (Z + (X * oy - Y * ox + edotb * oz)) * denom;
-    JH.v[0][n] = (first ? (T)0 : JH.v[0][n]) + rx;
-    JH.v[1][n] = (first ? (T)0 : JH.v[1][n]) + ry;
-    JH.v[2][n] = (first ? (T)0 : JH.v[2][n]) + rz;
+    JH.v[0][n] = jh[0];
+    JH.v[1][n] = jh[1];
+    JH.v[2][n] = jh[2];
   }
 }
 
@@ -298,33 +337,45 @@ int hat_densities(const spb_hat_desc *d, const T *const *mom, const T *const B[3
   g.inv[1] = d->invdy;
   g.inv[2] = d->invdz;
   const long cells = (long)g.nxc * g.nyc * g.nzc, nodes = (long)g.nxn * g.nyn * g.nzn;
-  T *tc = nullptr;   // the three centre temporaries
-  SPB_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tc), 3 * cells * sizeof(T), st));
+  const int ns = d->ns;
+  T *tc = nullptr;   // three centre temporaries per species
+  SPB_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tc), 3 * ns * cells * sizeof(T), st));
   Fill fc{g.nxc, g.nyc, g.nzc, 1, g.nyn - 1, {d->periodic[0], d->periodic[1], d->periodic[2]}};
   Fill fn{g.nxn, g.nyn, g.nzn, 2, g.nyn - 1, {d->periodic[0], d->periodic[1], d->periodic[2]}};
+  Species6<T> S;   // kernel parameters (copied at launch)
+  Arrays<T> A;
+  std::memset(&S, 0, sizeof(S));
+  std::memset(&A, 0, sizeof(A));
+  for (int is = 0; is < ns; ++is) {
+    const T *const *M = mom + 10 * is;
+    for (int c = 0; c < 6; ++c) S.p[is][c] = M[4 + c];
+    for (int r = 0; r < 3; ++r) {
+      S.j[is][r] = M[1 + r];
+      S.tc[is][r] = tc + (3 * is + r) * cells;
+      A.a[3 * is + r] = S.tc[is][r];
+    }
+    S.beta[is] = (T)(.5 * d->qom[is] * d->dt / d->c);
+  }
   const T alfa = (T)(-d->dt / 2.0);
   const long inner = (long)(g.nxc - 2) * (g.nyc - 2) * (g.nzc - 2);
   int rc = SPB_OK;
-  for (int is = 0; is < d->ns && rc == SPB_OK; ++is) {
-    const T *const *M = mom + 10 * is;
-    Tensor6<T> P{{M[4], M[5], M[6], M[7], M[8], M[9]}};
-    k_hat_div_tensor<T><<<blocks_for(inner, 256), 256, 0, st>>>(g, P, alfa, tc, tc + cells,
-                                                                 tc + 2 * cells);
-    k_hat_fill<T><<<3, 1024, 0, st>>>(fc, tc, tc + cells, tc + 2 * cells);
-    const T beta = (T)(.5 * d->qom[is] * d->dt / d->c);
-    k_hat_pidot<T><<<blocks_for(nodes, 256), 256, 0, st>>>(
-        g, Vec3<T>{{tc, tc + cells, tc + 2 * cells}}, Vec3<T>{{M[1], M[2], M[3]}},
-        Vec3<T>{{B[0], B[1], B[2]}}, beta, is == 0 ? 1 : 0, Out3<T>{{jxh, jyh, jzh}});
-    if (cudaGetLastError() != cudaSuccess) rc = fail(SPB_ERR_CUDA, "spb_hat_densities: launch");
-  }
-  if (rc == SPB_OK) {
-    k_hat_fill<T><<<3, 1024, 0, st>>>(fn, jxh, jyh, jzh);
-    k_hat_rho<T><<<blocks_for(cells, 256), 256, 0, st>>>(g, Vec3<T>{{jxh, jyh, jzh}}, rhoc,
-                                                         d->dt * d->th, rhoh);
-    k_hat_fill<T><<<1, 1024, 0, st>>>(fc, rhoh, (T *)nullptr, (T *)nullptr);
-    if (cudaGetLastError() != cudaSuccess) rc = fail(SPB_ERR_CUDA, "spb_hat_densities: launch");
-    g_launches += 3 * d->ns + 3;
-  }
+  const int gx = std::max(1, blocks_for(inner, 256) / ns);
+  k_hat_div_tensor<T><<<dim3(gx, ns), 256, 0, st>>>(g, S, alfa);
+  k_hat_fill<T><<<3 * ns, 1024, 0, st>>>(fc, A);
+  k_hat_pidot<T><<<blocks_for(nodes, 256), 256, 0, st>>>(g, S, ns, Vec3<T>{{B[0], B[1], B[2]}},
+                                                         Out3<T>{{jxh, jyh, jzh}});
+  Arrays<T> J{};
+  J.a[0] = jxh;
+  J.a[1] = jyh;
+  J.a[2] = jzh;
+  k_hat_fill<T><<<3, 1024, 0, st>>>(fn, J);
+  k_hat_rho<T><<<blocks_for(cells, 256), 256, 0, st>>>(g, Vec3<T>{{jxh, jyh, jzh}}, rhoc,
+                                                       d->dt * d->th, rhoh);
+  Arrays<T> R{};
+  R.a[0] = rhoh;
+  k_hat_fill<T><<<1, 1024, 0, st>>>(fc, R);
+  if (cudaGetLastError() != cudaSuccess) rc = fail(SPB_ERR_CUDA, "spb_hat_densities: launch");
+  g_launches += 6;
   cudaFreeAsync(tc, st);
   return rc;
 }
