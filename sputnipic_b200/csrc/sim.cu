@@ -886,17 +886,20 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
     float2 acc[40];
 #pragma unroll
     for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
-    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, a1 = a, b1 = a;
     if (n1 > 0) ld_rec(rec, a, b);
+    if (n1 > 1) ld_rec(rec + 2, a1, b1);
 #pragma unroll 1
     for (int k = 0; k < trips; ++k) {
-      // the next record loads while this one is summed; lanes past their
+      // two records in flight while this one is summed; lanes past their
       // count add zero terms
-      float4 na = a, nb = b;
-      if (k + 1 < n1) ld_rec(rec + 2 * (k + 1), na, nb);
+      float4 na = a1, nb = b1;
+      if (k + 2 < n1) ld_rec(rec + 2 * (k + 2), na, nb);
       add_terms(acc, k < n1 ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, 0);
-      a = na;
-      b = nb;
+      a = a1;
+      b = b1;
+      a1 = na;
+      b1 = nb;
     }
     if (own) {
 #pragma unroll
