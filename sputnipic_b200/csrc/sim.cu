@@ -194,6 +194,12 @@ struct Field6 {
   float2 exy, ezbx, byz;
 };
 
+__device__ __forceinline__ Field6 first_node(float w, float4 a, float2 b) {
+  const float2 w2 = make_float2(w, w);
+  return {__fmul2_rn(w2, make_float2(a.x, a.y)), __fmul2_rn(w2, make_float2(a.z, a.w)),
+          __fmul2_rn(w2, b)};
+}
+
 __device__ __forceinline__ void acc_node(Field6 &F, float w, float4 a, float2 b) {
   const float2 w2 = make_float2(w, w);
   F.exy = __ffma2_rn(w2, make_float2(a.x, a.y), F.exy);
@@ -250,7 +256,6 @@ __device__ __forceinline__ Field6 gather(const float *__restrict__ sF, int n0, f
   Field6 F[2];
 #pragma unroll
   for (int a = 0; a < 2; ++a) {
-    F[a] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
       const float wab = wx[a] * wy[b];
@@ -259,7 +264,10 @@ __device__ __forceinline__ Field6 gather(const float *__restrict__ sF, int n0, f
         const int n = n0 + (a * T::BY + b) * T::BZ + c;
         const float4 A = *reinterpret_cast<const float4 *>(sF + 8 * n);
         const float2 B = *reinterpret_cast<const float2 *>(sF + 8 * n + 4);
-        acc_node(F[a], wab * wz[c], A, B);
+        if (b == 0 && c == 0)   // each layer's sum starts from its first product
+          F[a] = first_node(wab * wz[c], A, B);
+        else
+          acc_node(F[a], wab * wz[c], A, B);
       }
     }
   }
@@ -279,53 +287,79 @@ __device__ __forceinline__ int tile_node(int c0x, int c0y, int c0z, int gx, int 
   return inbox ? (bx * T::BY + by) * T::BZ + bz : 0;
 }
 
+// One NiterMover step from the field F at the predicted position: the
+// implicit velocity solve (src/Mover.cpp:60-89), giving u-tilde and the
+// half-step displacement in cells.
+__device__ __forceinline__ void boris(const CycleParams &P, const Field6 &F, float qomdt2,
+                                      float u, float v, float w, float &up, float &vp, float &wp,
+                                      float &dx, float &dy, float &dz) {
+  const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
+  const float bx = F.ezbx.y, by = F.byz.x, bz = F.byz.y;
+  const float omdtsq = qomdt2 * qomdt2 * (bx * bx + by * by + bz * bz);
+  const float denom = __fdividef(1.0f, 1.0f + omdtsq);
+  const float ut = fmaf(qomdt2, ex, u);
+  const float vt = fmaf(qomdt2, ey, v);
+  const float wt = fmaf(qomdt2, ez, w);
+  const float qud = qomdt2 * (ut * bx + vt * by + wt * bz);
+  up = fmaf(qomdt2, vt * bz - wt * by + qud * bx, ut) * denom;
+  vp = fmaf(qomdt2, wt * bx - ut * bz + qud * by, vt) * denom;
+  wp = fmaf(qomdt2, ut * by - vt * bx + qud * bz, wt) * denom;
+  dx = up * P.hdt[0];
+  dy = vp * P.hdt[1];
+  dz = wp * P.hdt[2];
+}
+
+// Field at (cell g, fraction f): from the staged tile at node n0 when the
+// cell's nodes are staged (inbox), from HBM/L2 for the lanes whose are not.
+// All 32 lanes call.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ Field6 field_at(const CycleParams &P, const float *__restrict__ sF,
+                                           int n0, bool inbox, int gx, int gy, int gz, float fx,
+                                           float fy, float fz) {
+  Field6 F = gather<TX, TY, TZ>(sF, n0, fx, fy, fz);
+  if (__any_sync(0xffffffffu, !inbox)) {
+    if (!inbox)
+      F = gather_global(P.fields8, P.nxc, P.nyc, P.nzc, P.nyn, P.nzn, gx, gy, gz, fx, fy, fz);
+  }
+  return F;
+}
+
 // mover_PC for one particle in cell units (src/Mover.cpp:33-157). n0c is the
 // tile node of the particle's start cell (the first gather is there, at the
-// stored offsets), or -1 when the start cell is not known to be staged. All 32 lanes of the warp must call (the gathers vote:
-// lanes whose cell lies past the staged halo re-gather from HBM/L2).
+// stored offsets), or -1 when the start cell is not known to be staged. All
+// 32 lanes of the warp must call (the gathers vote: lanes whose cell lies
+// past the staged halo re-gather from HBM/L2). P.niter >= 1.
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ void push(const CycleParams &P, const float *__restrict__ sF, int c0x,
                                      int c0y, int c0z, int n0c, float qomdt2, int &cx, int &cy,
                                      int &cz, float &ox, float &oy, float &oz, float &u, float &v,
                                      float &w, int &bad) {
-  float dx = 0.f, dy = 0.f, dz = 0.f;   // predicted displacement in cells
-  float up = 0.f, vp = 0.f, wp = 0.f;
-#pragma unroll 1
-  for (int it = 0; it < P.niter; ++it) {
-    int gx = cx, gy = cy, gz = cz;
-    float fx = ox, fy = oy, fz = oz;
-    int n0 = n0c;
+  float dx, dy, dz;   // predicted displacement in cells
+  float up, vp, wp;
+  {
+    // the first iteration gathers at the stored position, in the start cell
     bool inbox = true;
-    if (it > 0) {
-      locate(ox + dx, cx, P.lim[0], gx, fx);
-      locate(oy + dy, cy, P.lim[1], gy, fy);
-      locate(oz + dz, cz, P.lim[2], gz, fz);
-      if (__any_sync(0xffffffffu, (gx | gy | gz) < 0)) {   // some lane is below the domain
-        truncate_below(gx, fx);
-        truncate_below(gy, fy);
-        truncate_below(gz, fz);
-      }
+    int n0 = n0c;
+    if (n0c < 0) n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, cx, cy, cz, inbox);
+    const Field6 F = field_at<TX, TY, TZ>(P, sF, n0, inbox, cx, cy, cz, ox, oy, oz);
+    boris(P, F, qomdt2, u, v, w, up, vp, wp, dx, dy, dz);
+  }
+#pragma unroll 1
+  for (int it = 1; it < P.niter; ++it) {
+    int gx, gy, gz;
+    float fx, fy, fz;
+    locate(ox + dx, cx, P.lim[0], gx, fx);
+    locate(oy + dy, cy, P.lim[1], gy, fy);
+    locate(oz + dz, cz, P.lim[2], gz, fz);
+    if (__any_sync(0xffffffffu, (gx | gy | gz) < 0)) {   // some lane is below the domain
+      truncate_below(gx, fx);
+      truncate_below(gy, fy);
+      truncate_below(gz, fz);
     }
-    if (it > 0 || n0c < 0) n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, gx, gy, gz, inbox);
-    Field6 F = gather<TX, TY, TZ>(sF, n0, fx, fy, fz);
-    if (__any_sync(0xffffffffu, !inbox)) {
-      if (!inbox)
-        F = gather_global(P.fields8, P.nxc, P.nyc, P.nzc, P.nyn, P.nzn, gx, gy, gz, fx, fy, fz);
-    }
-    const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
-    const float bx = F.ezbx.y, by = F.byz.x, bz = F.byz.y;
-    const float omdtsq = qomdt2 * qomdt2 * (bx * bx + by * by + bz * bz);
-    const float denom = __fdividef(1.0f, 1.0f + omdtsq);
-    const float ut = fmaf(qomdt2, ex, u);
-    const float vt = fmaf(qomdt2, ey, v);
-    const float wt = fmaf(qomdt2, ez, w);
-    const float qud = qomdt2 * (ut * bx + vt * by + wt * bz);
-    up = fmaf(qomdt2, vt * bz - wt * by + qud * bx, ut) * denom;
-    vp = fmaf(qomdt2, wt * bx - ut * bz + qud * by, vt) * denom;
-    wp = fmaf(qomdt2, ut * by - vt * bx + qud * bz, wt) * denom;
-    dx = up * P.hdt[0];
-    dy = vp * P.hdt[1];
-    dz = wp * P.hdt[2];
+    bool inbox;
+    const int n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, gx, gy, gz, inbox);
+    const Field6 F = field_at<TX, TY, TZ>(P, sF, n0, inbox, gx, gy, gz, fx, fy, fz);
+    boris(P, F, qomdt2, u, v, w, up, vp, wp, dx, dy, dz);
   }
   u = 2.0f * up - u;
   v = 2.0f * vp - v;
