@@ -124,7 +124,10 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
 
 // floor(p) for |p| < 2^22 as a float (s) and an int, from one add rounded
 // toward -infinity against 1.5 * 2^23 (whose neighbours are the integers):
-// full-rate adds instead of a rounding instruction and a conversion.
+// full-rate adds instead of a rounding instruction and a conversion. For
+// |p| >= 2^22, infinities and NaN the int is at least 2^22 away from 0 (the
+// float bit patterns are ordered), so a particle that far out lands outside
+// any grid, where the range check flags it.
 __device__ __forceinline__ int floor_split(float p, float &s) {
   constexpr float M = 12582912.0f;   // 1.5 * 2^23
   const float t = __fadd_rd(p, M);
@@ -133,11 +136,11 @@ __device__ __forceinline__ int floor_split(float p, float &s) {
 }
 
 // Gather cell and fraction of a predicted position p (cells, relative to the
-// particle's cell c), rounding down; |p| is clamped to lim = N + 8. Cells
-// outside [-1, N] are left to the gather's bounds handling.
-__device__ __forceinline__ void locate(float p, int c, float lim, int &g, float &f) {
+// particle's cell c), rounding down. Cells outside [-1, N] are left to the
+// gather's bounds handling.
+__device__ __forceinline__ void locate(float p, int c, int &g, float &f) {
   float s;
-  g = c + floor_split(fminf(fmaxf(p, -lim), lim), s);
+  g = c + floor_split(p, s);
   f = p - s;
 }
 
@@ -175,12 +178,11 @@ __device__ __forceinline__ void bc_cell(int &c, float &o, float &vel, int N, int
   o = top ? 1.0f : o;
 }
 
-// Final position update on one axis: p = o + displacement, new cell and offset
-// (|p| clamped to lim = N + 8 for the cell).
-__device__ __forceinline__ void advance(int &c, float &o, float disp, float lim) {
+// Final position update on one axis: p = o + displacement, new cell and offset.
+__device__ __forceinline__ void advance(int &c, float &o, float disp) {
   const float p = o + disp;
   float s;
-  c += floor_split(fminf(fmaxf(p, -lim), lim), s);
+  c += floor_split(p, s);
   o = p - s;
   const bool wrap = o >= 1.0f;
   c = wrap ? c + 1 : c;
@@ -348,9 +350,9 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   for (int it = 1; it < P.niter; ++it) {
     int gx, gy, gz;
     float fx, fy, fz;
-    locate(ox + dx, cx, P.lim[0], gx, fx);
-    locate(oy + dy, cy, P.lim[1], gy, fy);
-    locate(oz + dz, cz, P.lim[2], gz, fz);
+    locate(ox + dx, cx, gx, fx);
+    locate(oy + dy, cy, gy, fy);
+    locate(oz + dz, cz, gz, fz);
     if (__any_sync(0xffffffffu, (gx | gy | gz) < 0)) {   // some lane is below the domain
       truncate_below(gx, fx);
       truncate_below(gy, fy);
@@ -364,9 +366,9 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   u = 2.0f * up - u;
   v = 2.0f * vp - v;
   w = 2.0f * wp - w;
-  advance(cx, ox, up * P.fdt[0], P.lim[0]);
-  advance(cy, oy, vp * P.fdt[1], P.lim[1]);
-  advance(cz, oz, wp * P.fdt[2], P.lim[2]);
+  advance(cx, ox, up * P.fdt[0]);
+  advance(cy, oy, vp * P.fdt[1]);
+  advance(cz, oz, wp * P.fdt[2]);
   // the particle BC, the range flag and the clamps change nothing for a
   // particle whose new cell is inside the domain: skipped unless some lane
   // needs them
@@ -1504,7 +1506,6 @@ CycleParams make_params(spb_sim *s) {
     P.periodic[a] = s->d.periodic[a] ? 1 : 0;
     P.hdt[a] = (float)(0.5 * s->d.dt / s->dxyz[a]);
     P.fdt[a] = (float)(s->d.dt / s->dxyz[a]);
-    P.lim[a] = (float)(s->N[a] + 8);
   }
   P.scale = 1.0 / (s->dxyz[0] * s->dxyz[1] * s->dxyz[2]);
   P.fields8 = s->fields8;

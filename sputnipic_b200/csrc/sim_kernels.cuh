@@ -61,7 +61,6 @@ struct CycleParams {
   int periodic[3];
   float hdt[3];               // (dt/2)/d per axis: half-step displacement per unit velocity
   float fdt[3];               // dt/d per axis
-  float lim[3];               // N + 8 per axis: displacement clamp of locate/advance
   double scale;               // invVOL in double, applied when cell sums reach the moments
   const float *fields8;       // packed node fields in HBM (gathers past the staged tile)
   int *err;
