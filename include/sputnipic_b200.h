@@ -265,7 +265,9 @@ typedef struct spb_sim_desc {
   long capacity[SPB_SIM_MAX_SPECIES]; /* optional: particles to reserve for */
   int tile[3];              /* cells per tile (0,0,0: default 8x4x4) */
   int resort_every;         /* cycles between overflow checks (>= 1): a species
-                               whose overflow list is in use is re-laid out */
+                               whose overflow list holds more than 1/256 of
+                               its particles (at least 256, at most a quarter
+                               of the list) is re-laid out */
   int ctas;                 /* persistent CTAs of the push (0: per variant) */
   int variant;              /* push kernel residency: 0 three CTAs per SM (up
                                to 80 registers, 2 KB record-ring halves),
@@ -273,7 +275,7 @@ typedef struct spb_sim_desc {
                                64, 2 KB halves) */
   int bucket_slots;         /* record slots of every cell's bucket (0: each
                                cell's count at the last layout + max(16,
-                               count/4), rounded up to 4) */
+                               count/2), rounded up to 4) */
   int graph;                /* 1: each cycle's launches (zeroing, push,
                                deposit) replay as a CUDA graph captured per
                                buffer-parity pattern; not while timing */
@@ -299,8 +301,9 @@ int spb_sim_load_species(spb_sim *sim, int species, const float *x, const float 
                          void *stream);
 /* ncycles of mover + deposit for all species (the last cycle's moments
  * remain). Every desc.resort_every cycles the overflow lists are checked
- * (a synchronisation) and species using theirs are re-laid out, which
- * resizes every cell's bucket to its current count plus slack. */
+ * (a synchronisation) and species whose list is past its threshold are
+ * re-laid out, which resizes every cell's bucket to its current count plus
+ * slack. Overflow entries are pushed and deposited exactly in the meantime. */
 int spb_sim_cycle(spb_sim *sim, int ncycles, void *stream);
 /* Re-lay out every species now: buckets sized from the current counts, the
  * buckets and the overflow list copied into them (synchronises `stream`). */

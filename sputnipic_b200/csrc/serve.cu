@@ -238,7 +238,8 @@ extern "C" int spb_serve_step(spb_serve *s) {
   }
   lap(0);
   if (s->active.empty()) return 0;
-  // overflow lists in use: re-lay out those jobs (one synchronisation for all)
+  // overflow lists past their threshold: re-lay out those jobs (one
+  // synchronisation for all)
   if (s->steps > 0 && s->steps % s->d.check_every == 0) {
     int k = 0;
     for (ServeJob *j : s->active)
@@ -249,7 +250,8 @@ extern "C" int spb_serve_step(spb_serve *s) {
     k = 0;
     for (ServeJob *j : s->active) {
       bool over = false;
-      for (size_t i = 0; i < j->sim->sp.size(); ++i) over |= s->h_ovf[k++] > 0;
+      for (size_t i = 0; i < j->sim->sp.size(); ++i)
+        over |= s->h_ovf[k++] > spb::relayout_threshold(j->sim->sp[i]);
       if (over)
         if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
     }

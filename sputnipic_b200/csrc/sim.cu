@@ -1140,14 +1140,14 @@ __global__ void k_count_overflow(const int *__restrict__ okey, const int *__rest
 }
 
 // Bucket capacity of each cell from its particle count: fixed (`fixed` > 0)
-// or the count plus max(16, count/4) slots, rounded up to a multiple of 4
+// or the count plus max(16, count/2) slots, rounded up to a multiple of 4
 // (128-byte aligned buckets).
 __global__ void k_capacity(const int *__restrict__ count, long ncells, int fixed,
                            long long *__restrict__ cap) {
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < ncells;
        k += (long)gridDim.x * blockDim.x) {
     const long long c = count[k];
-    cap[k] = fixed > 0 ? fixed : ((c + max(16LL, c / 4) + 3) / 4) * 4;
+    cap[k] = fixed > 0 ? fixed : ((c + max(16LL, c / 2) + 3) / 4) * 4;
   }
 }
 
@@ -2284,6 +2284,15 @@ extern "C" int spb_sim_resort(spb_sim *s, void *stream) {
   return SPB_OK;
 }
 
+namespace spb {
+// Overflow entries at which a species is re-laid out: 1/256 of its particles
+// (at least 256), at most a quarter of the overflow list, so that the list
+// keeps room for the cycles until the next check.
+long relayout_threshold(const SimSpecies &q) {
+  return std::min<long>(q.ocap / 4, std::max<long>(256, q.n / 256));
+}
+}  // namespace spb
+
 extern "C" int spb_sim_cycle(spb_sim *s, int ncycles, void *stream) {
   if (!s || ncycles < 0) return fail(SPB_ERR_INVALID, "spb_sim_cycle: bad arguments");
   if (!s->fields_set) return fail(SPB_ERR_INVALID, "spb_sim_cycle: fields not set");
@@ -2292,13 +2301,15 @@ extern "C" int spb_sim_cycle(spb_sim *s, int ncycles, void *stream) {
   const int k = std::max(1, s->d.resort_every);
   for (int c = 0; c < ncycles; ++c) {
     if (s->cycles_since_check >= k) {
-      // re-lay out the species whose overflow list is in use
+      // re-lay out the species whose overflow list has grown past its
+      // threshold (the entries below it are pushed and deposited exactly,
+      // only more slowly)
       const cudaEvent_t b = record_event(s, st);
       bool any = false;
       for (int i = 0; i < (int)s->sp.size(); ++i) {
         const long o = spb_sim_overflow(s, i, stream);
         if (o < 0) return fail(SPB_ERR_CUDA, "spb_sim_cycle: overflow counter read failed");
-        if (o > 0) {
+        if (o > relayout_threshold(s->sp[i])) {
           drop_graphs(s);
           if (int rc = relayout(s, s->sp[i], st)) return rc;
           any = true;
