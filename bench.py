@@ -393,6 +393,10 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_hat:
         hat = measure_hat(torch, wl)
 
+    batching = None
+    if not args.no_batching:
+        batching = measure_batching(torch, rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         times, n, kind, cores = time_cpu(wl, args.cpu_slabs, 3, 1, min_seconds=10.0)
@@ -428,8 +432,31 @@ def run_ours(args, rank, world, local_rank):
                 "value": plain["value"], "unit": UNIT, "ms_per_step": plain["ms_per_step"],
                 "kernels": plain["kernels"], "speedup_of_precision_form": value / plain["value"]},
             "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "hat_densities": hat,
+            "batching": batching,
         }
         print(json.dumps(line), flush=True)
+
+
+def measure_batching(torch, rank):
+    """The batching form: 4 species of uneven counts (65.5M, 65.5M, 6.55M,
+    6.55M) on the GEM grid, 20 cycles from the loaded state, tile shape, push
+    residency and overflow-check interval k in {1, 2, 4, 8} picked by the
+    autotuner (sputnipic_b200.sim.autotune_batching)."""
+    from sputnipic_b200.device import gen_fields, gen_particles
+    from sputnipic_b200.sim import autotune_batching
+    wl = R.rank_workload(W.batching_gem(), rank)
+    fields = gen_fields(wl)
+    parts = [gen_particles(wl, s) for s in range(len(wl.species))]
+    tune = autotune_batching(wl, fields, parts, cycles=wl.cycles)
+    del parts, fields
+    torch.cuda.empty_cache()
+    counts = [wl.species_count(s) for s in range(len(wl.species))]
+    return {"workload": f"{wl.name}: species of {', '.join(f'{c:,}' for c in counts)} "
+                        f"particles, {wl.cycles} cycles, CUDA graphs",
+            "value": tune["particles_per_s"], "unit": UNIT,
+            "ms_per_cycle": tune["ms"] / tune["cycles"], "tile": tune["tile"],
+            "push_variant": tune["variant"], "check_every": tune["check_every"],
+            "intervals": tune["intervals"], "tile_trials": tune["tile_trials"]}
 
 
 def measure_hat(torch, wl, reps=10, warmup=3):
@@ -551,6 +578,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-hat", action="store_true",
                     help="skip the calculateHatDensities measurement")
+    ap.add_argument("--no-batching", action="store_true",
+                    help="skip the batching-form measurement (uneven species, autotuned)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -174,3 +174,38 @@ def autotune(wl, fields, parts, tiles=((8, 4, 4), (4, 4, 4), (8, 8, 4)), variant
     torch.cuda.synchronize()
     return {"tile": best[1], "variant": best[2], "cycle_ms": best[0], "trials": trials,
             "particles": n}
+
+
+def autotune_batching(wl, fields, parts, cycles=20, intervals=(1, 2, 4, 8), graph=True,
+                      stream=None):
+    """The batching form's autotuner: tile shape and push residency as
+    ``autotune`` picks them, then the overflow-check (re-layout) interval k
+    from ``intervals`` by timing ``cycles`` cycles from the loaded state with
+    each (CUDA events around the whole run: cycles, checks and re-layouts).
+    Returns the choice, the best run's milliseconds and all trials."""
+    import torch
+    tune = autotune(wl, fields, parts, stream=stream)
+    n = tune["particles"]
+    runs = []
+    for k in intervals:
+        sim = Simulation(wl, tile=tune["tile"], resort_every=k, variant=tune["variant"],
+                         graph=graph)
+        sim.set_fields(fields)
+        for s, p in enumerate(parts):
+            sim.load_species(s, p)
+        st = torch.cuda.current_stream() if stream is None else stream
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(st)
+        sim.cycle(cycles, stream=st)
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        assert sim.check() == 0
+        sim.close()
+        runs.append({"check_every": k, "ms": ms, "particles_per_s": n * cycles / (ms * 1e-3)})
+    best = min(runs, key=lambda r: r["ms"])
+    return {"tile": list(tune["tile"]), "variant": tune["variant"],
+            "check_every": best["check_every"], "ms": best["ms"], "cycles": cycles,
+            "particles": n, "particles_per_s": best["particles_per_s"], "intervals": runs,
+            "tile_trials": tune["trials"]}
