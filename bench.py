@@ -386,7 +386,9 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_serving:
         # independent replicas under torchrun; rank 0 reports its own
         from sputnipic_b200.serve import measure_stream
-        serving = measure_stream(rate=args.serve_rate, njobs=args.serve_jobs)
+        serving = measure_stream(njobs=args.serve_jobs,
+                                 rates=[args.serve_rate] + [r for r in (50.0, 200.0, 500.0)
+                                                            if r != args.serve_rate])
         torch.cuda.empty_cache()
 
     hat = None
@@ -573,7 +575,9 @@ def main():
                     help="launch each cycle directly instead of replaying a CUDA graph")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the serving stream (Poisson arrivals of mixed jobs)")
-    ap.add_argument("--serve-rate", type=float, default=10.0, help="serving arrivals, jobs/s")
+    ap.add_argument("--serve-rate", type=float, default=10.0,
+                    help="serving arrivals, jobs/s (the headline rate; 50, 200 and 500 jobs/s "
+                         "are swept too)")
     ap.add_argument("--serve-jobs", type=int, default=100, help="jobs in the serving stream")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-hat", action="store_true",

@@ -221,11 +221,13 @@ def device_jobs(configs):
     return jobs
 
 
-def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4)):
-    """Poisson stream of `njobs` jobs at `rate` jobs/s drawn from a seeded mix
-    of configurations. Every configuration is also run alone (its single-job
-    latency). Returns latency percentiles, slowdowns against running alone and
-    the aggregate throughput in particle-cycles per second."""
+def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), rates=None):
+    """Poisson streams of `njobs` jobs drawn from a seeded mix of
+    configurations, at `rate` jobs/s or at each of `rates`. Every
+    configuration is also run alone (its single-job latency). Returns per
+    rate the latency percentiles, slowdowns against running alone and the
+    aggregate throughput in particle-cycles per second (the first rate's also
+    at the top level)."""
     import numpy as np
     configs = job_mix(n_configs, seed)
     pool = device_jobs(configs)
@@ -237,37 +239,45 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4)):
         assert done[0].status == DONE
         alone.append(done[0].latency)
     # warm-up burst: every configuration at once, so the device memory pool has
-    # grown to a mix's footprint before the timed stream
+    # grown to a mix's footprint before the timed streams
     srv = Server(tile=tile)
     run_stream(srv, pool, [0.0] * len(pool))
     srv.close()
-    rng = np.random.default_rng(seed + 1)
-    pick = rng.integers(0, len(pool), size=njobs)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=njobs))
-    arrivals -= arrivals[0]
-    jobs = [pool[i] for i in pick]
-    srv = Server(tile=tile)
-    done, wall = run_stream(srv, jobs, list(arrivals))
-    stats = srv.stats()
-    stats["release_s"] = srv.release_s
-    srv.close()
     index = {id(j): k for k, j in enumerate(pool)}
-    ok = [d for d in done if d.status == DONE]
-    lat = np.array([d.latency for d in ok])
-    slow = np.array([d.latency / alone[index[id(d.job)]] for d in ok])
-    work = sum(d.job.particles() * d.job.ncycles for d in ok)
-    return {
-        "jobs": njobs, "completed": len(ok), "rate_jobs_per_s": rate,
-        "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
-                       "p99": 1e3 * float(np.percentile(lat, 99))},
+    sweep = []
+    for r in (rates or [rate]):
+        rng = np.random.default_rng(seed + 1)
+        pick = rng.integers(0, len(pool), size=njobs)
+        arrivals = np.cumsum(rng.exponential(1.0 / r, size=njobs))
+        arrivals -= arrivals[0]
+        jobs = [pool[i] for i in pick]
+        srv = Server(tile=tile)
+        done, wall = run_stream(srv, jobs, list(arrivals))
+        stats = srv.stats()
+        stats["release_s"] = srv.release_s
+        srv.close()
+        ok = [d for d in done if d.status == DONE]
+        lat = np.array([d.latency for d in ok])
+        slow = np.array([d.latency / alone[index[id(d.job)]] for d in ok])
+        work = sum(d.job.particles() * d.job.ncycles for d in ok)
+        sweep.append({
+            "rate_jobs_per_s": r, "jobs": njobs, "completed": len(ok),
+            "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
+                           "p99": 1e3 * float(np.percentile(lat, 99))},
+            "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
+                                  "p99": float(np.percentile(slow, 99))},
+            "throughput_particle_cycles_per_s": work / wall, "wall_s": wall, "engine": stats})
+    out = dict(sweep[0])
+    out.update({
         "single_job_latency_ms": {"p50": 1e3 * float(np.percentile(alone, 50)),
                                   "p99": 1e3 * float(np.percentile(alone, 99))},
-        "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
-                              "p99": float(np.percentile(slow, 99))},
-        "throughput_particle_cycles_per_s": work / wall,
-        "wall_s": wall, "engine": stats,
+        "p99_over_single_job_p99": sweep[0]["latency_ms"]["p99"] / (1e3 * float(np.percentile(alone, 99))),
         "mix": f"{n_configs} configurations: grids {list(SERVING_GRIDS)} "
                f"(weights {list(SERVING_GRID_WEIGHTS)}), ppc from {list(SERVING_PPC)} "
                "(capped at 5M particles per species), 2 or 4 species, 1-50 cycles, "
-               "frozen GEM fields; Poisson arrivals",
-    }
+               "frozen GEM fields; Poisson arrivals"})
+    if rates:
+        out["sweep"] = [{k: v for k, v in e.items() if k != "engine"} for e in sweep]
+        for e in out["sweep"]:
+            e["p99_over_single_job_p99"] = e["latency_ms"]["p99"] / out["single_job_latency_ms"]["p99"]
+    return out
