@@ -354,12 +354,20 @@ int spb_sim_kernel_timing(spb_sim *sim, double *push_ms, double *deposit_ms,
  * ------------------------------------------------------------------------- */
 typedef struct spb_serve spb_serve;
 
+/* Returns the device memory that the library's allocation pool holds but no
+ * simulation uses (after a device synchronisation). Simulations keep freed
+ * memory in the pool, so that creating and destroying them maps nothing. */
+int spb_release_cached_memory(void);
+
 typedef struct spb_serve_desc {
   int tile[3];              /* tile shape of every job (0,0,0: 4x4x4) */
   long long hbm_budget;     /* bytes the admitted jobs may hold (0: 90% of the
                                free device memory at creation) */
   int max_jobs;             /* jobs per launch (0 or above 64: 64) */
   int check_every;          /* steps between overflow checks (0: 4) */
+  long long reserve_bytes;  /* device memory the library's pool maps up front
+                               (0: none), so that admitting jobs maps nothing;
+                               spb_release_cached_memory gives it back */
 } spb_serve_desc;
 
 typedef struct spb_job_desc {

@@ -163,7 +163,7 @@ class HatDesc(ctypes.Structure):
 class ServeDesc(ctypes.Structure):
     """spb_serve_desc of include/sputnipic_b200.h."""
     _fields_ = [("tile", c_int * 3), ("hbm_budget", ctypes.c_longlong), ("max_jobs", c_int),
-                ("check_every", c_int)]
+                ("check_every", c_int), ("reserve_bytes", ctypes.c_longlong)]
 
 
 class JobDesc(ctypes.Structure):
@@ -269,6 +269,7 @@ def load():
     for fp in ("f32", "f64"):
         _proto(lib, "spb_hat_densities_" + fp, c_int, [R(HatDesc), P, P, P, P, P, P, P, P])
     _proto(lib, "spb_serve_create", c_int, [R(ServeDesc), R(P)])
+    _proto(lib, "spb_release_cached_memory", c_int, [])
     _proto(lib, "spb_serve_destroy", None, [P])
     _proto(lib, "spb_serve_submit", c_long, [P, R(JobDesc), P, P, P, c_int])
     _proto(lib, "spb_serve_step", c_int, [P])

@@ -161,6 +161,8 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
     SPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     s->budget = (long long)(0.9 * (double)free_b);
   }
+  if (d.reserve_bytes < 0) return fail(SPB_ERR_INVALID, "spb_serve_create: negative reserve");
+  if (d.reserve_bytes > 0) pool_reserve(std::min(d.reserve_bytes, s->budget));
   s->t0 = Clock::now();
   *out = s.release();
   return SPB_OK;

@@ -2285,6 +2285,25 @@ extern "C" int spb_sim_resort(spb_sim *s, void *stream) {
 }
 
 namespace spb {
+// Maps up to `bytes` of device memory into the pool (chunks allocated and
+// freed again; the pool keeps them). Stops quietly at the first chunk that
+// does not fit.
+void pool_reserve(long long bytes) {
+  cudaStream_t st = pool_stream();
+  std::vector<void *> chunks;
+  const long long chunk = 1LL << 30;
+  for (long long got = 0; got < bytes; got += chunk) {
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, (size_t)std::min(chunk, bytes - got), st) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    chunks.push_back(p);
+  }
+  for (void *p : chunks) cudaFreeAsync(p, st);
+  cudaStreamSynchronize(st);
+}
+
 // Overflow entries at which a species is re-laid out: 1/256 of its particles
 // (at least 256), at most a quarter of the overflow list, so that the list
 // keeps room for the cycles until the next check.
@@ -2292,6 +2311,16 @@ long relayout_threshold(const SimSpecies &q) {
   return std::min<long>(q.ocap / 4, std::max<long>(256, q.n / 256));
 }
 }  // namespace spb
+
+extern "C" int spb_release_cached_memory(void) {
+  SPB_CUDA(cudaDeviceSynchronize());
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  SPB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  SPB_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return SPB_OK;
+}
 
 extern "C" int spb_sim_cycle(spb_sim *s, int ncycles, void *stream) {
   if (!s || ncycles < 0) return fail(SPB_ERR_INVALID, "spb_sim_cycle: bad arguments");

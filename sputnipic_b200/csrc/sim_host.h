@@ -92,6 +92,7 @@ namespace spb {
 // Kernel parameters of a simulation's next cycle (reads buffer set cur).
 CycleParams make_params(spb_sim *s);
 long relayout_threshold(const SimSpecies &q);
+void pool_reserve(long long bytes);
 
 // One cycle of n simulations (all with the same tile shape) in one launch
 // each of zeroing, push and deposit; flips their buffer sets.

@@ -49,12 +49,14 @@ class Finished:
 
 
 class Server:
-    def __init__(self, tile=(4, 4, 4), hbm_budget=0, max_jobs=64, check_every=4):
+    def __init__(self, tile=(4, 4, 4), hbm_budget=0, max_jobs=64, check_every=4,
+                 reserve_bytes=0):
         self.lib = _lib.load()
         d = _lib.ServeDesc()
         for a in range(3):
             d.tile[a] = tile[a]
         d.hbm_budget, d.max_jobs, d.check_every = int(hbm_budget), max_jobs, check_every
+        d.reserve_bytes = int(reserve_bytes)
         h = ctypes.c_void_p()
         _lib.check(self.lib.spb_serve_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h
@@ -150,6 +152,12 @@ class Server:
                 "retire_s": t[4]}
 
 
+def release_cached_memory():
+    """Hands the device memory the library's pool keeps for reuse back
+    (spb_release_cached_memory)."""
+    _lib.check(_lib.load().spb_release_cached_memory())
+
+
 def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
     """The request loop. jobs[i] arrives `arrivals[i]` seconds after the start
     (sorted). Returns the finished jobs (with results for the indices in
@@ -238,10 +246,12 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         srv.close()
         assert done[0].status == DONE
         alone.append(done[0].latency)
-    # warm-up burst: every configuration at once, so the device memory pool has
-    # grown to a mix's footprint before the timed streams
+    # warm-up burst of a full launch's worth of jobs (every configuration,
+    # repeated), so the device memory pool has grown to a saturated engine's
+    # footprint before the timed streams
     srv = Server(tile=tile)
-    run_stream(srv, pool, [0.0] * len(pool))
+    burst = [pool[i % len(pool)] for i in range(max(len(pool), 64))]
+    run_stream(srv, burst, [0.0] * len(burst))
     srv.close()
     index = {id(j): k for k, j in enumerate(pool)}
     sweep = []
@@ -267,6 +277,7 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
             "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
                                   "p99": float(np.percentile(slow, 99))},
             "throughput_particle_cycles_per_s": work / wall, "wall_s": wall, "engine": stats})
+    release_cached_memory()
     out = dict(sweep[0])
     out.update({
         "single_job_latency_ms": {"p50": 1e3 * float(np.percentile(alone, 50)),

@@ -127,3 +127,11 @@ def test_grid_create_without_device_reports_no_device():
     lib = _lib.load()
     h = ctypes.c_void_p()
     assert lib.spb_grid_create_uniform(4, 4, 4, 1.0, 1.0, 1.0, ctypes.byref(h)) == 4
+
+
+def test_library_has_no_unresolved_internal_symbols():
+    """Every symbol of the library's own namespace is defined in it (a shared
+    library links with undefined symbols; loading would fail later)."""
+    out = subprocess.run(["nm", "-u", _lib.LIB_PATH], check=True, capture_output=True,
+                         text=True).stdout
+    assert not [line for line in out.splitlines() if "3spb" in line or " spb_" in line]
