@@ -227,9 +227,10 @@ struct Particle {
 // Adds one warp's deposits to the moments. For each of up to four distinct
 // cells among the warp's particles (cell-ordered particles give one or two),
 // the members compute their terms and the warp sums them (warp_sum80) and
-// issues 80 atomics; lone particles of further cells (unordered input) issue
-// 80 atomics each. Terms are recomputed per round rather than kept, which
-// halves the registers. All 32 lanes call.
+// issues 80 atomics; the 80 terms of each lone particle of a further cell
+// (a particle that moved, unordered input) are spread over the warp, one
+// atomic each. Terms are recomputed per round rather than kept, which halves
+// the registers. All 32 lanes call.
 __device__ __forceinline__ void deposit_warp(const GeomDev &g, const MomStrided &M, bool valid,
                                              const Particle &p, int &bad) {
   const int lane = threadIdx.x & 31;
@@ -271,18 +272,47 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const MomStrided 
       if (i >= lo && i < hi) atomicAdd(M.base + (mbase + i) * M.stride + n, r[i]);
     if (member) valid = false;   // done
   }
-  if (valid) {
-    float2 t[40];
-    deposit_terms(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, ignored);
-    const int pa = (lane >> 4) & 1, pb = (lane >> 3) & 1, pc = (lane >> 2) & 1;
+  // lone particles of further cells, one at a time: the warp spreads the
+  // particle's 80 terms over its lanes (term j on lane j mod 32), each
+  // computed as deposit_terms does, and adds each with one atomic
+  unsigned lone = __ballot_sync(FULL, valid);
+  if (lone) {
+    const int ix = (int)(key / sx), iy = (int)((key / sy) % g.nyn), iz = (int)(key % sy);
+    float d[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // xi0, xi1, eta0, eta1, zeta0, zeta1
+    if (valid) {
+      d[0] = p.x - __ldg(g.xn + ix - 1);
+      d[1] = __ldg(g.xn + ix) - p.x;
+      d[2] = p.y - __ldg(g.yn + iy - 1);
+      d[3] = __ldg(g.yn + iy) - p.y;
+      d[4] = p.z - __ldg(g.zn + iz - 1);
+      d[5] = __ldg(g.zn + iz) - p.z;
+    }
+    const float inv = g.invVOL;
+    while (lone) {
+      const int L = __ffs(lone) - 1;
+      lone &= lone - 1;
+      float e[6];
 #pragma unroll
-    for (int node = 0; node < 8; ++node) {
-      const int a = (node >> 2) ^ pa, b = ((node >> 1) & 1) ^ pb, c = (node & 1) ^ pc;
-      const long n = key - a * sx - b * sy - c;
+      for (int j = 0; j < 6; ++j) e[j] = __shfl_sync(FULL, d[j], L);
+      const float q = __shfl_sync(FULL, p.q, L), u = __shfl_sync(FULL, p.u, L);
+      const float v = __shfl_sync(FULL, p.v, L), w = __shfl_sync(FULL, p.w, L);
+      const long k = __shfl_sync(FULL, key, L);
 #pragma unroll
-      for (int kk = 0; kk < 5; ++kk) {
-        atomicAdd(M.base + kk * M.stride + n, t[node * 5 + kk].x);
-        atomicAdd(M.base + (kk + 5) * M.stride + n, t[node * 5 + kk].y);
+      for (int r = 0; r < 3; ++r) {
+        const int t = lane + 32 * r;
+        if (t < 80) {
+          const int node = t / 10, m = t % 10;
+          const int a = node >> 2, b = (node >> 1) & 1, c = node & 1;
+          const float wgt = q * (a ? e[1] : e[0]) * (b ? e[3] : e[2]) * (c ? e[5] : e[4]) * inv;
+          // moment factor: 1, u, v, w, uu, uv, uw, vv, vw, ww (rhon's
+          // (1 * wgt) * inv is the reference's wgt * inv exactly)
+          const float s1 = m == 1 || m == 4 || m == 5 || m == 6 ? u
+                           : (m == 2 || m == 7 || m == 8 ? v : (m == 3 || m == 9 ? w : 1.0f));
+          const float s2 = m == 4 ? u : (m == 5 || m == 7 ? v : (m == 6 || m == 8 || m == 9 ? w : 1.0f));
+          const float fm = m >= 4 ? s1 * s2 : s1;
+          const float term = (fm * wgt) * inv;
+          atomicAdd(M.base + m * M.stride + (k - a * sx - b * sy - c), term);
+        }
       }
     }
   }
