@@ -1000,24 +1000,76 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
   }
 }
 
-// Overflow entries of every species of job P, one by one with FP64 atomics.
+// Overflow entries of every species of job P. Each warp takes 32 consecutive
+// entries; the push appends the particles of one slot that overflow the same
+// full bucket next to each other, so most entries of a warp share their cell.
+// Up to four groups of at least two entries with one cell are summed by the
+// warp in FP32 (warp_sum80) and added with one FP64 atomic per node and
+// moment; the remaining entries deposit one by one (deposit_global). Called
+// by whole warps.
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
+  const int lane = threadIdx.x & 31;
+  const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
+  const long gwarp = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long nodes = (long)P.nxn * P.nyn * P.nzn;
+  const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
+  // this lane's totals after warp_sum80: node corner (bit4, bit3, bit2),
+  // moments mbase + [lo, hi)
+  const int ca = (lane >> 4) & 1, cb = (lane >> 3) & 1, cc = (lane >> 2) & 1;
+  const int mbase = 5 * ((lane >> 1) & 1);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
-    const int on = min(*S.ocout, S.ocap);
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < on;
-         i += (long)gridDim.x * blockDim.x) {
-      int cx, cy, cz;
-      key_cell<TX, TY, TZ>(S.okout[i], P.nty, P.ntz, cx, cy, cz);
-      deposit_global(P, S, cx, cy, cz, S.oout[2 * i], S.oout[2 * i + 1]);
+    const long on = min(*S.ocout, S.ocap);
+    for (long base = gwarp * 32; base < on; base += nwarps * 32) {
+      const long i = base + lane;
+      bool valid = i < on;
+      int key = -1;
+      float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+      if (valid) {
+        key = S.okout[i];
+        a = S.oout[2 * i];
+        b = S.oout[2 * i + 1];
+      }
+      unsigned remaining = __ballot_sync(FULL, valid);
+      int groups = 0;
+#pragma unroll 1
+      while (remaining && groups < 4) {
+        const int leader = __ffs(remaining) - 1;
+        const int k = __shfl_sync(FULL, key, leader);
+        const bool member = valid && key == k;
+        const unsigned members = __ballot_sync(FULL, member);
+        remaining &= ~members;
+        if (__popc(members) < 2) continue;   // a lone entry: deposited below
+        ++groups;
+        float2 acc[40];
+#pragma unroll
+        for (int j = 0; j < 40; ++j) acc[j] = make_float2(0.f, 0.f);
+        add_terms(acc, member ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, lane);
+        float r[5];
+        warp_sum80(acc, r, lane);
+        int cx, cy, cz;
+        key_cell<TX, TY, TZ>(k, P.nty, P.ntz, cx, cy, cz);
+        const long n = (long)(cx + 1 + ca) * sx + (long)(cy + 1 + cb) * sy + (cz + 1 + cc);
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+          if (m >= lo && m < hi)
+            atomicAdd(S.mom + (mbase + m) * nodes + n, (double)r[m] * P.scale);
+        if (member) valid = false;
+      }
+      if (valid) {
+        int cx, cy, cz;
+        key_cell<TX, TY, TZ>(key, P.nty, P.ntz, cx, cy, cz);
+        deposit_global(P, S, cx, cy, cz, a, b);
+      }
     }
   }
 }
 
 // The deposit (interpP2G, src/Mover.cpp:385-572) for every species, from the
 // buckets the push wrote: persistent CTAs walk the tiles, one thread per cell
-// (deposit_tile). Overflow entries deposit one by one with FP64 atomics.
+// (deposit_tile); then the overflow entries (deposit_overflow).
 // MULTI as for k_push.
 template <int TX, int TY, int TZ, bool MULTI>
 __global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(), 512 / dep_tpb<TX, TY, TZ>())

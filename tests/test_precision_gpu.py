@@ -143,7 +143,9 @@ def test_edge_fixture_vs_reference_fp64(cuda, golden_edge, qi):
 def test_overflow_path_vs_fp64(cuda, orc64, slots, resort_every):
     """Buckets far smaller than the cells' counts (27 ppc on average): most
     particles live in the overflow list, are pushed with gathers from L2 and
-    deposited with FP64 atomics, and re-enter buckets when room appears. Ten
+    deposited by the overflow pass (groups of entries of one cell summed by
+    the warp, lone entries one by one; FP64 atomics), and re-enter buckets
+    when room appears. Ten
     cycles, with and without re-layouts in between; moments and tagged
     particles against the FP64 oracle."""
     torch = cuda
