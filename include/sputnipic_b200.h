@@ -211,11 +211,15 @@ int spb_grid_set_fields(spb_grid_ctx *ctx, const float *const fields[6],
 int spb_grid_mover(spb_grid_ctx *ctx, const spb_push *push, float *x, float *y,
                    float *z, float *u, float *v, float *w, long n, void *stream);
 /* interpP2G over n particles: ADDS into mom[0..9] (device, nodes floats each,
- * order rhon, Jx, Jy, Jz, pxx, pxy, pxz, pyy, pyz, pzz). */
+ * anywhere in memory; order rhon, Jx, Jy, Jz, pxx, pxy, pxz, pyy, pyz, pzz).
+ * The deposit accumulates into a node-interleaved buffer (48 bytes per node,
+ * from the device's stream-ordered pool on `stream`), which a second kernel
+ * adds into the ten arrays. */
 int spb_grid_p2g(spb_grid_ctx *ctx, const float *x, const float *y,
                  const float *z, const float *u, const float *v, const float *w,
                  const float *q, long n, float *const mom[10], void *stream);
-/* mover_interp: move then deposit, one kernel. */
+/* mover_interp: move then deposit, one kernel (plus the accumulator fold, as
+ * spb_grid_p2g). */
 int spb_grid_mover_interp(spb_grid_ctx *ctx, const spb_push *push, float *x,
                           float *y, float *z, float *u, float *v, float *w,
                           const float *q, long n, float *const mom[10],

@@ -350,7 +350,7 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
       rc = launch_plain_p2g(ctx->geom, d[0], d[1], d[2], d[3], d[4], d[5], d[6], cnt, dm,
                             sp->d_err, s);
     if (rc) return rc;
-    ctx->launches++;
+    ctx->launches += deposits ? 2 : 1;   // a deposit folds its accumulator
     if (moves)
       for (int a = 0; a < 6; ++a)
         SPB_CUDA(cudaMemcpyAsync(h[a] + off, d[a], bytes, cudaMemcpyDeviceToHost, s));
@@ -432,13 +432,13 @@ int run(Op op, struct particles *part, struct EMfield *field, struct interpDensS
       rc = launch_plain_mover(ctx->geom, p, F, sp->d[0], sp->d[1], sp->d[2], sp->d[3], sp->d[4],
                               sp->d[5], n, sp->d_err, sp->stream, op == Op::MoverV ? 1 : 0);
     if (rc) return rc;
-    ctx->launches++;
+    ctx->launches += op == Op::Fused ? 2 : 1;
     SPB_CUDA(cudaStreamSynchronize(sp->stream));
   } else {
     rc = launch_plain_p2g(ctx->geom, sp->d[0], sp->d[1], sp->d[2], sp->d[3], sp->d[4], sp->d[5],
                           sp->d[6], n, dm, sp->d_err, sp->stream);
     if (rc) return rc;
-    ctx->launches++;
+    ctx->launches += 2;
   }
   // results back to the host
   if (deposits && !dev_mom)

@@ -212,7 +212,6 @@ extern "C" void spb_grid_destroy(spb_grid_ctx *c) {
   cudaFree(c->d_eb4);
   cudaFree(c->d_eb2);
   cudaFree(c->d_stage);
-  cudaFree(c->d_mom_tmp);
   cudaFree(c->d_net);
   cudaFree(c->d_err);
   delete c;
@@ -273,28 +272,6 @@ extern "C" int spb_grid_mover(spb_grid_ctx *c, const spb_push *push, float *x, f
   return rc;
 }
 
-namespace {
-// The deposit kernels need the ten moment arrays equally spaced. Arrays that
-// are not get a zeroed contiguous scratch in their place (added into them
-// after the deposit).
-int strided_or_scratch(spb_grid_ctx *c, float *const mom[10], float *tm[10], cudaStream_t st,
-                       float *const **dst) {
-  if (moments_strided(mom)) {
-    *dst = mom;
-    return SPB_OK;
-  }
-  if (!c->d_mom_tmp && cudaMalloc(&c->d_mom_tmp, 10 * c->nodes * sizeof(float)) != cudaSuccess) {
-    cudaGetLastError();
-    c->d_mom_tmp = nullptr;
-    return fail(SPB_ERR_ALLOC, "moment scratch allocation failed");
-  }
-  SPB_CUDA(cudaMemsetAsync(c->d_mom_tmp, 0, 10 * c->nodes * sizeof(float), st));
-  for (int m = 0; m < 10; ++m) tm[m] = c->d_mom_tmp + m * c->nodes;
-  *dst = tm;
-  return SPB_OK;
-}
-}  // namespace
-
 extern "C" int spb_grid_p2g(spb_grid_ctx *c, const float *x, const float *y, const float *z,
                             const float *u, const float *v, const float *w, const float *q,
                             long n, float *const mom[10], void *stream) {
@@ -304,12 +281,8 @@ extern "C" int spb_grid_p2g(spb_grid_ctx *c, const float *x, const float *y, con
   if (n < 0 || (n > 0 && (!x || !y || !z || !u || !v || !w || !q)))
     return fail(SPB_ERR_INVALID, "spb_grid_p2g: bad particle arrays");
   cudaStream_t st = (cudaStream_t)stream;
-  float *tm[10];
-  float *const *dst = mom;
-  if (int rc = strided_or_scratch(c, mom, tm, st, &dst)) return rc;
-  int rc = launch_plain_p2g(c->geom, x, y, z, u, v, w, q, n, dst, c->d_err, st);
-  if (!rc && dst != mom) rc = launch_add_moments(c->d_mom_tmp, c->nodes, mom, st);
-  if (!rc && n > 0) c->launches++;
+  int rc = launch_plain_p2g(c->geom, x, y, z, u, v, w, q, n, mom, c->d_err, st);
+  if (!rc && n > 0) c->launches += 2;
   return rc;
 }
 
@@ -325,13 +298,9 @@ extern "C" int spb_grid_mover_interp(spb_grid_ctx *c, const spb_push *push, floa
     return fail(SPB_ERR_INVALID, "spb_grid_mover_interp: bad particle arrays");
   const PushDev p = make_push(*push);
   cudaStream_t st = (cudaStream_t)stream;
-  float *tm[10];
-  float *const *dst = mom;
-  if (int rc = strided_or_scratch(c, mom, tm, st, &dst)) return rc;
   int rc = launch_plain_mover_interp(c->geom, p, PackedFields{c->d_eb4, c->d_eb2}, x, y, z, u, v,
-                                     w, q, n, dst, c->d_err, st);
-  if (!rc && dst != mom) rc = launch_add_moments(c->d_mom_tmp, c->nodes, mom, st);
-  if (!rc && n > 0) c->launches++;
+                                     w, q, n, mom, c->d_err, st);
+  if (!rc && n > 0) c->launches += 2;
   return rc;
 }
 

@@ -15,7 +15,6 @@ struct spb_grid_ctx {
   float4 *d_eb4 = nullptr;       // packed fields (Ex, Ey, Ez, Bx)
   float2 *d_eb2 = nullptr;       // packed fields (By, Bz)
   float *d_stage = nullptr;      // 6*nodes staging for host field uploads
-  float *d_mom_tmp = nullptr;    // 10*nodes: deposits for moment arrays not equally spaced
   float *d_net = nullptr;        // 10*nodes: net densities (sum over species)
   int *d_err = nullptr;
   bool fields_set = false;

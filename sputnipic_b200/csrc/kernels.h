@@ -22,14 +22,9 @@ size_t particle_sort_scratch_bytes(long n);
 int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const SortBins &B,
                          void *scratch, cudaStream_t st);
 
-// Whether mom[0..9] are equally spaced, as launch_plain_p2g and
-// launch_plain_mover_interp require.
-bool moments_strided(float *const mom[10]);
 // net[m*nodes + i] = sum over species s (in order) of bases[s][m*nodes + i].
 int launch_sum_species(const float *const *bases, int ns, long nodes, float *net,
                        cudaStream_t s);
-// mom[m][i] += src[m * nodes + i].
-int launch_add_moments(const float *src, long nodes, float *const mom[10], cudaStream_t s);
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
                      const float *u, const float *v, const float *w, const float *q, long n,
                      float *const mom[10], int *err, cudaStream_t s);

@@ -19,6 +19,8 @@
 #include "grid_ctx.h"
 #include "warp_sum.cuh"
 
+#include <atomic>
+
 namespace spb {
 
 namespace {
@@ -29,25 +31,6 @@ constexpr int TPB = 256;
 struct Moments10 {
   float *m[10];
 };
-
-// The ten moment arrays of a deposit, equally spaced: moment m of node n is
-// base[m * stride + n] (one pointer, so the kernels index it arithmetically
-// instead of through a per-lane index into an array of pointers).
-struct MomStrided {
-  float *base;
-  long stride;
-};
-
-// Whether mom[0..9] are equally spaced (a [10][nodes] buffer is).
-bool as_strided(float *const mom[10], MomStrided &M) {
-  const long step = (long)((intptr_t)mom[1] - (intptr_t)mom[0]);
-  if (step % (long)sizeof(float)) return false;
-  for (int m = 2; m < 10; ++m)
-    if ((intptr_t)mom[m] - (intptr_t)mom[0] != (intptr_t)(m * step)) return false;
-  M.base = mom[0];
-  M.stride = step / (long)sizeof(float);
-  return true;
-}
 
 // The double product (x - start) * inv, limited to [-8, n + 8] so that the
 // int conversion below never overflows (NaN maps to -8). Exact for every
@@ -224,15 +207,31 @@ struct Particle {
   float x, y, z, u, v, w, q;
 };
 
+// One 16-byte add to global memory (p 16-byte aligned): one L2 atomic
+// operation for four floats.
+__device__ __forceinline__ void red_v4(float *p, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b),
+               "f"(c), "f"(d)
+               : "memory");
+}
+
+// The plain deposit's accumulator: the ten moments of node n side by side,
+// acc[n * ACC_STRIDE + m] (m = rhon, Jx, Jy, Jz, pxx, pxy, pxz, pyy, pyz, pzz;
+// two pad floats keep every node's record on a 16-byte boundary). A
+// particle's 80 terms then land in about a dozen 32-byte sectors instead of
+// the forty that ten separate arrays take; k_fold_acc adds it into the ten
+// arrays afterwards.
+constexpr int ACC_STRIDE = 12;
+
 // Adds one warp's deposits to the moments. For each of up to four distinct
 // cells among the warp's particles (cell-ordered particles give one or two),
 // the members compute their terms and the warp sums them (warp_sum80) and
-// issues 80 atomics; the 80 terms of each lone particle of a further cell
-// (a particle that moved, unordered input) are spread over the warp, one
-// atomic each. Terms are recomputed per round rather than kept, which halves
-// the registers. All 32 lanes call.
-__device__ __forceinline__ void deposit_warp(const GeomDev &g, const MomStrided &M, bool valid,
-                                             const Particle &p, int &bad) {
+// adds the 40 z-node pairs of totals (add_pair); the 40 pairs of each lone
+// particle of a further cell (a particle that moved, unordered input) are
+// spread over the warp, one pair per lane. Terms are recomputed per round
+// rather than kept, which halves the registers. All 32 lanes call.
+__device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict__ acc,
+                                             bool valid, const Particle &p, int &bad) {
   const int lane = threadIdx.x & 31;
   const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
   long key = 0;
@@ -266,15 +265,15 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const MomStrided 
     }
     float r[5];
     warp_sum80(t, r, lane);
-    const long n = k - na * sx - nb * sy - nc;
+    float *const dst = acc + (k - na * sx - nb * sy - nc) * ACC_STRIDE + mbase;
 #pragma unroll
     for (int i = 0; i < 5; ++i)
-      if (i >= lo && i < hi) atomicAdd(M.base + (mbase + i) * M.stride + n, r[i]);
+      if (i >= lo && i < hi) atomicAdd(dst + i, r[i]);
     if (member) valid = false;   // done
   }
-  // lone particles of further cells, one at a time: the warp spreads the
-  // particle's 80 terms over its lanes (term j on lane j mod 32), each
-  // computed as deposit_terms does, and adds each with one atomic
+  // lone particles of further cells, one at a time: lane j < 24 takes node
+  // j / 3 and moments 4 (j % 3) .. 4 (j % 3) + 3 of the particle, each term
+  // computed as deposit_terms does, and adds them with one 16-byte add
   unsigned lone = __ballot_sync(FULL, valid);
   if (lone) {
     const int ix = (int)(key / sx), iy = (int)((key / sy) % g.nyn), iz = (int)(key % sy);
@@ -297,22 +296,19 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const MomStrided 
       const float q = __shfl_sync(FULL, p.q, L), u = __shfl_sync(FULL, p.u, L);
       const float v = __shfl_sync(FULL, p.v, L), w = __shfl_sync(FULL, p.w, L);
       const long k = __shfl_sync(FULL, key, L);
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        const int t = lane + 32 * r;
-        if (t < 80) {
-          const int node = t / 10, m = t % 10;
-          const int a = node >> 2, b = (node >> 1) & 1, c = node & 1;
-          const float wgt = q * (a ? e[1] : e[0]) * (b ? e[3] : e[2]) * (c ? e[5] : e[4]) * inv;
-          // moment factor: 1, u, v, w, uu, uv, uw, vv, vw, ww (rhon's
-          // (1 * wgt) * inv is the reference's wgt * inv exactly)
-          const float s1 = m == 1 || m == 4 || m == 5 || m == 6 ? u
-                           : (m == 2 || m == 7 || m == 8 ? v : (m == 3 || m == 9 ? w : 1.0f));
-          const float s2 = m == 4 ? u : (m == 5 || m == 7 ? v : (m == 6 || m == 8 || m == 9 ? w : 1.0f));
-          const float fm = m >= 4 ? s1 * s2 : s1;
-          const float term = (fm * wgt) * inv;
-          atomicAdd(M.base + m * M.stride + (k - a * sx - b * sy - c), term);
-        }
+      if (lane < 24) {
+        const int node = lane / 3, grp = lane % 3;
+        const int a = node >> 2, b = (node >> 1) & 1, c = node & 1;
+        const float wgt = q * (a ? e[1] : e[0]) * (b ? e[3] : e[2]) * (c ? e[5] : e[4]) * inv;
+        // moment factors of the group: (1, u, v, w), (uu, uv, uw, vv) or
+        // (vw, ww, 0, 0) (rhon's (1 * wgt) * inv is the reference's wgt * inv
+        // exactly; the pad slots add zeros)
+        const float f0 = grp == 0 ? 1.0f : (grp == 1 ? u * u : v * w);
+        const float f1 = grp == 0 ? u : (grp == 1 ? u * v : w * w);
+        const float f2 = grp == 0 ? v : (grp == 1 ? u * w : 0.0f);
+        const float f3 = grp == 0 ? w : (grp == 1 ? v * v : 0.0f);
+        red_v4(acc + (k - a * sx - b * sy - c) * ACC_STRIDE + 4 * grp, (f0 * wgt) * inv,
+               (f1 * wgt) * inv, (f2 * wgt) * inv, (f3 * wgt) * inv);
       }
     }
   }
@@ -360,20 +356,20 @@ __global__ void __launch_bounds__(TPB) k_plain_p2g(GeomDev g, const float *__res
                                                    const float *__restrict__ v,
                                                    const float *__restrict__ w,
                                                    const float *__restrict__ q, long n,
-                                                   MomStrided M, int *__restrict__ err) {
+                                                   float *__restrict__ acc, int *__restrict__ err) {
   const long i = blockIdx.x * (long)TPB + threadIdx.x;
   const bool valid = i < n;
   Particle p{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (valid) p = Particle{x[i], y[i], z[i], u[i], v[i], w[i], q[i]};
   int bad = 0;
-  deposit_warp(g, M, valid, p, bad);
+  deposit_warp(g, acc, valid, p, bad);
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
 __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
     GeomDev g, PushDev p, PackedFields F, float *__restrict__ x, float *__restrict__ y,
     float *__restrict__ z, float *__restrict__ u, float *__restrict__ v,
-    float *__restrict__ w, const float *__restrict__ q, long n, MomStrided M,
+    float *__restrict__ w, const float *__restrict__ q, long n, float *__restrict__ acc,
     int *__restrict__ err) {
   const long i = blockIdx.x * (long)TPB + threadIdx.x;
   const bool valid = i < n;
@@ -390,7 +386,7 @@ __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
     w[i] = pw;
     pt = Particle{px, py, pz, pu, pv, pw, q[i]};
   }
-  deposit_warp(g, M, valid, pt, bad);
+  deposit_warp(g, acc, valid, pt, bad);
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
@@ -417,13 +413,17 @@ __global__ void __launch_bounds__(TPB) k_sum_species(SpeciesBases S, int ns, lon
   }
 }
 
-// mom[m][i] += src[m * nodes + i] (moments deposited into a contiguous buffer)
-__global__ void __launch_bounds__(TPB) k_add_moments(const float *__restrict__ src, long nodes,
-                                                     Moments10 M) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nodes;
-       i += (long)gridDim.x * blockDim.x) {
+// mom[m][n] += acc[n * ACC_STRIDE + m] for the non-zero entries (atomically:
+// the two pipeline streams of the drop-in fold into the same arrays).
+__global__ void __launch_bounds__(TPB) k_fold_acc(const float4 *__restrict__ acc, long nodes,
+                                                  Moments10 M) {
+  for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < nodes;
+       n += (long)gridDim.x * blockDim.x) {
+    const float4 a = acc[3 * n], b = acc[3 * n + 1], c = acc[3 * n + 2];
+    const float v[10] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y};
 #pragma unroll
-    for (int m = 0; m < 10; ++m) M.m[m][i] += src[m * nodes + i];
+    for (int m = 0; m < 10; ++m)
+      if (v[m] != 0.0f) atomicAdd(M.m[m] + n, v[m]);
   }
 }
 
@@ -494,22 +494,6 @@ int launch_plain_mover(const GeomDev &g, const PushDev &p, const PackedFields &F
   return SPB_OK;
 }
 
-bool moments_strided(float *const mom[10]) {
-  MomStrided M;
-  return as_strided(mom, M);
-}
-
-int launch_add_moments(const float *src, long nodes, float *const mom[10], cudaStream_t s) {
-  if (nodes <= 0) return SPB_OK;
-  Moments10 M;
-  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
-  k_add_moments<<<(unsigned)std::min<long>(ceil_div(nodes, TPB), 4096), TPB, 0, s>>>(src, nodes,
-                                                                                     M);
-  SPB_CUDA(cudaGetLastError());
-  g_launches++;
-  return SPB_OK;
-}
-
 int launch_sum_species(const float *const *bases, int ns, long nodes, float *net,
                        cudaStream_t s) {
   if (ns < 1 || ns > SUM_MAX_SPECIES) return fail(SPB_ERR_UNSUPPORTED, "1..32 species");
@@ -522,17 +506,78 @@ int launch_sum_species(const float *const *bases, int ns, long nodes, float *net
   return SPB_OK;
 }
 
+namespace {
+// The device's stream-ordered pool keeps freed memory for reuse (once per
+// device), so the per-deposit accumulators map nothing after the first.
+void keep_pool_memory() {
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64 || ((done.load() >> dev) & 1ull)) {
+    cudaGetLastError();
+    return;
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done |= 1ull << dev;
+}
+
+// A zeroed node-interleaved accumulator for one deposit on stream s, from the
+// device's stream-ordered pool.
+int acc_alloc(const GeomDev &g, cudaStream_t s, float **acc, long *nodes) {
+  keep_pool_memory();
+  *nodes = (long)g.nxn * g.nyn * g.nzn;
+  const size_t bytes = (size_t)*nodes * ACC_STRIDE * sizeof(float);
+  if (cudaMallocAsync(reinterpret_cast<void **>(acc), bytes, s) != cudaSuccess) {
+    cudaGetLastError();
+    *acc = nullptr;
+    return fail(SPB_ERR_ALLOC, "deposit accumulator allocation failed");
+  }
+  if (reinterpret_cast<uintptr_t>(*acc) & 15u) {   // the 16-byte adds need it
+    cudaFreeAsync(*acc, s);
+    *acc = nullptr;
+    return fail(SPB_ERR_ALLOC, "deposit accumulator not 16-byte aligned");
+  }
+  const cudaError_t e = cudaMemsetAsync(*acc, 0, bytes, s);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(*acc, s);
+    *acc = nullptr;
+    return fail_cuda(e, "cudaMemsetAsync(deposit accumulator)");
+  }
+  return SPB_OK;
+}
+
+// Adds the accumulator into the ten moment arrays and returns it to the pool.
+int acc_fold(float *acc, long nodes, float *const mom[10], cudaStream_t s) {
+  Moments10 M;
+  for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
+  k_fold_acc<<<(unsigned)std::min<long>(ceil_div(nodes, TPB), 4096), TPB, 0, s>>>(
+      reinterpret_cast<const float4 *>(acc), nodes, M);
+  const cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(acc, s);
+  if (e != cudaSuccess) return fail_cuda(e, "k_fold_acc");
+  g_launches++;
+  return SPB_OK;
+}
+}  // namespace
+
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
                      const float *u, const float *v, const float *w, const float *q, long n,
                      float *const mom[10], int *err, cudaStream_t s) {
   if (n <= 0) return SPB_OK;
-  MomStrided M;
-  if (!as_strided(mom, M))
-    return fail(SPB_ERR_UNSUPPORTED, "the ten moment arrays must be equally spaced");
-  k_plain_p2g<<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, M, err);
-  SPB_CUDA(cudaGetLastError());
+  float *acc;
+  long nodes;
+  if (int rc = acc_alloc(g, s, &acc, &nodes)) return rc;
+  k_plain_p2g<<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, acc, err);
+  if (const cudaError_t e = cudaGetLastError()) {
+    cudaFreeAsync(acc, s);
+    return fail_cuda(e, "k_plain_p2g");
+  }
   g_launches++;
-  return SPB_OK;
+  return acc_fold(acc, nodes, mom, s);
 }
 
 int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFields &F,
@@ -540,13 +585,16 @@ int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFi
                               const float *q, long n, float *const mom[10], int *err,
                               cudaStream_t s) {
   if (n <= 0) return SPB_OK;
-  MomStrided M;
-  if (!as_strided(mom, M))
-    return fail(SPB_ERR_UNSUPPORTED, "the ten moment arrays must be equally spaced");
-  k_plain_mover_interp<<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n, M, err);
-  SPB_CUDA(cudaGetLastError());
+  float *acc;
+  long nodes;
+  if (int rc = acc_alloc(g, s, &acc, &nodes)) return rc;
+  k_plain_mover_interp<<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n, acc, err);
+  if (const cudaError_t e = cudaGetLastError()) {
+    cudaFreeAsync(acc, s);
+    return fail_cuda(e, "k_plain_mover_interp");
+  }
   g_launches++;
-  return SPB_OK;
+  return acc_fold(acc, nodes, mom, s);
 }
 
 int launch_apply_bc_ids(int nxn, int nyn, int nzn, const int periodic[3],

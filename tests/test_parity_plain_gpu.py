@@ -327,10 +327,10 @@ def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64):
 
 
 def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64):
-    """spb_grid_p2g into ten separately allocated moment arrays (not equally
-    spaced: the deposit goes through a contiguous scratch and is added into
-    them) that already hold values: the result is those values plus the
-    deposit, within the reordering bound."""
+    """spb_grid_p2g into ten moment arrays at irregular offsets (the deposit's
+    node-interleaved accumulator is added into them) that already hold
+    values: the result is those values plus the deposit, within the
+    reordering bound."""
     torch = cuda
     from sputnipic_b200.device import GridContext
     wl = W.small_gem()
@@ -340,7 +340,7 @@ def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64):
     ctx.set_fields([torch.from_numpy(f).cuda() for f in fields])
     host = W.gem_particles(wl, 1)
     dev = {k: torch.from_numpy(host[k]).cuda() for k in "xyzuvwq"}
-    # slices of one buffer at irregular offsets: not equally spaced
+    # slices of one buffer at irregular offsets
     offs = [m * wl.nodes + 4 * m * m for m in range(10)]
     buf = torch.full((offs[-1] + wl.nodes,), 0.25, device="cuda")
     mom = [buf[o:o + wl.nodes] for o in offs]
