@@ -164,43 +164,44 @@ __device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
   }
 }
 
-// The 80 summands of one particle (src/Mover.cpp:399-570), each computed as
-// the reference does (weight = q * xi * eta * zeta * invVOL, then e.g.
-// (u * weight) * invVOL, no FMA), stored in the packed, lane-permuted layout of
-// warp_sum80: t[node * 5 + k] = (moment k, moment k + 5), node = a*4 + b*2 + c
-// with physical node (a ^ bit4(lane), b ^ bit3(lane), c ^ bit2(lane)); the
-// physical node (a, b, c) is (ix - a, iy - b, iz - c). Returns the linear index
-// of node (ix, iy, iz).
-__device__ __forceinline__ long deposit_terms(const GeomDev &g, float x, float y, float z,
-                                              float u, float v, float w, float q,
-                                              float2 (&t)[40], int lane, int &bad) {
-  const int ix = clamp_cell(cell_floor(x, g.xStart, g.invdx, g.nxn), g.nxn, bad);
-  const int iy = clamp_cell(cell_floor(y, g.yStart, g.invdy, g.nyn), g.nyn, bad);
-  const int iz = clamp_cell(cell_floor(z, g.zStart, g.invdz, g.nzn), g.nzn, bad);
+// The 40 summands of one x half of a particle (src/Mover.cpp:399-570), each
+// computed as the reference does (weight = q * xi * eta * zeta * invVOL,
+// then e.g. (u * weight) * invVOL, no FMA), in the packed, lane-permuted
+// layout of warp_sum80: t[(b * 2 + c) * 5 + k] = (moment k, moment k + 5) of
+// node slot (a, b, c), slot a = `a` given, with physical node (a ^ bit4(lane),
+// b ^ bit3(lane), c ^ bit2(lane)); the physical node (a, b, c) is (ix - a,
+// iy - b, iz - c). ADD: added to t (else stored).
+template <bool ADD>
+__device__ __forceinline__ void half_terms(const GeomDev &g, float x, float y, float z, float u,
+                                           float v, float w, float q, float2 (&t)[20], int lane,
+                                           int a) {
+  int ignored = 0;   // the range flag was raised when the cell key was formed
+  const int ix = clamp_cell(cell_floor(x, g.xStart, g.invdx, g.nxn), g.nxn, ignored);
+  const int iy = clamp_cell(cell_floor(y, g.yStart, g.invdy, g.nyn), g.nyn, ignored);
+  const int iz = clamp_cell(cell_floor(z, g.zStart, g.invdz, g.nzn), g.nzn, ignored);
   const float xi0 = x - __ldg(g.xn + ix - 1), xi1 = __ldg(g.xn + ix) - x;
   const float eta0 = y - __ldg(g.yn + iy - 1), eta1 = __ldg(g.yn + iy) - y;
   const float zeta0 = z - __ldg(g.zn + iz - 1), zeta1 = __ldg(g.zn + iz) - z;
-  const bool pa = lane & 16, pb = lane & 8, pc = lane & 4;
-  const float xi[2] = {pa ? xi1 : xi0, pa ? xi0 : xi1};
+  const bool pb = lane & 8, pc = lane & 4;
+  const float xia = (a ^ ((lane >> 4) & 1)) ? xi1 : xi0;
   const float eta[2] = {pb ? eta1 : eta0, pb ? eta0 : eta1};
   const float zeta[2] = {pc ? zeta1 : zeta0, pc ? zeta0 : zeta1};
   const float uu = u * u, uv = u * v, uw = u * w, vv = v * v, vw = v * w, ww = w * w;
   const float inv = g.invVOL;
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int b = 0; b < 2; ++b)
 #pragma unroll
-    for (int b = 0; b < 2; ++b)
+    for (int c = 0; c < 2; ++c) {
+      const float wgt = q * xia * eta[b] * zeta[c] * inv;
+      float2 *o = t + (b * 2 + c) * 5;
+      const float2 n[5] = {make_float2(wgt * inv, (uv * wgt) * inv),
+                           make_float2((u * wgt) * inv, (uw * wgt) * inv),
+                           make_float2((v * wgt) * inv, (vv * wgt) * inv),
+                           make_float2((w * wgt) * inv, (vw * wgt) * inv),
+                           make_float2((uu * wgt) * inv, (ww * wgt) * inv)};
 #pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const float wgt = q * xi[a] * eta[b] * zeta[c] * inv;
-        float2 *o = t + (a * 4 + b * 2 + c) * 5;
-        o[0] = make_float2(wgt * inv, (uv * wgt) * inv);
-        o[1] = make_float2((u * wgt) * inv, (uw * wgt) * inv);
-        o[2] = make_float2((v * wgt) * inv, (vv * wgt) * inv);
-        o[3] = make_float2((w * wgt) * inv, (vw * wgt) * inv);
-        o[4] = make_float2((uu * wgt) * inv, (ww * wgt) * inv);
-      }
-  return ((long)ix * g.nyn + iy) * g.nzn + iz;
+      for (int k = 0; k < 5; ++k) o[k] = ADD ? __fadd2_rn(o[k], n[k]) : n[k];
+    }
 }
 
 struct Particle {
@@ -223,13 +224,14 @@ __device__ __forceinline__ void red_v4(float *p, float a, float b, float c, floa
 // arrays afterwards.
 constexpr int ACC_STRIDE = 12;
 
-// Adds one warp's deposits to the moments. For each of up to four distinct
-// cells among the warp's particles (cell-ordered particles give one or two),
-// the members compute their terms and the warp sums them (warp_sum80) and
-// adds the 40 z-node pairs of totals (add_pair); the 40 pairs of each lone
-// particle of a further cell (a particle that moved, unordered input) are
-// spread over the warp, one pair per lane. Terms are recomputed per round
-// rather than kept, which halves the registers. All 32 lanes call.
+// Adds one warp's deposits to the accumulator. For each of up to four
+// distinct cells among the warp's particles (cell-ordered particles give one
+// or two), the members compute their terms and the warp sums them (the steps
+// of warp_sum80, one x half of the terms at a time) and adds the 80 totals;
+// each lone particle of a further cell (a particle that moved, unordered
+// input) is spread over 24 lanes, four moments of one node each, added with
+// one 16-byte add per lane. Terms are recomputed per round rather than kept,
+// which keeps the registers down. All 32 lanes call.
 __device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict__ acc,
                                              bool valid, const Particle &p, int &bad) {
   const int lane = threadIdx.x & 31;
@@ -246,7 +248,6 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict
   const int na = (lane >> 4) & 1, nb = (lane >> 3) & 1, nc = (lane >> 2) & 1;
   const int mbase = 5 * ((lane >> 1) & 1);
   const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
-  int ignored = 0;
   unsigned remaining = __ballot_sync(FULL, valid);
 #pragma unroll 1
   for (int round = 0; round < 4 && remaining; ++round) {
@@ -256,15 +257,21 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict
     const unsigned members = __ballot_sync(FULL, member);
     remaining &= ~members;
     if (__popc(members) < 2 && round > 0) continue;   // lone particle: direct atomics below
-    float2 t[40];
+    // warp_sum80 in halves: the slot a = 1 terms go to lane ^ 16, whose slot
+    // a = 0 holds the same physical x node, and each lane adds its own slot
+    // a = 0 terms to what it received (40 live values instead of 80)
+    float2 t[20];
     if (member) {
-      deposit_terms(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, ignored);
+      half_terms<false>(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, 1);
     } else {
 #pragma unroll
-      for (int j = 0; j < 40; ++j) t[j] = make_float2(0.0f, 0.0f);
+      for (int j = 0; j < 20; ++j) t[j] = make_float2(0.0f, 0.0f);
     }
+#pragma unroll
+    for (int j = 0; j < 20; ++j) t[j] = shfl_xor2(t[j], 16);
+    if (member) half_terms<true>(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, 0);
     float r[5];
-    warp_sum80(t, r, lane);
+    warp_sum80_tail(t, r, lane);
     float *const dst = acc + (k - na * sx - nb * sy - nc) * ACC_STRIDE + mbase;
 #pragma unroll
     for (int i = 0; i < 5; ++i)
@@ -273,7 +280,7 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict
   }
   // lone particles of further cells, one at a time: lane j < 24 takes node
   // j / 3 and moments 4 (j % 3) .. 4 (j % 3) + 3 of the particle, each term
-  // computed as deposit_terms does, and adds them with one 16-byte add
+  // computed as half_terms does, and adds them with one 16-byte add
   unsigned lone = __ballot_sync(FULL, valid);
   if (lone) {
     const int ix = (int)(key / sx), iy = (int)((key / sy) % g.nyn), iz = (int)(key % sy);

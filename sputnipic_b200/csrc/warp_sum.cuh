@@ -19,9 +19,10 @@ __device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
 // half and receives its partner's upper half. Afterwards lane l holds in
 // r[0..4] the totals of physical node (a, b, c) = (bit4, bit3, bit2) of l,
 // moments 5*bit1(l) .. 5*bit1(l)+4; both lanes of a pair (l, l^1) hold them.
-__device__ __forceinline__ void warp_sum80(float2 (&acc)[40], float (&r)[5], int lane) {
-#pragma unroll
-  for (int i = 0; i < 20; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 20], 16));
+//
+// warp_sum80_tail runs the steps after the first (x) halving on the 20 pairs
+// of the lane's x half (its slot a = 0 after that step).
+__device__ __forceinline__ void warp_sum80_tail(float2 (&acc)[20], float (&r)[5], int lane) {
 #pragma unroll
   for (int i = 0; i < 10; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 10], 8));
 #pragma unroll
@@ -35,6 +36,12 @@ __device__ __forceinline__ void warp_sum80(float2 (&acc)[40], float (&r)[5], int
   }
 #pragma unroll
   for (int k = 0; k < 5; ++k) r[k] += __shfl_xor_sync(0xffffffffu, r[k], 1);
+}
+
+__device__ __forceinline__ void warp_sum80(float2 (&acc)[40], float (&r)[5], int lane) {
+#pragma unroll
+  for (int i = 0; i < 20; ++i) acc[i] = __fadd2_rn(acc[i], shfl_xor2(acc[i + 20], 16));
+  warp_sum80_tail(*reinterpret_cast<float2(*)[20]>(&acc[0]), r, lane);
 }
 
 }  // namespace spb
