@@ -71,6 +71,16 @@ const char *spb_version(void);
 /* Number of kernels this library has launched in this process. */
 long spb_launch_count(void);
 
+/* How the plain interpP2G / mover_interp deposits (process-wide):
+ * SPB_DEPOSIT_ACCUMULATOR (default) adds into a node-interleaved buffer of
+ * 48 bytes per node from the device's stream-ordered pool, then into the
+ * ten moment arrays (fewer L2 transactions); SPB_DEPOSIT_DIRECT adds straight
+ * into the ten arrays and needs no memory. The accumulator form falls back to
+ * the direct one when its buffer cannot be allocated. Returns the previous
+ * mode, or SPB_ERR_INVALID for an unknown mode. */
+enum { SPB_DEPOSIT_ACCUMULATOR = 0, SPB_DEPOSIT_DIRECT = 1 };
+int spb_set_plain_deposit_mode(int mode);
+
 /* JSON object: "struct.member": offset for every member of the boundary
  * structs as this library lays them out (see sputnipic_ref_layout.h). */
 const char *spb_abi_layout_json(void);

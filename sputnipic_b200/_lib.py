@@ -211,6 +211,7 @@ def load():
     _proto(lib, "spb_error_string", ctypes.c_char_p, [c_int])
     _proto(lib, "spb_version", ctypes.c_char_p, [])
     _proto(lib, "spb_launch_count", c_long, [])
+    _proto(lib, "spb_set_plain_deposit_mode", c_int, [c_int])
     _proto(lib, "spb_abi_layout_json", ctypes.c_char_p, [])
     _proto(lib, "spb_set_device", c_int, [c_int])
     _proto(lib, "spb_mover_PC", c_int, [R(Particles), R(EMfield), R(Grid), R(Parameters)])

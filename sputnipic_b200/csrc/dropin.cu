@@ -324,8 +324,11 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
       if (!f[a]) return fail(SPB_ERR_INVALID, "field array is null");
     if (int rc = spb_grid_set_fields(ctx, f, 0, sp->stream)) return rc;
   }
-  if (deposits)
+  float *acc = nullptr;   // one accumulator for all chunks, folded once
+  if (deposits) {
     if (int rc = upload_moments(sp, ids, nodes, dev_mom, hm, dm)) return rc;
+    acc = plain_acc_alloc(ctx->geom, sp->stream);
+  }
   SPB_CUDA(cudaEventRecord(sp->ev_in, sp->stream));
   for (int j = 0; j < 2; ++j) SPB_CUDA(cudaStreamWaitEvent(sp->pipe[j], sp->ev_in, 0));
   const PushDev p = moves ? make_push(push_of(part, param)) : PushDev{};
@@ -341,16 +344,22 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
       SPB_CUDA(cudaMemcpyAsync(d[a], h[a] + off, bytes, cudaMemcpyHostToDevice, s));
     int rc;
     if (op == Op::Fused)
-      rc = launch_plain_mover_interp(ctx->geom, p, F, d[0], d[1], d[2], d[3], d[4], d[5], d[6],
-                                     cnt, dm, sp->d_err, s);
+      rc = launch_plain_mover_interp_into(ctx->geom, p, F, d[0], d[1], d[2], d[3], d[4], d[5],
+                                          d[6], cnt, acc, dm, sp->d_err, s);
     else if (moves)
       rc = launch_plain_mover(ctx->geom, p, F, d[0], d[1], d[2], d[3], d[4], d[5], cnt,
                               sp->d_err, s, op == Op::MoverV ? 1 : 0);
     else
-      rc = launch_plain_p2g(ctx->geom, d[0], d[1], d[2], d[3], d[4], d[5], d[6], cnt, dm,
-                            sp->d_err, s);
-    if (rc) return rc;
-    ctx->launches += deposits ? 2 : 1;   // a deposit folds its accumulator
+      rc = launch_plain_p2g_into(ctx->geom, d[0], d[1], d[2], d[3], d[4], d[5], d[6], cnt, acc,
+                                 dm, sp->d_err, s);
+    if (rc) {
+      if (acc) {   // after the chunks already queued on both streams
+        for (int j = 0; j < 2; ++j) cudaStreamSynchronize(sp->pipe[j]);
+        cudaFreeAsync(acc, sp->stream);
+      }
+      return rc;
+    }
+    ctx->launches++;
     if (moves)
       for (int a = 0; a < 6; ++a)
         SPB_CUDA(cudaMemcpyAsync(h[a] + off, d[a], bytes, cudaMemcpyDeviceToHost, s));
@@ -358,6 +367,10 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
   for (int j = 0; j < 2; ++j) {
     SPB_CUDA(cudaEventRecord(sp->ev_done[j], sp->pipe[j]));
     SPB_CUDA(cudaStreamWaitEvent(sp->stream, sp->ev_done[j], 0));
+  }
+  if (acc) {
+    if (int rc = plain_acc_fold(acc, ctx->geom, dm, sp->stream)) return rc;
+    ctx->launches++;
   }
   if (deposits && !dev_mom)
     for (int m = 0; m < 10; ++m)

@@ -25,6 +25,23 @@ int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const
 // net[m*nodes + i] = sum over species s (in order) of bases[s][m*nodes + i].
 int launch_sum_species(const float *const *bases, int ns, long nodes, float *net,
                        cudaStream_t s);
+// The plain deposit's accumulator: a zeroed node-interleaved buffer (the ten
+// moments of a node side by side, 48 bytes per node) from the device's
+// stream-ordered pool on stream s, or nullptr when it cannot be had (the
+// deposits then add straight into the moment arrays).
+float *plain_acc_alloc(const GeomDev &g, cudaStream_t s);
+// Adds the accumulator into mom[0..9] and returns it to the pool (nothing
+// for nullptr).
+int plain_acc_fold(float *acc, const GeomDev &g, float *const mom[10], cudaStream_t s);
+// interpP2G / mover_interp deposits into acc (mom when acc is nullptr).
+int launch_plain_p2g_into(const GeomDev &g, const float *x, const float *y, const float *z,
+                          const float *u, const float *v, const float *w, const float *q, long n,
+                          float *acc, float *const mom[10], int *err, cudaStream_t s);
+int launch_plain_mover_interp_into(const GeomDev &g, const PushDev &p, const PackedFields &F,
+                                   float *x, float *y, float *z, float *u, float *v, float *w,
+                                   const float *q, long n, float *acc, float *const mom[10],
+                                   int *err, cudaStream_t s);
+// The same with their own accumulator: allocate, deposit, fold.
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
                      const float *u, const float *v, const float *w, const float *q, long n,
                      float *const mom[10], int *err, cudaStream_t s);

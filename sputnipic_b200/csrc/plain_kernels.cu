@@ -224,6 +224,36 @@ __device__ __forceinline__ void red_v4(float *p, float a, float b, float c, floa
 // arrays afterwards.
 constexpr int ACC_STRIDE = 12;
 
+// Where a plain deposit adds: the accumulator (ACC) or, when none could be
+// allocated, the ten moment arrays themselves.
+struct DepTarget {
+  float *acc;
+  Moments10 mom;
+};
+
+// Adds v to moment m of node n.
+template <bool ACC>
+__device__ __forceinline__ void dep_add(const DepTarget &T, long n, int m, float v) {
+  if (ACC)
+    atomicAdd(T.acc + n * ACC_STRIDE + m, v);
+  else
+    atomicAdd(T.mom.m[m] + n, v);
+}
+
+// Adds v0..v3 to moments 4 grp .. 4 grp + 3 of node n (moments below 10).
+template <bool ACC>
+__device__ __forceinline__ void dep_add4(const DepTarget &T, long n, int grp, float v0, float v1,
+                                         float v2, float v3) {
+  if (ACC) {
+    red_v4(T.acc + n * ACC_STRIDE + 4 * grp, v0, v1, v2, v3);
+  } else {
+    const float v[4] = {v0, v1, v2, v3};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (4 * grp + i < 10) atomicAdd(T.mom.m[4 * grp + i] + n, v[i]);
+  }
+}
+
 // Adds one warp's deposits to the accumulator. For each of up to four
 // distinct cells among the warp's particles (cell-ordered particles give one
 // or two), the members compute their terms and the warp sums them (the steps
@@ -232,8 +262,9 @@ constexpr int ACC_STRIDE = 12;
 // input) is spread over 24 lanes, four moments of one node each, added with
 // one 16-byte add per lane. Terms are recomputed per round rather than kept,
 // which keeps the registers down. All 32 lanes call.
-__device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict__ acc,
-                                             bool valid, const Particle &p, int &bad) {
+template <bool ACC>
+__device__ __forceinline__ void deposit_warp(const GeomDev &g, const DepTarget &T, bool valid,
+                                             const Particle &p, int &bad) {
   const int lane = threadIdx.x & 31;
   const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
   long key = 0;
@@ -272,10 +303,10 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict
     if (member) half_terms<true>(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, 0);
     float r[5];
     warp_sum80_tail(t, r, lane);
-    float *const dst = acc + (k - na * sx - nb * sy - nc) * ACC_STRIDE + mbase;
+    const long node = k - na * sx - nb * sy - nc;
 #pragma unroll
     for (int i = 0; i < 5; ++i)
-      if (i >= lo && i < hi) atomicAdd(dst + i, r[i]);
+      if (i >= lo && i < hi) dep_add<ACC>(T, node, mbase + i, r[i]);
     if (member) valid = false;   // done
   }
   // lone particles of further cells, one at a time: lane j < 24 takes node
@@ -314,8 +345,8 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, float *__restrict
         const float f1 = grp == 0 ? u : (grp == 1 ? u * v : w * w);
         const float f2 = grp == 0 ? v : (grp == 1 ? u * w : 0.0f);
         const float f3 = grp == 0 ? w : (grp == 1 ? v * v : 0.0f);
-        red_v4(acc + (k - a * sx - b * sy - c) * ACC_STRIDE + 4 * grp, (f0 * wgt) * inv,
-               (f1 * wgt) * inv, (f2 * wgt) * inv, (f3 * wgt) * inv);
+        dep_add4<ACC>(T, k - a * sx - b * sy - c, grp, (f0 * wgt) * inv, (f1 * wgt) * inv,
+                      (f2 * wgt) * inv, (f3 * wgt) * inv);
       }
     }
   }
@@ -356,6 +387,7 @@ __global__ void __launch_bounds__(TPB) k_plain_mover(GeomDev g, PushDev p, Packe
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
+template <bool ACC>
 __global__ void __launch_bounds__(TPB) k_plain_p2g(GeomDev g, const float *__restrict__ x,
                                                    const float *__restrict__ y,
                                                    const float *__restrict__ z,
@@ -363,21 +395,23 @@ __global__ void __launch_bounds__(TPB) k_plain_p2g(GeomDev g, const float *__res
                                                    const float *__restrict__ v,
                                                    const float *__restrict__ w,
                                                    const float *__restrict__ q, long n,
-                                                   float *__restrict__ acc, int *__restrict__ err) {
+                                                   const __grid_constant__ DepTarget T,
+                                                   int *__restrict__ err) {
   const long i = blockIdx.x * (long)TPB + threadIdx.x;
   const bool valid = i < n;
   Particle p{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (valid) p = Particle{x[i], y[i], z[i], u[i], v[i], w[i], q[i]};
   int bad = 0;
-  deposit_warp(g, acc, valid, p, bad);
+  deposit_warp<ACC>(g, T, valid, p, bad);
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
+template <bool ACC>
 __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
     GeomDev g, PushDev p, PackedFields F, float *__restrict__ x, float *__restrict__ y,
     float *__restrict__ z, float *__restrict__ u, float *__restrict__ v,
-    float *__restrict__ w, const float *__restrict__ q, long n, float *__restrict__ acc,
-    int *__restrict__ err) {
+    float *__restrict__ w, const float *__restrict__ q, long n,
+    const __grid_constant__ DepTarget T, int *__restrict__ err) {
   const long i = blockIdx.x * (long)TPB + threadIdx.x;
   const bool valid = i < n;
   Particle pt{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -393,7 +427,7 @@ __global__ void __launch_bounds__(TPB) k_plain_mover_interp(
     w[i] = pw;
     pt = Particle{px, py, pz, pu, pv, pw, q[i]};
   }
-  deposit_warp(g, acc, valid, pt, bad);
+  deposit_warp<ACC>(g, T, valid, pt, bad);
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
 
@@ -532,33 +566,34 @@ void keep_pool_memory() {
   done |= 1ull << dev;
 }
 
-// A zeroed node-interleaved accumulator for one deposit on stream s, from the
-// device's stream-ordered pool.
-int acc_alloc(const GeomDev &g, cudaStream_t s, float **acc, long *nodes) {
+}  // namespace
+
+namespace {
+std::atomic<int> g_deposit_mode{SPB_DEPOSIT_ACCUMULATOR};
+}  // namespace
+
+float *plain_acc_alloc(const GeomDev &g, cudaStream_t s) {
+  if (g_deposit_mode.load() == SPB_DEPOSIT_DIRECT) return nullptr;
   keep_pool_memory();
-  *nodes = (long)g.nxn * g.nyn * g.nzn;
-  const size_t bytes = (size_t)*nodes * ACC_STRIDE * sizeof(float);
-  if (cudaMallocAsync(reinterpret_cast<void **>(acc), bytes, s) != cudaSuccess) {
+  const size_t bytes = (size_t)g.nxn * g.nyn * g.nzn * ACC_STRIDE * sizeof(float);
+  float *acc = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void **>(&acc), bytes, s) != cudaSuccess) {
     cudaGetLastError();
-    *acc = nullptr;
-    return fail(SPB_ERR_ALLOC, "deposit accumulator allocation failed");
+    return nullptr;
   }
-  if (reinterpret_cast<uintptr_t>(*acc) & 15u) {   // the 16-byte adds need it
-    cudaFreeAsync(*acc, s);
-    *acc = nullptr;
-    return fail(SPB_ERR_ALLOC, "deposit accumulator not 16-byte aligned");
+  // the 16-byte adds need the alignment (pool allocations have it)
+  if ((reinterpret_cast<uintptr_t>(acc) & 15u) || cudaMemsetAsync(acc, 0, bytes, s) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeAsync(acc, s);
+    cudaGetLastError();
+    return nullptr;
   }
-  const cudaError_t e = cudaMemsetAsync(*acc, 0, bytes, s);
-  if (e != cudaSuccess) {
-    cudaFreeAsync(*acc, s);
-    *acc = nullptr;
-    return fail_cuda(e, "cudaMemsetAsync(deposit accumulator)");
-  }
-  return SPB_OK;
+  return acc;
 }
 
-// Adds the accumulator into the ten moment arrays and returns it to the pool.
-int acc_fold(float *acc, long nodes, float *const mom[10], cudaStream_t s) {
+int plain_acc_fold(float *acc, const GeomDev &g, float *const mom[10], cudaStream_t s) {
+  if (!acc) return SPB_OK;
+  const long nodes = (long)g.nxn * g.nyn * g.nzn;
   Moments10 M;
   for (int m = 0; m < 10; ++m) M.m[m] = mom[m];
   k_fold_acc<<<(unsigned)std::min<long>(ceil_div(nodes, TPB), 4096), TPB, 0, s>>>(
@@ -569,22 +604,58 @@ int acc_fold(float *acc, long nodes, float *const mom[10], cudaStream_t s) {
   g_launches++;
   return SPB_OK;
 }
+
+namespace {
+DepTarget target(float *acc, float *const mom[10]) {
+  DepTarget T;
+  T.acc = acc;
+  for (int m = 0; m < 10; ++m) T.mom.m[m] = mom[m];
+  return T;
+}
 }  // namespace
+
+int launch_plain_p2g_into(const GeomDev &g, const float *x, const float *y, const float *z,
+                          const float *u, const float *v, const float *w, const float *q, long n,
+                          float *acc, float *const mom[10], int *err, cudaStream_t s) {
+  if (n <= 0) return SPB_OK;
+  const DepTarget T = target(acc, mom);
+  if (acc)
+    k_plain_p2g<true><<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
+  else
+    k_plain_p2g<false><<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
+
+int launch_plain_mover_interp_into(const GeomDev &g, const PushDev &p, const PackedFields &F,
+                                   float *x, float *y, float *z, float *u, float *v, float *w,
+                                   const float *q, long n, float *acc, float *const mom[10],
+                                   int *err, cudaStream_t s) {
+  if (n <= 0) return SPB_OK;
+  const DepTarget T = target(acc, mom);
+  if (acc)
+    k_plain_mover_interp<true><<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n, T,
+                                                             err);
+  else
+    k_plain_mover_interp<false><<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n,
+                                                              T, err);
+  SPB_CUDA(cudaGetLastError());
+  g_launches++;
+  return SPB_OK;
+}
 
 int launch_plain_p2g(const GeomDev &g, const float *x, const float *y, const float *z,
                      const float *u, const float *v, const float *w, const float *q, long n,
                      float *const mom[10], int *err, cudaStream_t s) {
   if (n <= 0) return SPB_OK;
-  float *acc;
-  long nodes;
-  if (int rc = acc_alloc(g, s, &acc, &nodes)) return rc;
-  k_plain_p2g<<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, acc, err);
-  if (const cudaError_t e = cudaGetLastError()) {
-    cudaFreeAsync(acc, s);
-    return fail_cuda(e, "k_plain_p2g");
+  float *acc = plain_acc_alloc(g, s);
+  const int rc = launch_plain_p2g_into(g, x, y, z, u, v, w, q, n, acc, mom, err, s);
+  if (rc) {
+    if (acc) cudaFreeAsync(acc, s);
+    return rc;
   }
-  g_launches++;
-  return acc_fold(acc, nodes, mom, s);
+  return plain_acc_fold(acc, g, mom, s);
 }
 
 int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFields &F,
@@ -592,16 +663,13 @@ int launch_plain_mover_interp(const GeomDev &g, const PushDev &p, const PackedFi
                               const float *q, long n, float *const mom[10], int *err,
                               cudaStream_t s) {
   if (n <= 0) return SPB_OK;
-  float *acc;
-  long nodes;
-  if (int rc = acc_alloc(g, s, &acc, &nodes)) return rc;
-  k_plain_mover_interp<<<blocks_for(n), TPB, 0, s>>>(g, p, F, x, y, z, u, v, w, q, n, acc, err);
-  if (const cudaError_t e = cudaGetLastError()) {
-    cudaFreeAsync(acc, s);
-    return fail_cuda(e, "k_plain_mover_interp");
+  float *acc = plain_acc_alloc(g, s);
+  const int rc = launch_plain_mover_interp_into(g, p, F, x, y, z, u, v, w, q, n, acc, mom, err, s);
+  if (rc) {
+    if (acc) cudaFreeAsync(acc, s);
+    return rc;
   }
-  g_launches++;
-  return acc_fold(acc, nodes, mom, s);
+  return plain_acc_fold(acc, g, mom, s);
 }
 
 int launch_apply_bc_ids(int nxn, int nyn, int nzn, const int periodic[3],
@@ -624,3 +692,9 @@ int launch_apply_bc_ids(int nxn, int nyn, int nzn, const int periodic[3],
 }
 
 }  // namespace spb
+
+extern "C" int spb_set_plain_deposit_mode(int mode) {
+  if (mode != SPB_DEPOSIT_ACCUMULATOR && mode != SPB_DEPOSIT_DIRECT)
+    return spb::fail(SPB_ERR_INVALID, "spb_set_plain_deposit_mode: unknown mode");
+  return spb::g_deposit_mode.exchange(mode);
+}

@@ -26,6 +26,22 @@ def _ptr(t) -> int:
     return t.data_ptr()
 
 
+DEPOSIT_MODES = {"accumulator": 0, "direct": 1}
+
+
+def set_plain_deposit_mode(mode: str) -> str:
+    """How the plain interpP2G / mover_interp deposits, process-wide
+    (spb_set_plain_deposit_mode): "accumulator" (a node-interleaved buffer
+    from the device pool, then added into the ten moment arrays; the default)
+    or "direct" (straight into the ten arrays, no extra memory). Returns the
+    previous mode."""
+    if mode not in DEPOSIT_MODES:
+        raise ValueError(f"unknown deposit mode {mode!r}")
+    prev = _lib.load().spb_set_plain_deposit_mode(DEPOSIT_MODES[mode])
+    _lib.check(min(prev, 0))
+    return {v: k for k, v in DEPOSIT_MODES.items()}[prev]
+
+
 def push_params(wl, s: int) -> _lib.SpbPush:
     """spb_push of species ``s`` of a workload."""
     p = _lib.SpbPush()

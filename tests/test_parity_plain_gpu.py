@@ -116,8 +116,19 @@ def test_edge_interp_p2g(golden_edge, orc64, qi):
     check_moments(np.stack(dropin.moments(ids)), 2.0 * d[f"fp32_q{qi}_p2g"], 2.0 * absm)
 
 
+@pytest.fixture(params=["accumulator", "direct"])
+def deposit_mode(request):
+    """Both plain deposit forms: through the node-interleaved accumulator and
+    straight into the ten moment arrays (the fallback when the accumulator
+    cannot be allocated)."""
+    from sputnipic_b200.device import set_plain_deposit_mode
+    prev = set_plain_deposit_mode(request.param)
+    yield request.param
+    set_plain_deposit_mode(prev)
+
+
 @pytest.mark.parametrize("qi", [0, 1])
-def test_edge_mover_interp(golden_edge, orc64, qi):
+def test_edge_mover_interp(golden_edge, orc64, qi, deposit_mode):
     d = golden_edge
     wl, param, grd, field, P = edge_inputs(d, qi)
     ids = dropin.interp_dens_species_allocate(grd, 0)
@@ -301,11 +312,12 @@ def test_out_of_grid_particle_is_flagged_not_faulting(orc32):
         assert np.array_equal(out[k][good], sel[k])
 
 
-def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64):
+def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64, deposit_mode):
     """COPY residency moves species above 4M particles through PCIe in chunks on
     alternating streams. 9.2M particles (two chunk boundaries and a ragged last
     chunk): mover_PC bit-identical to the reference code, interpP2G within the
-    reordering bound, as for one launch."""
+    reordering bound, as for one launch; both deposit forms (the chunks of
+    both streams add into one accumulator, folded once)."""
     wl = W.small_gem(nxc=64, nyc=32, nzc=32, E_amp=1e-3,
                      species=W.gem_species((140, 140, 140, 140)))
     fields = W.gem_fields(wl)
@@ -326,7 +338,7 @@ def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64):
     check_moments(np.stack(dropin.moments(ids)), np.stack(mom), abs_moments(orc64, setup, wl, ref))
 
 
-def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64):
+def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64, deposit_mode):
     """spb_grid_p2g into ten moment arrays at irregular offsets (the deposit's
     node-interleaved accumulator is added into them) that already hold
     values: the result is those values plus the deposit, within the
