@@ -88,6 +88,22 @@ def test_dropin_rejects_null_arguments_without_touching_the_gpu():
     assert lib.spb_mover_interp(None, None, None, None, None) == 2
 
 
+def test_plain_deposit_mode_switch():
+    """spb_set_plain_deposit_mode returns the previous mode and rejects
+    unknown ones (no device work)."""
+    from sputnipic_b200.device import set_plain_deposit_mode
+    lib = _lib.load()
+    assert lib.spb_set_plain_deposit_mode(7) == 2
+    assert lib.spb_last_error() == 2
+    lib.spb_clear_error()
+    prev = set_plain_deposit_mode("direct")
+    try:
+        assert set_plain_deposit_mode("accumulator") == "direct"
+        assert set_plain_deposit_mode("accumulator") == "accumulator"
+    finally:
+        set_plain_deposit_mode(prev)
+
+
 def test_dropin_rejects_bad_mover_parameters():
     wl = W.small_gem()
     param = dropin.make_parameters(wl)
