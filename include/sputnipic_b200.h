@@ -271,8 +271,11 @@ typedef struct spb_sim spb_sim;
 typedef struct spb_sim_desc {
   int nxc, nyc, nzc;        /* active cells; multiples of the tile shape */
   double Lx, Ly, Lz;
-  double dt, c;             /* param->dt, param->c */
-  int niter;                /* NiterMover */
+  double dt, c;             /* param->dt (divided by part->n_sub_cycles when
+                               the species sub-cycle: mover_PC's time step,
+                               src/Mover.cpp:11), param->c */
+  int niter;                /* NiterMover (param->NiterMover, which
+                               particle_allocate gives every species) */
   int periodic[3];          /* param->PERIODICX/Y/Z */
   int ns;                   /* species, 1..8 */
   double qom[SPB_SIM_MAX_SPECIES];
