@@ -37,11 +37,17 @@ using namespace spb;
 
 namespace {
 
+// Streams the chunks of a pipelined COPY call rotate over. A stream runs its
+// chunks in order, so with two streams the upload of chunk k + 2 would wait
+// for the download of chunk k (and that for chunk k's kernel): four keep the
+// upload engine busy while a chunk's kernel and download complete.
+constexpr int NPIPE = 4;
+
 struct Species {
   cudaStream_t stream = nullptr;
-  cudaStream_t pipe[2] = {};      // COPY residency: streams the particle chunks alternate on
+  cudaStream_t pipe[NPIPE] = {};  // COPY residency: streams the particle chunks rotate over
   cudaEvent_t ev_in = nullptr;    // fields / moments uploaded
-  cudaEvent_t ev_done[2] = {};    // a pipe stream's chunks finished
+  cudaEvent_t ev_done[NPIPE] = {};   // a pipe stream's chunks finished
   long cap = 0;
   float *d[7] = {};           // x y z u v w q
   float *d_mom = nullptr;     // 10 * mom_nodes
@@ -59,7 +65,7 @@ struct Species {
     cudaFree(d_mom);
     cudaFree(d_err);
     if (stream) cudaStreamDestroy(stream);
-    for (int j = 0; j < 2; ++j) {
+    for (int j = 0; j < NPIPE; ++j) {
       if (pipe[j]) cudaStreamDestroy(pipe[j]);
       if (ev_done[j]) cudaEventDestroy(ev_done[j]);
     }
@@ -265,7 +271,7 @@ spb_push push_of(const struct particles *part, const struct parameters *param) {
 enum class Op { Mover, MoverV, Interp, Fused };
 
 // COPY residency for large species: the particles go through PCIe in chunks
-// of PIPE_CHUNK, alternating between two streams, so one chunk's upload, its
+// of PIPE_CHUNK, rotating over NPIPE streams, so one chunk's upload, its
 // kernel and the previous chunk's download run at the same time (with pinned
 // host arrays; pageable arrays are copied synchronously by CUDA, which is
 // still correct). The results are those of one launch over all particles: the
@@ -290,7 +296,7 @@ int upload_moments(Species *sp, struct interpDensSpecies *ids, long nodes, bool 
 }
 
 int ensure_pipe(Species *sp) {
-  for (int j = 0; j < 2; ++j) {
+  for (int j = 0; j < NPIPE; ++j) {
     if (!sp->pipe[j]) SPB_CUDA(cudaStreamCreateWithFlags(&sp->pipe[j], cudaStreamNonBlocking));
     if (!sp->ev_done[j])
       SPB_CUDA(cudaEventCreateWithFlags(&sp->ev_done[j], cudaEventDisableTiming));
@@ -330,12 +336,12 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
     acc = plain_acc_alloc(ctx->geom, sp->stream);
   }
   SPB_CUDA(cudaEventRecord(sp->ev_in, sp->stream));
-  for (int j = 0; j < 2; ++j) SPB_CUDA(cudaStreamWaitEvent(sp->pipe[j], sp->ev_in, 0));
+  for (int j = 0; j < NPIPE; ++j) SPB_CUDA(cudaStreamWaitEvent(sp->pipe[j], sp->ev_in, 0));
   const PushDev p = moves ? make_push(push_of(part, param)) : PushDev{};
   const PackedFields F{ctx->d_eb4, ctx->d_eb2};
   long k = 0;
   for (long off = 0; off < n; off += PIPE_CHUNK, ++k) {
-    cudaStream_t s = sp->pipe[k & 1];
+    cudaStream_t s = sp->pipe[k % NPIPE];
     const long cnt = std::min(PIPE_CHUNK, n - off);
     const size_t bytes = (size_t)cnt * sizeof(float);
     float *d[7];
@@ -353,8 +359,8 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
       rc = launch_plain_p2g_into(ctx->geom, d[0], d[1], d[2], d[3], d[4], d[5], d[6], cnt, acc,
                                  dm, sp->d_err, s);
     if (rc) {
-      if (acc) {   // after the chunks already queued on both streams
-        for (int j = 0; j < 2; ++j) cudaStreamSynchronize(sp->pipe[j]);
+      if (acc) {   // after the chunks already queued on the pipe streams
+        for (int j = 0; j < NPIPE; ++j) cudaStreamSynchronize(sp->pipe[j]);
         cudaFreeAsync(acc, sp->stream);
       }
       return rc;
@@ -364,7 +370,7 @@ int run_copy_pipelined(Op op, Species *sp, struct particles *part, struct EMfiel
       for (int a = 0; a < 6; ++a)
         SPB_CUDA(cudaMemcpyAsync(h[a] + off, d[a], bytes, cudaMemcpyDeviceToHost, s));
   }
-  for (int j = 0; j < 2; ++j) {
+  for (int j = 0; j < NPIPE; ++j) {
     SPB_CUDA(cudaEventRecord(sp->ev_done[j], sp->pipe[j]));
     SPB_CUDA(cudaStreamWaitEvent(sp->stream, sp->ev_done[j], 0));
   }

@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(TPB) k_sum_species(SpeciesBases S, int ns, lon
 }
 
 // mom[m][n] += acc[n * ACC_STRIDE + m] for the non-zero entries (atomically:
-// the two pipeline streams of the drop-in fold into the same arrays).
+// the pipeline streams of the drop-in fold into the same arrays).
 __global__ void __launch_bounds__(TPB) k_fold_acc(const float4 *__restrict__ acc, long nodes,
                                                   Moments10 M) {
   for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < nodes;

@@ -314,8 +314,8 @@ def test_out_of_grid_particle_is_flagged_not_faulting(orc32):
 
 def test_copy_residency_pipeline_over_chunk_boundaries(orc32, orc64, deposit_mode):
     """COPY residency moves species above 4M particles through PCIe in chunks on
-    alternating streams. 9.2M particles (two chunk boundaries and a ragged last
-    chunk): mover_PC bit-identical to the reference code, interpP2G within the
+    rotating streams. 9.2M particles (several chunk boundaries, chunks of
+    unequal sizes): mover_PC bit-identical to the reference code, interpP2G within the
     reordering bound, as for one launch; both deposit forms (the chunks of
     both streams add into one accumulator, folded once)."""
     wl = W.small_gem(nxc=64, nyc=32, nzc=32, E_amp=1e-3,
