@@ -113,11 +113,13 @@ __global__ void k_hat_div_tensor(HatGeom g, const __grid_constant__ Species6<T> 
   }
 }
 
-// Guard-cell fill of n0 x n1 x n2 scalar arrays, one CTA per array (A.a[blockIdx.x])
-// (applyBCscalarDensC with s = 1, applyBCscalarDensN with s = 2). Phases in
-// the reference order: periodic faces X, Y, Z; edges along X, Y, Z; corners;
-// non-periodic faces X, Y, Z. A periodic face copies from n-1-s to 0 and from
-// s to n-1; yhi ends the Y-edge loop (nyn - 1 in both reference functions).
+// Guard-cell fill of n0 x n1 x n2 scalar arrays (applyBCscalarDensC with
+// s = 1, applyBCscalarDensN with s = 2). The reference's phases: periodic
+// faces X, Y, Z; edges along X, Y, Z; corners; non-periodic faces X, Y, Z. A
+// periodic face copies from n-1-s to 0 and from s to n-1; yhi ends the
+// Y-edge loop (nyn - 1 in both reference functions). Every guard cell gets
+// the value of one cell of the array before the fill (fill_source), so the
+// fill runs as one gather of all guard values and one scatter.
 struct Fill {
   int n0, n1, n2, s, yhi;
   int per[3];
@@ -128,113 +130,103 @@ struct Arrays {
   T *a[3 * HAT_MAXS];
 };
 
-// One fill phase over N elements of C copies each (dst <- src, as linear
-// indices from idx(t, c, dst, src)): every thread loads the sources of U
-// elements before storing them, which no phase makes unsafe (a phase never
-// writes what it reads).
-template <typename T, int C, int U, typename Idx>
-__device__ __forceinline__ void fill_phase(T *a, int N, Idx idx) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int t0 = tid; t0 < N; t0 += U * nt) {
-    T v[U][C];
-    long d[U][C];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int t = t0 + u * nt;
-      if (t < N) {
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-          long sidx;
-          idx(t, c, d[u][c], sidx);
-          v[u][c] = a[sidx];
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (t0 + u * nt < N) {
-#pragma unroll
-        for (int c = 0; c < C; ++c) a[d[u][c]] = v[u][c];
-      }
-  }
-  __syncthreads();
+// The guard cells of an n0 x n1 x n2 array, numbered face by face: the two x
+// faces (every j, k), the two y faces (inner i, every k), the two z faces
+// (inner i, j).
+__host__ __device__ __forceinline__ long guard_count(const Fill &f) {
+  return 2L * f.n1 * f.n2 + 2L * (f.n0 - 2) * f.n2 + 2L * (f.n0 - 2) * (f.n1 - 2);
 }
 
+__device__ __forceinline__ void guard_cell(const Fill &f, long g, int &i, int &j, int &k) {
+  const long fx = (long)f.n1 * f.n2, fy = (long)(f.n0 - 2) * f.n2;
+  if (g < 2 * fx) {
+    i = g < fx ? 0 : f.n0 - 1;
+    const long r = g % fx;
+    j = (int)(r / f.n2);
+    k = (int)(r % f.n2);
+  } else if ((g -= 2 * fx) < 2 * fy) {
+    j = g < fy ? 0 : f.n1 - 1;
+    const long r = g % fy;
+    i = 1 + (int)(r / f.n2);
+    k = (int)(r % f.n2);
+  } else {
+    g -= 2 * fy;
+    const long fz = (long)(f.n0 - 2) * (f.n1 - 2);
+    k = g < fz ? 0 : f.n2 - 1;
+    const long r = g % fz;
+    i = 1 + (int)(r / (f.n1 - 2));
+    j = 1 + (int)(r % (f.n1 - 2));
+  }
+}
+
+// Periodic source along one axis: the guard at e copies from s, the guard
+// at 0 from e - s.
+__device__ __forceinline__ int per_src(int x, int e, int s) {
+  return x == e ? s : (x == 0 ? e - s : x);
+}
+
+// The cell whose value before the fill ends up in cell (i, j, k) after it
+// (every phase of the reference's fill copies one cell into another and
+// never writes what it reads). The phases in the reference order are:
+// periodic faces X, Y, Z; edges along X, Y (j < yhi only), Z; corners;
+// non-periodic faces X, Y, Z. Walking them backwards, each phase that writes
+// the current cell replaces it by that phase's source.
+__device__ __forceinline__ void fill_source(const Fill &f, int &i, int &j, int &k) {
+  const int e0 = f.n0 - 1, e1 = f.n1 - 1, e2 = f.n2 - 1, s = f.s;
+  const bool p0 = f.per[0], p1 = f.per[1], p2 = f.per[2];
+  auto guard = [](int x, int e) { return x == 0 || x == e; };
+  auto inner = [](int x, int e) { return x >= 1 && x <= e - 1; };
+  if (!p2 && guard(k, e2)) k = k == 0 ? 1 : e2 - 1;   // non-periodic Z faces
+  if (!p1 && guard(j, e1)) j = j == 0 ? 1 : e1 - 1;   // non-periodic Y faces
+  if (!p0 && guard(i, e0)) i = i == 0 ? 1 : e0 - 1;   // non-periodic X faces
+  if ((p0 || p1 || p2) && guard(i, e0) && guard(j, e1) && guard(k, e2)) {   // corners
+    i = per_src(i, e0, s);
+    j = per_src(j, e1, s);
+    k = per_src(k, e2, s);
+  }
+  if ((p0 || p1) && inner(k, e2) && guard(i, e0) && guard(j, e1)) {   // edges along Z
+    i = per_src(i, e0, s);
+    j = per_src(j, e1, s);
+  }
+  if ((p0 || p2) && j >= 1 && j <= f.yhi - 1 && guard(i, e0) && guard(k, e2)) {   // along Y
+    i = per_src(i, e0, s);
+    k = per_src(k, e2, s);
+  }
+  if ((p1 || p2) && inner(i, e0) && guard(j, e1) && guard(k, e2)) {   // edges along X
+    j = per_src(j, e1, s);
+    k = per_src(k, e2, s);
+  }
+  if (p2 && inner(i, e0) && inner(j, e1) && guard(k, e2)) k = per_src(k, e2, s);   // Z faces
+  if (p1 && inner(i, e0) && inner(k, e2) && guard(j, e1)) j = per_src(j, e1, s);   // Y faces
+  if (p0 && inner(j, e1) && inner(k, e2) && guard(i, e0)) i = per_src(i, e0, s);   // X faces
+}
+
+// Guard-cell fill of narr arrays, first pass: every guard cell's final value
+// (from its fill_source, before any guard cell changes) into tmp.
 template <typename T>
-__global__ void __launch_bounds__(1024) k_hat_fill(Fill f, const __grid_constant__ Arrays<T> A) {
-  T *a = A.a[blockIdx.x];
-  const int n0 = f.n0, n1 = f.n1, n2 = f.n2, s = f.s;
-  const int e0 = n0 - 1, e1 = n1 - 1, e2 = n2 - 1;
-  const int f0 = e0 - s, f1 = e1 - s, f2 = e2 - s;
-  auto L = [=](int i, int j, int k) -> long { return ((long)i * n1 + j) * n2 + k; };
-  if (f.per[0])
-    fill_phase<T, 2, 4>(a, (e1 - 1) * (e2 - 1), [=](int t, int c, long &d, long &src) {
-      const int j = 1 + t / (e2 - 1), k = 1 + t % (e2 - 1);
-      d = c ? L(e0, j, k) : L(0, j, k);
-      src = c ? L(s, j, k) : L(f0, j, k);
-    });
-  if (f.per[1])
-    fill_phase<T, 2, 4>(a, (e0 - 1) * (e2 - 1), [=](int t, int c, long &d, long &src) {
-      const int i = 1 + t / (e2 - 1), k = 1 + t % (e2 - 1);
-      d = c ? L(i, e1, k) : L(i, 0, k);
-      src = c ? L(i, s, k) : L(i, f1, k);
-    });
-  if (f.per[2])
-    fill_phase<T, 2, 4>(a, (e0 - 1) * (e1 - 1), [=](int t, int c, long &d, long &src) {
-      const int i = 1 + t / (e1 - 1), j = 1 + t % (e1 - 1);
-      d = c ? L(i, j, e2) : L(i, j, 0);
-      src = c ? L(i, j, s) : L(i, j, f2);
-    });
-  if (f.per[1] || f.per[2])
-    fill_phase<T, 4, 2>(a, e0 - 1, [=](int t, int c, long &d, long &src) {
-      const int i = 1 + t;
-      const int dj[4] = {e1, 0, 0, e1}, dk[4] = {e2, 0, e2, 0};
-      const int sj[4] = {s, f1, f1, s}, sk[4] = {s, f2, s, f2};
-      d = L(i, dj[c], dk[c]);
-      src = L(i, sj[c], sk[c]);
-    });
-  if (f.per[0] || f.per[2])
-    fill_phase<T, 4, 2>(a, f.yhi - 1, [=](int t, int c, long &d, long &src) {
-      const int j = 1 + t;
-      const int di[4] = {e0, 0, 0, e0}, dk[4] = {e2, 0, e2, 0};
-      const int si[4] = {s, f0, f0, s}, sk[4] = {s, f2, s, f2};
-      d = L(di[c], j, dk[c]);
-      src = L(si[c], j, sk[c]);
-    });
-  if (f.per[0] || f.per[1])
-    fill_phase<T, 4, 2>(a, e2 - 1, [=](int t, int c, long &d, long &src) {
-      const int k = 1 + t;
-      const int di[4] = {e0, 0, e0, 0}, dj[4] = {e1, 0, 0, e1};
-      const int si[4] = {s, f0, s, f0}, sj[4] = {s, f1, f1, s};
-      d = L(di[c], dj[c], k);
-      src = L(si[c], sj[c], k);
-    });
-  if (f.per[0] || f.per[1] || f.per[2])
-    fill_phase<T, 8, 1>(a, 1, [=](int, int c, long &d, long &src) {
-      // corners in the reference's order; (bit 2, bit 1, bit 0) of c pick
-      // the far (e) or near (0) face along (x, y, z), reversed
-      const int ci = (c & 1) ? 0 : 1, cj = (c & 2) ? 0 : 1, ck = (c & 4) ? 0 : 1;
-      d = L(ci ? e0 : 0, cj ? e1 : 0, ck ? e2 : 0);
-      src = L(ci ? s : f0, cj ? s : f1, ck ? s : f2);
-    });
-  if (!f.per[0])
-    fill_phase<T, 2, 4>(a, n1 * n2, [=](int t, int c, long &d, long &src) {
-      const int j = t / n2, k = t % n2;
-      d = c ? L(e0, j, k) : L(0, j, k);
-      src = c ? L(e0 - 1, j, k) : L(1, j, k);
-    });
-  if (!f.per[1])
-    fill_phase<T, 2, 4>(a, n0 * n2, [=](int t, int c, long &d, long &src) {
-      const int i = t / n2, k = t % n2;
-      d = c ? L(i, e1, k) : L(i, 0, k);
-      src = c ? L(i, e1 - 1, k) : L(i, 1, k);
-    });
-  if (!f.per[2])
-    fill_phase<T, 2, 4>(a, n0 * n1, [=](int t, int c, long &d, long &src) {
-      const int i = t / n1, j = t % n1;
-      d = c ? L(i, j, e2) : L(i, j, 0);
-      src = c ? L(i, j, e2 - 1) : L(i, j, 1);
-    });
+__global__ void k_hat_guard_gather(Fill f, const __grid_constant__ Arrays<T> A, int narr,
+                                   T *__restrict__ tmp) {
+  const long G = guard_count(f), total = narr * G;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    guard_cell(f, t % G, i, j, k);
+    fill_source(f, i, j, k);
+    tmp[t] = A.a[t / G][((long)i * f.n1 + j) * f.n2 + k];
+  }
+}
+
+// Second pass: the values into the guard cells.
+template <typename T>
+__global__ void k_hat_guard_scatter(Fill f, const __grid_constant__ Arrays<T> A, int narr,
+                                    const T *__restrict__ tmp) {
+  const long G = guard_count(f), total = narr * G;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    guard_cell(f, t % G, i, j, k);
+    A.a[t / G][((long)i * f.n1 + j) * f.n2 + k] = tmp[t];
+  }
 }
 
 template <typename T>
@@ -338,10 +330,19 @@ int hat_densities(const spb_hat_desc *d, const T *const *mom, const T *const B[3
   g.inv[2] = d->invdz;
   const long cells = (long)g.nxc * g.nyc * g.nzc, nodes = (long)g.nxn * g.nyn * g.nzn;
   const int ns = d->ns;
-  T *tc = nullptr;   // three centre temporaries per species
-  SPB_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tc), 3 * ns * cells * sizeof(T), st));
   Fill fc{g.nxc, g.nyc, g.nzc, 1, g.nyn - 1, {d->periodic[0], d->periodic[1], d->periodic[2]}};
   Fill fn{g.nxn, g.nyn, g.nzn, 2, g.nyn - 1, {d->periodic[0], d->periodic[1], d->periodic[2]}};
+  // three centre temporaries per species, then the guard fills' buffer
+  const long gtmp = std::max(3 * ns * guard_count(fc), 3 * guard_count(fn));
+  T *tc = nullptr;
+  SPB_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tc),
+                           (3 * ns * cells + gtmp) * sizeof(T), st));
+  T *const gbuf = tc + 3 * ns * cells;
+  auto fill = [&](const Fill &f, const Arrays<T> &arr, int narr) {
+    const unsigned blocks = (unsigned)std::min<long>(blocks_for(narr * guard_count(f), 256), 4096);
+    k_hat_guard_gather<T><<<blocks, 256, 0, st>>>(f, arr, narr, gbuf);
+    k_hat_guard_scatter<T><<<blocks, 256, 0, st>>>(f, arr, narr, gbuf);
+  };
   Species6<T> S;   // kernel parameters (copied at launch)
   Arrays<T> A;
   std::memset(&S, 0, sizeof(S));
@@ -361,21 +362,21 @@ int hat_densities(const spb_hat_desc *d, const T *const *mom, const T *const B[3
   int rc = SPB_OK;
   const int gx = std::max(1, blocks_for(inner, 256) / ns);
   k_hat_div_tensor<T><<<dim3(gx, ns), 256, 0, st>>>(g, S, alfa);
-  k_hat_fill<T><<<3 * ns, 1024, 0, st>>>(fc, A);
+  fill(fc, A, 3 * ns);
   k_hat_pidot<T><<<blocks_for(nodes, 256), 256, 0, st>>>(g, S, ns, Vec3<T>{{B[0], B[1], B[2]}},
                                                          Out3<T>{{jxh, jyh, jzh}});
   Arrays<T> J{};
   J.a[0] = jxh;
   J.a[1] = jyh;
   J.a[2] = jzh;
-  k_hat_fill<T><<<3, 1024, 0, st>>>(fn, J);
+  fill(fn, J, 3);
   k_hat_rho<T><<<blocks_for(cells, 256), 256, 0, st>>>(g, Vec3<T>{{jxh, jyh, jzh}}, rhoc,
                                                        d->dt * d->th, rhoh);
   Arrays<T> R{};
   R.a[0] = rhoh;
-  k_hat_fill<T><<<1, 1024, 0, st>>>(fc, R);
+  fill(fc, R, 1);
   if (cudaGetLastError() != cudaSuccess) rc = fail(SPB_ERR_CUDA, "spb_hat_densities: launch");
-  g_launches += 6;
+  g_launches += 9;
   cudaFreeAsync(tc, st);
   return rc;
 }
