@@ -22,8 +22,8 @@
 //
 // Guard values. The reference leaves its temporaries' guard entries
 // uninitialised; the guard-cell fills overwrite every one of them before it
-// is read, in a fixed phase order that the fill kernel keeps (one CTA per
-// array, phases separated by barriers).
+// is read, each with the value its phase-by-phase fill would leave there
+// (fill_source).
 #include <algorithm>
 #include <cstring>
 
