@@ -113,6 +113,9 @@ int create_from_coords(const std::vector<float> &xn, const std::vector<float> &y
                        double Lx, double Ly, double Lz, spb_grid_ctx **out) {
   if (!out) return fail(SPB_ERR_INVALID, "spb_grid_create: null output pointer");
   *out = nullptr;
+  // the plain kernels index nodes with 32-bit integers
+  if ((double)xn.size() * (double)yn.size() * (double)zn.size() >= 2147483648.0)
+    return fail(SPB_ERR_UNSUPPORTED, "spb_grid_create: 2^31 nodes or more");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(SPB_ERR_NO_DEVICE, "spb_grid_create: no CUDA device");

@@ -107,7 +107,7 @@ __device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
   const float qomdt2 = p.qomdt2;
   float upt = 0.0f, vpt = 0.0f, wpt = 0.0f;
   float xc = x, yc = y, zc = z;
-  const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
+  const int sx = g.nyn * g.nzn, sy = g.nzn;   // nodes < 2^31 (spb_grid_create)
   for (int it = 0; it < p.niter; ++it) {
     const int ix = clamp_cell(cell_trunc(xc, g.xStart, g.invdx, g.nxn), g.nxn, bad);
     const int iy = clamp_cell(cell_trunc(yc, g.yStart, g.invdy, g.nyn), g.nyn, bad);
@@ -116,7 +116,7 @@ __device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
     const float eta[2] = {yc - __ldg(g.yn + iy - 1), __ldg(g.yn + iy) - yc};
     const float zeta[2] = {zc - __ldg(g.zn + iz - 1), __ldg(g.zn + iz) - zc};
     float Ex = 0.0f, Ey = 0.0f, Ez = 0.0f, Bx = 0.0f, By = 0.0f, Bz = 0.0f;
-    const long base = ix * sx + iy * sy + iz;
+    const int base = ix * sx + iy * sy + iz;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -124,7 +124,7 @@ __device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
           const float wgt = xi[a] * eta[b] * zeta[c] * g.invVOL;
-          const long n = base - a * sx - b * sy - c;
+          const int n = base - a * sx - b * sy - c;
           const float4 f4 = __ldg(F.eb4 + n);
           const float2 f2 = __ldg(F.eb2 + n);
           Ex += wgt * f4.x;
