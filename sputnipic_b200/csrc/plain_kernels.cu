@@ -266,13 +266,13 @@ template <bool ACC>
 __device__ __forceinline__ void deposit_warp(const GeomDev &g, const DepTarget &T, bool valid,
                                              const Particle &p, int &bad) {
   const int lane = threadIdx.x & 31;
-  const long sx = (long)g.nyn * g.nzn, sy = g.nzn;
-  long key = 0;
+  const int sx = g.nyn * g.nzn, sy = g.nzn;   // nodes < 2^31 (spb_grid_create)
+  int key = 0;
   if (valid) {
     const int ix = clamp_cell(cell_floor(p.x, g.xStart, g.invdx, g.nxn), g.nxn, bad);
     const int iy = clamp_cell(cell_floor(p.y, g.yStart, g.invdy, g.nyn), g.nyn, bad);
     const int iz = clamp_cell(cell_floor(p.z, g.zStart, g.invdz, g.nzn), g.nzn, bad);
-    key = ((long)ix * g.nyn + iy) * g.nzn + iz;
+    key = (ix * g.nyn + iy) * g.nzn + iz;
   }
   // this lane's totals after warp_sum80: physical node (bit4, bit3, bit2),
   // moments mbase + [lo, hi)
@@ -283,7 +283,7 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const DepTarget &
 #pragma unroll 1
   for (int round = 0; round < 4 && remaining; ++round) {
     const int leader = __ffs(remaining) - 1;
-    const long k = __shfl_sync(FULL, key, leader);
+    const int k = __shfl_sync(FULL, key, leader);
     const bool member = valid && key == k;
     const unsigned members = __ballot_sync(FULL, member);
     remaining &= ~members;
@@ -303,7 +303,7 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const DepTarget &
     if (member) half_terms<true>(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, 0);
     float r[5];
     warp_sum80_tail(t, r, lane);
-    const long node = k - na * sx - nb * sy - nc;
+    const int node = k - na * sx - nb * sy - nc;
 #pragma unroll
     for (int i = 0; i < 5; ++i)
       if (i >= lo && i < hi) dep_add<ACC>(T, node, mbase + i, r[i]);
@@ -333,7 +333,7 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const DepTarget &
       for (int j = 0; j < 6; ++j) e[j] = __shfl_sync(FULL, d[j], L);
       const float q = __shfl_sync(FULL, p.q, L), u = __shfl_sync(FULL, p.u, L);
       const float v = __shfl_sync(FULL, p.v, L), w = __shfl_sync(FULL, p.w, L);
-      const long k = __shfl_sync(FULL, key, L);
+      const int k = __shfl_sync(FULL, key, L);
       if (lane < 24) {
         const int node = lane / 3, grp = lane % 3;
         const int a = node >> 2, b = (node >> 1) & 1, c = node & 1;
