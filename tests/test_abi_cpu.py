@@ -88,6 +88,19 @@ def test_dropin_rejects_null_arguments_without_touching_the_gpu():
     assert lib.spb_mover_interp(None, None, None, None, None) == 2
 
 
+def test_grid_of_2_to_31_nodes_is_rejected_before_any_device_work():
+    """The plain kernels index nodes with 32-bit integers: a grid of 2^31
+    nodes or more is refused at creation, before the library looks for a
+    device."""
+    import ctypes
+    lib = _lib.load()
+    out = ctypes.c_void_p()
+    assert lib.spb_grid_create_uniform(1300, 1300, 1300, 1.0, 1.0, 1.0, ctypes.byref(out)) == 6
+    assert b"2^31" in lib.spb_last_error_message()
+    assert not out.value
+    lib.spb_clear_error()
+
+
 def test_plain_deposit_mode_switch():
     """spb_set_plain_deposit_mode returns the previous mode and rejects
     unknown ones (no device work)."""
