@@ -335,6 +335,13 @@ int spb_sim_moments(spb_sim *sim, int species, double *out, int on_device,
                     void *stream);
 /* applyBCids (src/BC.cpp:362-615) on a species' FP64 moments, in place. */
 int spb_sim_apply_bc_ids(spb_sim *sim, int species, void *stream);
+/* Device address of a species' FP64 moments ([10][nodes], reference order),
+ * valid until spb_sim_destroy; NULL on a bad argument. The caller may read
+ * or update them in place between cycles, as the reference's
+ * mpi_reduce_densities (src/mpi_comm.cpp:58-117) sums the ranks' moments
+ * into ids[is] after interpP2G (src/sputniPIC_CPU.cpp:262-265); the next
+ * cycle zeroes them. */
+double *spb_sim_moments_device(spb_sim *sim, int species);
 /* Positions x = (cell + offset) * dx, velocities and (if q is not NULL)
  * charges, as floats: cells in tile-major order, each cell's particles in
  * bucket order, then the overflow list. */

@@ -251,6 +251,7 @@ def load():
     _proto(lib, "spb_sim_resort", c_int, [P, P])
     _proto(lib, "spb_sim_moments", c_int, [P, c_int, P, c_int, P])
     _proto(lib, "spb_sim_apply_bc_ids", c_int, [P, c_int, P])
+    _proto(lib, "spb_sim_moments_device", P, [P, c_int])
     _proto(lib, "spb_sim_particles", c_int, [P, c_int] + [P] * 7 + [c_int, P])
     _proto(lib, "spb_sim_check", c_int, [P, P])
     _proto(lib, "spb_sort_particles_noalloc", c_int,

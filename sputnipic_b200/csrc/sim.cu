@@ -2421,6 +2421,14 @@ extern "C" int spb_sim_moments(spb_sim *s, int species, double *out, int on_devi
   return SPB_OK;
 }
 
+extern "C" double *spb_sim_moments_device(spb_sim *s, int species) {
+  if (!s || species < 0 || species >= (int)s->sp.size()) {
+    fail(SPB_ERR_INVALID, "spb_sim_moments_device: bad arguments");
+    return nullptr;
+  }
+  return s->sp[species].mom;
+}
+
 extern "C" int spb_sim_apply_bc_ids(spb_sim *s, int species, void *stream) {
   if (!s || species < 0 || species >= (int)s->sp.size())
     return fail(SPB_ERR_INVALID, "spb_sim_apply_bc_ids: bad arguments");

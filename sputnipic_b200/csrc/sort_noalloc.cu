@@ -14,8 +14,10 @@
 // each call clears the counters it needs first, so calls that run one after
 // another are fine, but calls that overlap on the GPU race on the scratch.
 // The first call on a device looks the array's device address up with
-// cudaGetSymbolAddress (a host-side name is not a device address); make that
-// first call before any stream capture.
+// cudaGetSymbolAddress (a host-side name is not a device address) and keeps
+// it for the life of the process; make that first call before any stream
+// capture. The stream must belong to the current device. Every call waits for
+// its stream before returning (it reads its error word back).
 #include <mutex>
 
 #include "grid_ctx.h"
@@ -187,13 +189,23 @@ __global__ void k_na_scatter(NaGrid g, const float *__restrict__ x, const float 
   if (bad) atomicOr(err, bad);
 }
 
-// Device address of the scratch array, looked up once per device.
-int scratch_address(int **out) {
+// Device address of the scratch array on the current device, looked up once
+// per device for the life of the process (a cudaDeviceReset invalidates it).
+// The stream must belong to the current device: the address is that device's.
+int scratch_address(cudaStream_t st, int **out) {
   static std::mutex mu;
   static int *addr[64] = {};
   int dev = 0;
   SPB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(SPB_ERR_UNSUPPORTED, "device index above 63");
+  if (st) {
+    int sdev = -1;
+    SPB_CUDA(cudaStreamGetDevice(st, &sdev));
+    if (sdev != dev)
+      return fail(SPB_ERR_INVALID,
+                  "spb_sort_particles_noalloc: the stream belongs to another device than the "
+                  "current one");
+  }
   std::lock_guard<std::mutex> lk(mu);
   if (!addr[dev]) {
     void *p = nullptr;
@@ -267,8 +279,9 @@ extern "C" int spb_sort_particles_noalloc(const spb_sim_desc *d, const float *x,
                     d->tile[2] ? d->tile[2] : 4};
   if (d->nxc % t[0] || d->nyc % t[1] || d->nzc % t[2])
     return fail(SPB_ERR_UNSUPPORTED, "spb_sort_particles_noalloc: cells must be tile multiples");
+  cudaStream_t st = (cudaStream_t)stream;
   int *scratch = nullptr;
-  if (int rc = scratch_address(&scratch)) return rc;
+  if (int rc = scratch_address(st, &scratch)) return rc;
   NaGrid g;
   g.nxc = d->nxc;
   g.nyc = d->nyc;
@@ -280,7 +293,6 @@ extern "C" int spb_sort_particles_noalloc(const spb_sim_desc *d, const float *x,
   g.invdz = 1.0 / (d->Lz / d->nzc);
   const float *in[7] = {x, y, z, u, v, w, q};
   float *out[7] = {ox, oy, oz, u_out, v_out, w_out, q_out};
-  cudaStream_t st = (cudaStream_t)stream;
   if (t[0] == 8 && t[1] == 4 && t[2] == 4)
     return na_sort<8, 4, 4>(g, ncells, in, n, cell, out, cell_start, scratch, st);
   if (t[0] == 4 && t[1] == 4 && t[2] == 4)

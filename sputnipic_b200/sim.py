@@ -108,6 +108,23 @@ class Simulation:
         _lib.check(self.lib.spb_sim_moments(self.h, s, out.data_ptr(), 1, _stream(stream)))
         return out
 
+    def apply_bc_ids(self, s: int, stream=None):
+        """applyBCids on species s's FP64 moments, in place."""
+        _lib.check(self.lib.spb_sim_apply_bc_ids(self.h, s, _stream(stream)))
+
+    def moments_view(self, s: int):
+        """Species s's FP64 moments as a (10, nodes) CUDA tensor sharing the
+        simulation's memory (no copy); valid until close(), zeroed by the
+        next cycle. Used to sum the moments over ranks in place."""
+        import torch
+        ptr = self.lib.spb_sim_moments_device(self.h, s)
+        if not ptr:
+            raise RuntimeError(_lib.last_error())
+        iface = {"shape": (10, self.nodes), "typestr": "<f8", "data": (ptr, False),
+                 "version": 3, "strides": None}
+        view = type("MomentsView", (), {"__cuda_array_interface__": iface})()
+        return torch.as_tensor(view, device="cuda")
+
     def particles(self, s: int, stream=None) -> dict:
         """Positions (domain units), velocities and charges of species s,
         float32 CUDA tensors in cell order (then the overflow list)."""

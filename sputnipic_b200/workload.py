@@ -274,6 +274,41 @@ def gem_particles(wl: GemWorkload, s: int, cell_lo: int = 0, cell_hi: int | None
             "qom": sp.qom, "cell": cell.astype(np.int32)}
 
 
+def _particles_chunk(args):
+    wl, s, lo, hi = args
+    p = gem_particles(wl, s, lo, hi)
+    return lo, {k: p[k] for k in "xyzuvwq"}
+
+
+def gem_particles_host(wl: GemWorkload, species=None, procs: int | None = None,
+                       slabs_per_chunk: int = 2) -> list:
+    """gem_particles of every cell for each species in ``species`` (all by
+    default), generated by a pool of ``procs`` spawned processes (default:
+    the host's cores), chunk by chunk of ``slabs_per_chunk`` x-slabs of cells
+    and assembled in cell order: the same arrays as one gem_particles call per
+    species. Returns a list of dicts (x..q float32, qom)."""
+    import multiprocessing as mp
+    import os
+    species = range(len(wl.species)) if species is None else species
+    plane = wl.nyc * wl.nzc
+    step = slabs_per_chunk * plane
+    procs = procs or os.cpu_count() or 1
+    out = []
+    with mp.get_context("spawn").Pool(procs) as pool:
+        for s in species:
+            ppc = wl.species[s].ppc
+            n = wl.species_count(s)
+            arr = {k: np.empty(n, np.float32) for k in "xyzuvwq"}
+            chunks = [(wl, s, lo, min(lo + step, wl.cells)) for lo in range(0, wl.cells, step)]
+            for lo, p in pool.imap_unordered(_particles_chunk, chunks):
+                a = int(np.floor(lo * ppc + 1e-9))
+                for k in "xyzuvwq":
+                    arr[k][a:a + len(p[k])] = p[k]
+            arr["qom"] = wl.species[s].qom
+            out.append(arr)
+    return out
+
+
 def zero_moments(wl: GemWorkload, dtype=np.float32):
     return [np.zeros(wl.nodes, dtype) for _ in range(10)]
 

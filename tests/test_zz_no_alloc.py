@@ -45,17 +45,17 @@ def tile_keys(wl, cx, cy, cz, tile=TILE):
         + ((cx % TX) * TY + cy % TY) * TZ + cz % TZ
 
 
-def noalloc_sort(torch, wl, dev, n):
+def noalloc_sort(torch, wl, dev, n, tile=TILE, expect=0):
     lib = _lib.load()
     out = {"cell": torch.empty(n, dtype=torch.int32, device="cuda")}
     for k in ("ox", "oy", "oz", "u", "v", "w", "q"):
         out[k] = torch.empty(n, dtype=torch.float32, device="cuda")
     cs = torch.empty(wl.cells + 1, dtype=torch.int32, device="cuda")
     rc = lib.spb_sort_particles_noalloc(
-        ctypes.byref(desc_for(wl)), *[dev[k].data_ptr() for k in "xyzuvwq"], n,
+        ctypes.byref(desc_for(wl, tile)), *[dev[k].data_ptr() for k in "xyzuvwq"], n,
         *[out[k].data_ptr() for k in ("cell", "ox", "oy", "oz", "u", "v", "w", "q")],
         cs.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
-    assert rc == 0, _lib.last_error()
+    assert rc == expect, _lib.last_error()
     h = {k: v.cpu().numpy() for k, v in out.items()}
     return h, cs.cpu().numpy()
 
@@ -71,12 +71,12 @@ def positions(wl, h):
     return x, y, z, cx, cy, cz
 
 
-def check_against_existing(wl, h, cs, ref, n):
+def check_against_existing(wl, h, cs, ref, n, tile=TILE):
     assert cs[0] == 0 and cs[-1] == n and (np.diff(cs) >= 0).all()
     x, y, z, cx, cy, cz = positions(wl, h)
     # every particle sits in the segment of its own cell
     seg = np.repeat(np.arange(wl.cells), np.diff(cs))
-    assert np.array_equal(seg, tile_keys(wl, cx, cy, cz))
+    assert np.array_equal(seg, tile_keys(wl, cx, cy, cz, tile))
     order = np.argsort(h["q"], kind="stable")
     rorder = np.argsort(ref["q"], kind="stable")
     assert np.array_equal(h["q"][order], ref["q"][rorder])
@@ -86,7 +86,10 @@ def check_against_existing(wl, h, cs, ref, n):
         assert np.array_equal(h[k][order], ref[k][rorder]), k
 
 
-def test_noalloc_sort_matches_allocating_load_two_calls(cuda):
+@pytest.mark.parametrize("tile", [(8, 4, 4), (4, 4, 4), (2, 2, 2), (8, 8, 4)])
+def test_noalloc_sort_matches_allocating_load_two_calls(cuda, tile):
+    """Every tile shape the library instantiates: two calls in a row against
+    the allocating load, then a smaller call after the larger one."""
     torch = cuda
     from sputnipic_b200.sim import Simulation
     wl = W.small_gem()
@@ -94,22 +97,40 @@ def test_noalloc_sort_matches_allocating_load_two_calls(cuda):
     n = len(host["x"])
     host["q"] = np.arange(n, dtype=np.float32)       # unique tags
     dev = {k: torch.from_numpy(host[k]).cuda() for k in "xyzuvwq"}
-    sim = Simulation(wl, tile=TILE, species=[0])
+    sim = Simulation(wl, tile=tile, species=[0])
     sim.load_species(0, dev)
     ref = {k: v.cpu().numpy() for k, v in sim.particles(0).items()}
     sim.close()
     for _ in range(2):                               # two calls in a row
-        h, cs = noalloc_sort(torch, wl, dev, n)
-        check_against_existing(wl, h, cs, ref, n)
+        h, cs = noalloc_sort(torch, wl, dev, n, tile)
+        check_against_existing(wl, h, cs, ref, n, tile)
     # a smaller call after a larger one: the counters start from zero again
     m = n // 3
     half = {k: v[:m].contiguous() for k, v in dev.items()}
-    sim = Simulation(wl, tile=TILE, species=[0])
+    sim = Simulation(wl, tile=tile, species=[0])
     sim.load_species(0, half)
     ref_m = {k: v.cpu().numpy() for k, v in sim.particles(0).items()}
     sim.close()
-    h, cs = noalloc_sort(torch, wl, half, m)
-    check_against_existing(wl, h, cs, ref_m, m)
+    h, cs = noalloc_sort(torch, wl, half, m, tile)
+    check_against_existing(wl, h, cs, ref_m, m, tile)
+
+
+def test_noalloc_sort_reports_positions_outside_the_domain(cuda):
+    """One position beyond Lx: SPB_ERR_OUT_OF_GRID; the next clean call on
+    the shared scratch returns 0 again (its error word was cleared)."""
+    torch = cuda
+    wl = W.small_gem()
+    host = W.gem_particles(wl, 0)
+    n = len(host["x"])
+    host["q"] = np.arange(n, dtype=np.float32)
+    bad = {k: host[k].copy() for k in "xyzuvwq"}
+    bad["x"][n // 2] = np.float32(wl.Lx * 1.5)
+    dev_bad = {k: torch.from_numpy(bad[k]).cuda() for k in "xyzuvwq"}
+    noalloc_sort(torch, wl, dev_bad, n, expect=3)     # SPB_ERR_OUT_OF_GRID
+    assert b"outside" in _lib.load().spb_last_error_message()
+    dev = {k: torch.from_numpy(host[k]).cuda() for k in "xyzuvwq"}
+    h, cs = noalloc_sort(torch, wl, dev, n)
+    assert cs[-1] == n
 
 
 def test_noalloc_sort_rejects_grids_beyond_its_scratch(cuda):
@@ -118,10 +139,10 @@ def test_noalloc_sort_rejects_grids_beyond_its_scratch(cuda):
     assert big.cells > (1 << 20)
     rc = lib.spb_sort_particles_noalloc(ctypes.byref(desc_for(big)), *([None] * 7), 0,
                                         *([None] * 8), None, None)
-    assert rc == _lib.load().spb_last_error()
+    assert rc == 2 == lib.spb_last_error()            # SPB_ERR_INVALID: null cell_start
     # a null cell_start is rejected first; with one given, the capacity check fires
     cs = cuda.empty(1, dtype=cuda.int32, device="cuda")
     rc = lib.spb_sort_particles_noalloc(ctypes.byref(desc_for(big)), *([None] * 7), 0,
                                         *([None] * 8), cs.data_ptr(), None)
-    assert rc == 8
+    assert rc == 8 == lib.spb_last_error()            # SPB_ERR_CAPACITY
     assert b"cells" in lib.spb_last_error_message()
