@@ -6,8 +6,10 @@ Workload: 128x64x64 cells, 4 species x 65,536,000 particles (125 ppc on a
 5x5x5 jittered sub-lattice), NiterMover = 3, E ~ U(-1e-3, 1e-3) plus the
 Harris-sheet B; seeded synthetic inputs generated on the device. One step is
 one cycle of the hot section of the reference driver
-(src/sputniPIC_CPU.cpp:232-256): mover_PC for every species, zero the
-moments, interpP2G + applyBCids for every species.
+(src/sputniPIC_CPU.cpp:232-256, with the field refresh of :288-294): the new
+fields, mover_PC for every species, zero the moments, interpP2G + applyBCids
+for every species, and with N ranks the moment sum over the ranks
+(src/sputniPIC_CPU.cpp:262-265).
 
 Keys of the JSON line:
   value       particles pushed+deposited per second with all inputs already
@@ -18,15 +20,20 @@ Keys of the JSON line:
               moments and downloads the results, inside the timed region
   roofline    the dominant kernel's algorithmic bytes per launch / its mean
               CUDA-event duration, against MEASURED_PEAKS.json's HBM copy
-              bandwidth
+              bandwidth; frac_contract is the whole step against the
+              compulsory 60 bytes per particle plus the grid bytes
   cpu_baseline  the reference CPU code (oracle/_ref, else the restated port)
-              timed on this host's cores on a bounded sample of the workload
-The particle arrays (7.3 GB) are far larger than the 126 MB L2, so no L2
+              timed on this host's cores over whole cycles of the same
+              workload (one warm-up cycle, two timed)
+The particle arrays (8.4 GB) are far larger than the 126 MB L2, so no L2
 flush is needed between steps.
 
 ``--impl reference`` times the reference's own CPU mover_PC + interpP2G +
-applyBCids (the CPU driver's hot section) on a bounded sample per step with
-all host threads; under torchrun only rank 0 runs it.
+applyBCids (the CPU driver's hot section) on the full workload, W warm-up and
+K timed cycles, with all host threads; under torchrun only rank 0 runs it.
+
+``--gpus N`` without torchrun's environment starts N ranks itself (one per
+GPU, torch.distributed.run over 127.0.0.1).
 """
 from __future__ import annotations
 
@@ -111,56 +118,46 @@ class Clocks:
 
 
 # --- CPU reference arm ------------------------------------------------------------
-def cpu_sample(wl, slabs: int):
-    """Fields of the whole grid and the particles of the first ``slabs``
-    x-slabs of cells of every species (host generator)."""
-    fields = W.gem_fields(wl)
-    hi = slabs * wl.nyc * wl.nzc
-    parts = [W.gem_particles(wl, s, 0, hi) for s in range(len(wl.species))]
-    for p in parts:
-        p.pop("cell")
-    return fields, parts
-
-
-def time_cpu(wl, slabs: int, steps: int, warmup: int, min_seconds: float = 0.0):
-    """Times the CPU driver's hot section on a sample; returns per-step times,
-    the sample size and the oracle kind/threads."""
+def cpu_cycles(wl, parts, steps: int, warmup: int):
+    """Times whole cycles of the CPU driver's hot section (mover_PC for every
+    species, zero, interpP2G + applyBCids per species, timed inside the
+    library with omp_get_wtime) on ``parts`` (list of host particle dicts
+    with qom). Returns the timed cycles' seconds, the oracle kind ("reference"
+    when oracle/_ref was built, else "port") and its threads."""
     import oracle
     kind = "reference" if oracle.reference_available(32) else "restated"
     orc = oracle.CpuOracle(kind, 32)
-    fields, parts = cpu_sample(wl, slabs)
+    fields = W.gem_fields(wl)
     setup = oracle.setup_from(wl)
-    n = sum(len(p["x"]) for p in parts)
     mom = [np.zeros(wl.nodes, np.float32) for _ in range(10 * len(parts))]
     times = []
-    t_start = time.perf_counter()
-    i = 0
-    while i < warmup + steps or (time.perf_counter() - t_start < min_seconds and i < 200):
+    for i in range(warmup + steps):
         tm, ti = orc.cycle(setup, fields, parts, mom)
         if i >= warmup:
             times.append(tm + ti)
-        i += 1
-    return times, n, ("reference" if kind == "reference" else "port"), orc.threads
+    return times, ("reference" if kind == "reference" else "port"), orc.threads
 
 
 def run_reference_arm(args, rank):
     if rank != 0:
         return
     wl = W.gem()
-    slabs = args.cpu_slabs
-    times, n, kind, cores = time_cpu(wl, slabs, args.steps, args.warmup)
+    parts = W.gem_particles_host(wl)
+    n = sum(len(p["x"]) for p in parts)
+    times, kind, cores = cpu_cycles(wl, parts, args.steps, args.warmup)
     t = sum(times)
     pps = n * len(times) / t
-    sample = (f"first {slabs} of 128 x-slabs of cells of the GEM workload: {n} particles "
-              f"({n // len(wl.species)} per species), full 128x64x64 grid fields")
+    sample = (f"the whole workload every step: {n} particles ({n // len(parts)} per species), "
+              f"full 128x64x64 grid; {args.warmup} warm-up and {len(times)} timed cycles")
     line = {
         "impl": "reference", "metric": METRIC, "value": pps, "unit": UNIT,
         "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
-        "ms_per_step": 1e3 * t / len(times) * (wl.total_particles / n),
+        "ms_per_step": 1e3 * t / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": pps / PUBLISHED_PPS,
         "dtype": "fp32", "data": "synthetic (seeded GEM Harris sheet)",
-        "config": {"workload": wl.name, "particles": wl.total_particles, "niter": wl.niter,
-                   "sample_particles": n, "form": "reference CPU (mover_PC + interpP2G + applyBCids)"},
+        "config": {"workload": wl.name, "particles": n, "niter": wl.niter,
+                   "form": "reference CPU (mover_PC + interpP2G + applyBCids)",
+                   "step_seconds": times},
         "cpu_baseline": {"value": pps, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": pps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -218,6 +215,7 @@ def measure_plain(args, torch, wl, fields, parts, dist, stream):
     pushes = [push_params(wl, s) for s in range(ns)]
     mom = torch.zeros(ns, 10, wl.nodes, device="cuda")
     ev = {"mover": [], "p2g": []}
+    peak = peaks()[0]
 
     def timed(kind, n, fn, record):
         if record:
@@ -252,8 +250,10 @@ def measure_plain(args, torch, wl, fields, parts, dist, stream):
         durs = [a.elapsed_time(b) for a, b, _ in lst]
         n_mean = statistics.mean(c for _, _, c in lst)
         alg = algorithmic_bytes(k, int(n_mean), wl.nodes)
+        ach = alg / (statistics.mean(durs) / 1e3) / 1e9
         kern[k] = {"ms_mean": statistics.mean(durs), "share": sum(durs) / ms,
-                   "achieved_gbs": alg / (statistics.mean(durs) / 1e3) / 1e9}
+                   "algorithmic_bytes": alg, "achieved_gbs": ach, "frac": ach / peak,
+                   "peak_gbs": peak}
     ctx.close()
     del mom
     return {"value": sum(counts) * steps / (ms / 1e3), "ms_per_step": ms / steps,
@@ -278,8 +278,22 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     sim.set_fields(fields)
     for s, p in enumerate(parts):
         sim.load_species(s, p)
-    for _ in range(args.warmup):
+    views = [sim.moments_view(s) for s in range(ns)]
+
+    def step():
+        # the driver's cycle: new fields (uploaded from device arrays and
+        # packed), mover + deposit of every species, applyBCids per species,
+        # and with several ranks the moment sum (mpi_reduce_densities)
+        sim.set_fields(fields)
         sim.cycle(1)
+        for s in range(ns):
+            sim.apply_bc_ids(s)
+        if dist is not None:
+            for v in views:
+                R.reduce_moments(v, dist)
+
+    for _ in range(args.warmup):
+        step()
     rc = sim.check()
     if rc:
         raise RuntimeError(f"precision warm-up status {rc}: {_lib.last_error()}")
@@ -287,7 +301,7 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     l0 = lib.spb_launch_count()
     local_rank = torch.cuda.current_device()
     with Clocks(local_rank) as clk:
-        ms = device_timed(torch, dist, stream, args.steps, lambda: sim.cycle(1))
+        ms = device_timed(torch, dist, stream, args.steps, step)
     launches = lib.spb_launch_count() - l0
     # per-kernel breakdown: a separate pass with CUDA events around each kernel
     # (direct launches), outside the timed region above
@@ -321,9 +335,24 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
     d = kernels[dom]
     cyc_ms = kernels["push"]["ms_mean"] + kernels["deposit"]["ms_mean"]
     cyc_alg = kernels["push"]["algorithmic_bytes"] + kernels["deposit"]["algorithmic_bytes"]
+    # the contract's compulsory bytes of the whole step: 60 B per particle
+    # (read 32: int32 cell + 3 fp32 offsets + 3 fp32 velocities + fp32 q;
+    # write 28) plus the grid (fields read once, 6 x fp32; every species' ten
+    # fp64 moments written once), over the device-timed step
+    step_s = ms / args.steps / 1e3
+    grid_bytes = wl.nodes * (6 * 4 + ns * 10 * 8)
+    contract_bytes = 60 * n + grid_bytes
     roofline = {
         "kernel": d["kernel"], "bound": "hbm", "achieved": d["achieved"], "peak": peak,
         "unit": "GB/s", "frac": d["frac"], "traffic": d["traffic"],
+        "traffic_source": ("not measured in this run: DRAM bytes per particle (and per node and "
+                           "species) of the committed ncu capture profiles/traffic.json (one "
+                           "species, 64x64x64 cells at this workload's cell size and ppc) "
+                           "times this launch's particles (and nodes x species)"),
+        "frac_contract": contract_bytes / step_s / 1e9 / peak,
+        "contract": {"bytes_per_particle": 60, "grid_bytes": grid_bytes,
+                     "bytes_per_step": contract_bytes, "achieved": contract_bytes / step_s / 1e9,
+                     "basis": "whole device-timed step (fields, push, deposit, applyBCids)"},
         "algorithmic_bytes": d["algorithmic_bytes"], "kernel_ms_mean": d["ms_mean"],
         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
         "share_of_step": d["share_of_step"], "kernels": kernels,
@@ -401,11 +430,20 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        times, n, kind, cores = time_cpu(wl, args.cpu_slabs, 3, 1, min_seconds=10.0)
-        cpu = {"value": n / statistics.median(times), "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": f"first {args.cpu_slabs} of 128 x-slabs of cells ({n} particles, "
-                         f"full 128x64x64 grid fields); median of {len(times)} cycles of "
-                         "mover_PC + interpP2G + applyBCids"}
+        # whole cycles of the same workload on the host's cores: the pinned
+        # host copies (moved by the e2e leg, which is as good a state of the
+        # workload as any) or fresh copies of the device arrays
+        if host is None:
+            parts = [gen_particles(wl, s) for s in range(ns)]
+            host = [{k: p[k].cpu() for k in "xyzuvwq"} for p in parts]
+            del parts
+        cparts = [dict({k: host[s][k].numpy() for k in "xyzuvwq"}, qom=wl.species[s].qom)
+                  for s in range(ns)]
+        times, kind, cores = cpu_cycles(wl, cparts, 2, 1)
+        cpu = {"value": ntot * len(times) / sum(times), "unit": UNIT, "cores": cores,
+               "kind": kind, "ms_per_step": 1e3 * sum(times) / len(times),
+               "sample": f"the whole workload ({ntot} particles): one warm-up and "
+                         f"{len(times)} timed cycles of mover_PC + interpP2G + applyBCids"}
 
     if rank == 0:
         value = prec["value"]
@@ -559,13 +597,54 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
                     "pinned host arrays; timed on the host clock"}
 
 
+def launch_ranks(n: int) -> int:
+    """Runs this script with the same arguments as n ranks under
+    torch.distributed.run on this node (rendezvous on 127.0.0.1); returns the
+    launcher's exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def rank_selftest(out: str, rank: int, world: int):
+    """The multi-rank plumbing of the benchmark without a GPU: the ranks join
+    a gloo process group as the GPU run joins NCCL, each takes its own seeded
+    copy of a small GEM workload (sputnipic_b200.ranks.rank_workload), sums
+    its particles' charge-weighted x per cell (a linear deposit that depends
+    on the seeded positions) over the ranks with the
+    same reduce_moments the GPU step uses, and reports the slowest of
+    rank-dependent times through max_over_ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        wl = R.rank_workload(W.small_gem(nxc=8, nyc=4, nzc=4,
+                                         species=W.gem_species((8, 8, 8, 8))), rank)
+        p = W.gem_particles(wl, 0)
+        local = np.bincount(p["cell"], weights=p["q"].astype(np.float64) * p["x"],
+                            minlength=wl.cells)
+        mom = torch.from_numpy(local.copy())
+        R.reduce_moments(mom, dist)
+        slowest = R.max_over_ranks(1.5 + rank, dist, device="cpu")
+        np.savez(f"{out}.{rank}.npz", local=local, summed=mom.numpy(), slowest=slowest,
+                 world=world, seed=wl.seed)
+    finally:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-slabs", type=int, default=4)
     ap.add_argument("--tile", type=int, nargs=3, default=[8, 4, 4])
     ap.add_argument("--nspecies", type=int, default=4,
                     help="smaller profiling cases only; the benchmark uses all 4")
@@ -596,12 +675,24 @@ def main():
     ap.add_argument("--no-batching", action="store_true",
                     help="skip the batching-form measurement (uneven species, autotuned)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--selftest-ranks", metavar="OUT", default=None,
+                    help="check the multi-rank plumbing on the CPU (gloo): every rank sums its "
+                         "particles' charge-weighted x per cell over the ranks and writes "
+                         "OUT.<rank>.npz")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: run this script again under torch.distributed.run
+        sys.exit(launch_ranks(args.gpus))
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}")
+    if args.selftest_ranks:
+        rank_selftest(args.selftest_ranks, rank, world)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank)
         return
