@@ -296,6 +296,19 @@ typedef struct spb_sim_desc {
   int graph;                /* 1: each cycle's launches (zeroing, push,
                                deposit) replay as a CUDA graph captured per
                                buffer-parity pattern; not while timing */
+  int deterministic;        /* 1: bitwise reproducible moments. Every deposit
+                               term is rounded down to a power-of-two grid
+                               (2^-38 of the species' largest |q| x
+                               max(1, 16 |v|max^2) at load) and summed exactly
+                               in FP64, so the moments do not depend on the
+                               particles' order in their buckets or on the
+                               order of the atomics; the push gives every
+                               particle the same result on every path. Two
+                               runs from the same inputs give identical
+                               moments and the same particles. One thread per
+                               cell with 80 FP64 sums: slower than the default
+                               deposit. spb_sim_check reports SPB_ERR_CAPACITY
+                               if a sum ever left its exact range. */
 } spb_sim_desc;
 
 /* Whether a tile shape has an instantiated kernel. */

@@ -146,7 +146,8 @@ class SimDesc(ctypes.Structure):
                 ("dt", c_double), ("c", c_double), ("niter", c_int), ("periodic", c_int * 3),
                 ("ns", c_int), ("qom", c_double * 8), ("capacity", c_long * 8),
                 ("tile", c_int * 3), ("resort_every", c_int), ("ctas", c_int),
-                ("variant", c_int), ("bucket_slots", c_int), ("graph", c_int)]
+                ("variant", c_int), ("bucket_slots", c_int), ("graph", c_int),
+                ("deterministic", c_int)]
 
 
 HAT_MAX_SPECIES = 16

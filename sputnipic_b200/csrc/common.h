@@ -54,6 +54,7 @@ enum : int {
   ERRBIT_TIMEOUT = 2,       // a bounded wait for a TMA copy ran out
   ERRBIT_SMEM_ALIGN = 8,    // dynamic shared memory not 128-byte aligned
   ERRBIT_LOST = 16,         // a bucket and the overflow list were both full
+  ERRBIT_INEXACT = 32,      // a deterministic deposit sum left its exact range
 };
 
 inline long ceil_div(long a, long b) { return (a + b - 1) / b; }

@@ -131,7 +131,7 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
 __device__ __forceinline__ int floor_split(float p, float &s) {
   constexpr float M = 12582912.0f;   // 1.5 * 2^23
   const float t = __fadd_rd(p, M);
-  s = t - M;
+  s = __fsub_rn(t, M);
   return __float_as_int(t) - __float_as_int(M);
 }
 
@@ -141,7 +141,7 @@ __device__ __forceinline__ int floor_split(float p, float &s) {
 __device__ __forceinline__ void locate(float p, int c, int &g, float &f) {
   float s;
   g = c + floor_split(p, s);
-  f = p - s;
+  f = __fsub_rn(p, s);
 }
 
 // Below the domain the reference's int() truncates toward zero
@@ -180,10 +180,10 @@ __device__ __forceinline__ void bc_cell(int &c, float &o, float &vel, int N, int
 
 // Final position update on one axis: p = o + displacement, new cell and offset.
 __device__ __forceinline__ void advance(int &c, float &o, float disp) {
-  const float p = o + disp;
+  const float p = __fadd_rn(o, disp);
   float s;
   c += floor_split(p, s);
-  o = p - s;
+  o = __fsub_rn(p, s);
   const bool wrap = o >= 1.0f;
   c = wrap ? c + 1 : c;
   o = wrap ? 0.0f : o;
@@ -222,29 +222,35 @@ struct Tile {
 
 // Trilinear gather of E and B from the node array in HBM/L2, for a particle
 // whose nodes lie outside the staged tile (rare: kept out of line, so the
-// staged gather's registers and code stay those of the common case).
+// staged gather's registers and code stay those of the common case). The
+// same operations in the same order as the staged gather below, so a
+// particle's push does not depend on which of the two paths served it.
 __device__ __noinline__ Field6 gather_global(const float *__restrict__ fields8, int nxc, int nyc,
                                              int nzc, int nyn, int nzn, int gx, int gy, int gz,
                                              float fx, float fy, float fz) {
   const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
-  Field6 F = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   const long sy = nzn, sx = (long)nyn * nzn;
   const int hx = min(max(gx, -1), nxc), hy = min(max(gy, -1), nyc), hz = min(max(gz, -1), nzc);
   const long n0 = (long)(hx + 1) * sx + (long)(hy + 1) * sy + (hz + 1);
+  Field6 F[2];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
-      const float wab = wx[a] * wy[b];
+      const float wab = __fmul_rn(wx[a], wy[b]);
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const long n = n0 + a * sx + b * sy + c;
         const float4 A = __ldg(reinterpret_cast<const float4 *>(fields8 + 8 * n));
         const float2 B = __ldg(reinterpret_cast<const float2 *>(fields8 + 8 * n + 4));
-        acc_node(F, wab * wz[c], A, B);
+        if (b == 0 && c == 0)
+          F[a] = first_node(__fmul_rn(wab, wz[c]), A, B);
+        else
+          acc_node(F[a], __fmul_rn(wab, wz[c]), A, B);
       }
     }
-  return F;
+  return {__fadd2_rn(F[0].exy, F[1].exy), __fadd2_rn(F[0].ezbx, F[1].ezbx),
+          __fadd2_rn(F[0].byz, F[1].byz)};
 }
 
 // Trilinear gather of E and B at fraction f per axis from the staged tile,
@@ -260,16 +266,16 @@ __device__ __forceinline__ Field6 gather(const float *__restrict__ sF, int n0, f
   for (int a = 0; a < 2; ++a) {
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
-      const float wab = wx[a] * wy[b];
+      const float wab = __fmul_rn(wx[a], wy[b]);
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const int n = n0 + (a * T::BY + b) * T::BZ + c;
         const float4 A = *reinterpret_cast<const float4 *>(sF + 8 * n);
         const float2 B = *reinterpret_cast<const float2 *>(sF + 8 * n + 4);
         if (b == 0 && c == 0)   // each layer's sum starts from its first product
-          F[a] = first_node(wab * wz[c], A, B);
+          F[a] = first_node(__fmul_rn(wab, wz[c]), A, B);
         else
-          acc_node(F[a], wab * wz[c], A, B);
+          acc_node(F[a], __fmul_rn(wab, wz[c]), A, B);
       }
     }
   }
@@ -295,20 +301,26 @@ __device__ __forceinline__ int tile_node(int c0x, int c0y, int c0z, int gx, int 
 __device__ __forceinline__ void boris(const CycleParams &P, const Field6 &F, float qomdt2,
                                       float u, float v, float w, float &up, float &vp, float &wp,
                                       float &dx, float &dy, float &dz) {
+  // every operation spelled out (no contraction left to the compiler), so
+  // each inlined copy of the push rounds alike
   const float ex = F.exy.x, ey = F.exy.y, ez = F.ezbx.x;
   const float bx = F.ezbx.y, by = F.byz.x, bz = F.byz.y;
-  const float omdtsq = qomdt2 * qomdt2 * (bx * bx + by * by + bz * bz);
-  const float denom = __fdividef(1.0f, 1.0f + omdtsq);
-  const float ut = fmaf(qomdt2, ex, u);
-  const float vt = fmaf(qomdt2, ey, v);
-  const float wt = fmaf(qomdt2, ez, w);
-  const float qud = qomdt2 * (ut * bx + vt * by + wt * bz);
-  up = fmaf(qomdt2, vt * bz - wt * by + qud * bx, ut) * denom;
-  vp = fmaf(qomdt2, wt * bx - ut * bz + qud * by, vt) * denom;
-  wp = fmaf(qomdt2, ut * by - vt * bx + qud * bz, wt) * denom;
-  dx = up * P.hdt[0];
-  dy = vp * P.hdt[1];
-  dz = wp * P.hdt[2];
+  const float b2 = __fmaf_rn(bz, bz, __fmaf_rn(by, by, __fmul_rn(bx, bx)));
+  const float omdtsq = __fmul_rn(__fmul_rn(qomdt2, qomdt2), b2);
+  const float denom = __fdividef(1.0f, __fadd_rn(1.0f, omdtsq));
+  const float ut = __fmaf_rn(qomdt2, ex, u);
+  const float vt = __fmaf_rn(qomdt2, ey, v);
+  const float wt = __fmaf_rn(qomdt2, ez, w);
+  const float qud = __fmul_rn(qomdt2, __fmaf_rn(wt, bz, __fmaf_rn(vt, by, __fmul_rn(ut, bx))));
+  up = __fmul_rn(__fmaf_rn(qomdt2, __fmaf_rn(qud, bx, __fmaf_rn(-wt, by, __fmul_rn(vt, bz))), ut),
+                 denom);
+  vp = __fmul_rn(__fmaf_rn(qomdt2, __fmaf_rn(qud, by, __fmaf_rn(-ut, bz, __fmul_rn(wt, bx))), vt),
+                 denom);
+  wp = __fmul_rn(__fmaf_rn(qomdt2, __fmaf_rn(qud, bz, __fmaf_rn(-vt, bx, __fmul_rn(ut, by))), wt),
+                 denom);
+  dx = __fmul_rn(up, P.hdt[0]);
+  dy = __fmul_rn(vp, P.hdt[1]);
+  dz = __fmul_rn(wp, P.hdt[2]);
 }
 
 // Field at (cell g, fraction f): from the staged tile at node n0 when the
@@ -350,9 +362,9 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
   for (int it = 1; it < P.niter; ++it) {
     int gx, gy, gz;
     float fx, fy, fz;
-    locate(ox + dx, cx, gx, fx);
-    locate(oy + dy, cy, gy, fy);
-    locate(oz + dz, cz, gz, fz);
+    locate(__fadd_rn(ox, dx), cx, gx, fx);
+    locate(__fadd_rn(oy, dy), cy, gy, fy);
+    locate(__fadd_rn(oz, dz), cz, gz, fz);
     if (__any_sync(0xffffffffu, (gx | gy | gz) < 0)) {   // some lane is below the domain
       truncate_below(gx, fx);
       truncate_below(gy, fy);
@@ -363,12 +375,12 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
     const Field6 F = field_at<TX, TY, TZ>(P, sF, n0, inbox, gx, gy, gz, fx, fy, fz);
     boris(P, F, qomdt2, u, v, w, up, vp, wp, dx, dy, dz);
   }
-  u = 2.0f * up - u;
-  v = 2.0f * vp - v;
-  w = 2.0f * wp - w;
-  advance(cx, ox, up * P.fdt[0]);
-  advance(cy, oy, vp * P.fdt[1]);
-  advance(cz, oz, wp * P.fdt[2]);
+  u = __fmaf_rn(2.0f, up, -u);
+  v = __fmaf_rn(2.0f, vp, -v);
+  w = __fmaf_rn(2.0f, wp, -w);
+  advance(cx, ox, __fmul_rn(up, P.fdt[0]));
+  advance(cy, oy, __fmul_rn(vp, P.fdt[1]));
+  advance(cz, oz, __fmul_rn(wp, P.fdt[2]));
   // the particle BC, the range flag and the clamps change nothing for a
   // particle whose new cell is inside the domain: skipped unless some lane
   // needs them
@@ -849,6 +861,67 @@ __device__ __noinline__ void deposit_global(const CycleParams &P, const SpeciesD
   }
 }
 
+// The deterministic deposit. Every one of a particle's 80 terms W_node x mf
+// (W = q x the trilinear weight in FP32, mf = 1, u, v, w, uu, uv, uw, vv, vw,
+// ww in FP32) is formed exactly in FP64 (a product of two floats) and rounded
+// down to a multiple of the species' quantum Q, a power of two: a fused
+// multiply-add rounding toward -infinity into an accumulator that holds
+// M + S with M = 1.5 x 2^52 x Q, whose unit in the last place is exactly Q
+// while |S| < 2^51 Q. Every partial sum is then a multiple of Q below 2^53 Q,
+// so every later FP64 addition (across lanes, cells, tiles and the global
+// atomics) is exact and the moments do not depend on the order of the
+// particles in their buckets or of the atomics. Q = 2^(ceil(log2 T) - 38)
+// with T = max|q| x max(1, 16 max(u^2, v^2, w^2)) over the loaded species:
+// 2^-38 T resolution, 2^13 T headroom per cell and 2^15 T per node. The
+// moments are the sums times invVOL, applied once at the end.
+__device__ __forceinline__ double exact_offset(double quantum) {
+  return 6755399441055744.0 * quantum;   // 1.5 * 2^52 * Q
+}
+
+// The 8 node weights (q folded in; node = a*4 + b*2 + c, a/b/c = 1 the upper
+// node on x/y/z) and the 10 moment factors of one record, in FP32 with every
+// operation spelled out (both exact deposit paths must form them alike).
+__device__ __forceinline__ void exact_terms(float4 a, float4 b, float (&W)[8], float (&mf)[10]) {
+  const float q = a.w, ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
+  const float wx[2] = {__fmul_rn(q, __fsub_rn(1.0f, ox)), __fmul_rn(q, ox)};
+  const float wy[2] = {__fsub_rn(1.0f, oy), oy}, wz[2] = {__fsub_rn(1.0f, oz), oz};
+#pragma unroll
+  for (int n = 0; n < 8; ++n)
+    W[n] = __fmul_rn(__fmul_rn(wx[n >> 2], wy[(n >> 1) & 1]), wz[n & 1]);
+  mf[0] = 1.0f;
+  mf[1] = u;
+  mf[2] = v;
+  mf[3] = w;
+  mf[4] = __fmul_rn(u, u);
+  mf[5] = __fmul_rn(u, v);
+  mf[6] = __fmul_rn(u, w);
+  mf[7] = __fmul_rn(v, v);
+  mf[8] = __fmul_rn(v, w);
+  mf[9] = __fmul_rn(w, w);
+}
+
+// One overflow entry of the deterministic deposit: its 80 terms rounded down
+// to the species' grid, added with FP64 atomics (exact).
+__device__ __noinline__ void deposit_global_exact(const CycleParams &P, const SpeciesDev &S,
+                                                  int cx, int cy, int cz, float4 a, float4 b) {
+  const long nodes = (long)P.nxn * P.nyn * P.nzn;
+  const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
+  const long n0 = (long)(cx + 1) * sx + (long)(cy + 1) * sy + (cz + 1);
+  const double M = exact_offset(S.quantum);
+  float W[8], mf[10];
+  exact_terms(a, b, W, mf);
+#pragma unroll 1
+  for (int node = 0; node < 8; ++node) {
+    const long n = n0 + (node >> 2) * sx + ((node >> 1) & 1) * sy + (node & 1);
+    const double Wd = (double)W[node];
+#pragma unroll
+    for (int m = 0; m < 10; ++m) {
+      const double t = __fma_rd(Wd, (double)mf[m], M) - M;
+      if (t != 0.0) atomicAdd(S.mom + m * nodes + n, t);
+    }
+  }
+}
+
 // Threads of a deposit CTA: one per cell of the tile, in whole warps.
 template <int TX, int TY, int TZ>
 __host__ __device__ constexpr int dep_tpb() {
@@ -1000,6 +1073,89 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
   }
 }
 
+// The deterministic deposit of one tile (see exact_terms): thread t walks
+// cell t's whole bucket (no quota: a clumped cell keeps its thread longer),
+// rounding every term down to the species' grid into 80 FP64 accumulators;
+// the cells' exact sums go to shared memory and each node of the tile adds
+// its (up to 8) cells' sums and issues one FP64 atomic per moment, all exact.
+// The moments stay unscaled until k_scale_moments. All threads call.
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ void deposit_tile_exact(const CycleParams &P, int tile, double *sCell,
+                                                   int &inexact) {
+  using T = Tile<TX, TY, TZ>;
+  constexpr int NX = TX + 1, NY = TY + 1, NZ = TZ + 1, NB = NX * NY * NZ;
+  constexpr int TC = T::TC, NT = dep_tpb<TX, TY, TZ>();
+  const int tid = threadIdx.x;
+  const bool own = tid < TC;
+  const long nodes = (long)P.nxn * P.nyn * P.nzn;
+  const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
+  const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
+  for (int s = 0; s < P.ns; ++s) {
+    const SpeciesDev &S = P.sp[s];
+    const double M = exact_offset(S.quantum);
+    const float4 *rec = S.rout;
+    int cnt = 0;
+    if (own) {
+      const int key = tile * TC + tid;
+      const long long b0 = S.base[key];
+      cnt = (int)min((long long)S.cout[key], S.base[key + 1] - b0);
+      rec += 2 * b0;
+    }
+    double acc[80];
+#pragma unroll
+    for (int i = 0; i < 80; ++i) acc[i] = M;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, a1 = a, b1 = a;
+    if (cnt > 0) ld_rec(rec, a, b);
+    if (cnt > 1) ld_rec(rec + 2, a1, b1);
+#pragma unroll 1
+    for (int k = 0; k < cnt; ++k) {
+      float4 na = a1, nb = b1;
+      if (k + 2 < cnt) ld_rec(rec + 2 * (k + 2), na, nb);
+      float W[8], mf[10];
+      exact_terms(a, b, W, mf);
+#pragma unroll
+      for (int node = 0; node < 8; ++node) {
+        const double Wd = (double)W[node];
+#pragma unroll
+        for (int m = 0; m < 10; ++m) acc[node * 10 + m] = __fma_rd(Wd, (double)mf[m], acc[node * 10 + m]);
+      }
+      a = a1;
+      b = b1;
+      a1 = na;
+      b1 = nb;
+    }
+    if (own) {
+      const double lo = 4503599627370496.0 * S.quantum, hi = 2.0 * lo;   // 2^52 Q, 2^53 Q
+#pragma unroll
+      for (int i = 0; i < 80; ++i) {
+        inexact |= (acc[i] < lo) | (acc[i] >= hi);
+        sCell[i * TC + tid] = acc[i] - M;
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < 10 * NB; idx += NT) {
+      const int m = idx / NB, nb = idx % NB;
+      const int bz = nb % NZ, by = (nb / NZ) % NY, bx = nb / (NZ * NY);
+      double sum = 0.0;
+#pragma unroll
+      for (int a2 = 0; a2 < 2; ++a2)
+#pragma unroll
+        for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+          for (int c2 = 0; c2 < 2; ++c2) {
+            const int lx = bx - a2, ly = by - b2, lz = bz - c2;
+            if (lx >= 0 && lx < TX && ly >= 0 && ly < TY && lz >= 0 && lz < TZ)
+              sum += sCell[((a2 * 4 + b2 * 2 + c2) * 10 + m) * TC + (lx * TY + ly) * TZ + lz];
+          }
+      if (sum != 0.0) {
+        const long g = ((long)(c0x + bx + 1) * P.nyn + (c0y + by + 1)) * P.nzn + (c0z + bz + 1);
+        atomicAdd(S.mom + m * nodes + g, sum);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Overflow entries of every species of job P. Each warp takes 32 consecutive
 // entries; the push appends the particles of one slot that overflow the same
 // full bucket next to each other, so most entries of a warp share their cell.
@@ -1007,7 +1163,7 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
 // warp in FP32 (warp_sum80) and added with one FP64 atomic per node and
 // moment; the remaining entries deposit one by one (deposit_global). Called
 // by whole warps.
-template <int TX, int TY, int TZ>
+template <int TX, int TY, int TZ, bool EXACT>
 __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
   const int lane = threadIdx.x & 31;
   const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
@@ -1031,6 +1187,14 @@ __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
         key = S.okout[i];
         a = S.oout[2 * i];
         b = S.oout[2 * i + 1];
+      }
+      if constexpr (EXACT) {   // every entry on its own, exactly
+        if (valid) {
+          int cx, cy, cz;
+          key_cell<TX, TY, TZ>(key, P.nty, P.ntz, cx, cy, cz);
+          deposit_global_exact(P, S, cx, cy, cz, a, b);
+        }
+        continue;
       }
       unsigned remaining = __ballot_sync(FULL, valid);
       int groups = 0;
@@ -1071,15 +1235,28 @@ __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
 // buckets the push wrote: persistent CTAs walk the tiles, one thread per cell
 // (deposit_tile); then the overflow entries (deposit_overflow).
 // MULTI as for k_push.
-template <int TX, int TY, int TZ, bool MULTI>
-__global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(), 512 / dep_tpb<TX, TY, TZ>())
+template <int TX, int TY, int TZ, bool MULTI, bool EXACT>
+__global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(),
+                                  EXACT ? (256 / dep_tpb<TX, TY, TZ>() > 0
+                                               ? 256 / dep_tpb<TX, TY, TZ>() : 1)
+                                        : 512 / dep_tpb<TX, TY, TZ>())
     k_deposit(const __grid_constant__ CycleParams P1, const __grid_constant__ JobTable J) {
   using T = Tile<TX, TY, TZ>;
+  static_assert(!(MULTI && EXACT), "the deterministic deposit runs one simulation");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  float *sCell = reinterpret_cast<float *>(smem_raw);                       // 80 x TC
-  CycleParams *sP = reinterpret_cast<CycleParams *>(sCell + T::TC * 80);   // MULTI
+  float *sCell = reinterpret_cast<float *>(smem_raw);   // 80 x TC (float, or double if EXACT)
+  CycleParams *sP =
+      reinterpret_cast<CycleParams *>(smem_raw + (size_t)T::TC * 80 * (EXACT ? 8 : 4));   // MULTI
   const int ntiles = MULTI ? J.total_tiles : P1.ntx * P1.nty * P1.ntz;
   int cur_job = -1;
+  if constexpr (EXACT) {
+    int inexact = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+      deposit_tile_exact<TX, TY, TZ>(P1, tile, reinterpret_cast<double *>(smem_raw), inexact);
+    if (inexact) atomicOr(P1.err, ERRBIT_INEXACT);
+    deposit_overflow<TX, TY, TZ, true>(P1);
+    return;
+  }
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     if constexpr (MULTI) {
       const int job = job_of(J, tile);
@@ -1097,16 +1274,44 @@ __global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(), 512 / dep_tpb<TX, TY, T
     for (int job = 0; job < J.njobs; ++job) {
       __syncthreads();   // every thread is done with the staged parameters
       load_params(sP, J.params + job);
-      deposit_overflow<TX, TY, TZ>(*sP);
+      deposit_overflow<TX, TY, TZ, false>(*sP);
     }
   } else {
-    deposit_overflow<TX, TY, TZ>(P1);
+    deposit_overflow<TX, TY, TZ, false>(P1);
   }
 }
 
 // Zeroes every job's write-side fill counters and overflow counter and its
 // moments before a multi-job cycle (one launch instead of three memsets per
 // job and species).
+// The deterministic deposit's moments are unscaled sums: times invVOL, once.
+__global__ void k_scale_moments(const __grid_constant__ CycleParams P) {
+  const long n = 10L * P.nxn * P.nyn * P.nzn;
+  for (int s = 0; s < P.ns; ++s)
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+      P.sp[s].mom[i] *= P.scale;
+}
+
+// Largest |q| and largest velocity component of a species being loaded, as
+// the bit patterns of non-negative floats (ordered like the values).
+__global__ void k_species_bounds(const float *__restrict__ q, const float *__restrict__ u,
+                                 const float *__restrict__ v, const float *__restrict__ w, long n,
+                                 unsigned *out) {
+  float mq = 0.0f, mv = 0.0f;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    mq = fmaxf(mq, fabsf(q[i]));
+    mv = fmaxf(mv, fmaxf(fabsf(u[i]), fmaxf(fabsf(v[i]), fabsf(w[i]))));
+  }
+  const unsigned bq = __reduce_max_sync(0xffffffffu, __float_as_uint(mq));
+  const unsigned bv = __reduce_max_sync(0xffffffffu, __float_as_uint(mv));
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, bq);
+    atomicMax(out + 1, bv);
+  }
+}
+
 __global__ void k_zero_jobs(const __grid_constant__ JobTable J) {
   const long stride = (long)gridDim.x * blockDim.x;
   const long t0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -1534,8 +1739,9 @@ size_t push_smem(bool multi = false) {
          (2 + 2 * SIM_NW) * sizeof(uint64_t);
 }
 template <int TX, int TY, int TZ>
-size_t deposit_smem(bool multi = false) {
-  return (size_t)Tile<TX, TY, TZ>::TC * 80 * sizeof(float) + (multi ? sizeof(CycleParams) : 0);
+size_t deposit_smem(bool multi = false, bool exact = false) {
+  return (size_t)Tile<TX, TY, TZ>::TC * 80 * (exact ? sizeof(double) : sizeof(float)) +
+         (multi ? sizeof(CycleParams) : 0);
 }
 
 }  // namespace
@@ -1581,6 +1787,7 @@ CycleParams make_params(spb_sim *s) {
     D.mom = q.mom;
     D.ocap = q.ocap;
     D.qomdt2 = (float)(q.qom * (0.5 * s->d.dt) / s->d.c);
+    D.quantum = q.quantum;
   }
   return P;
 }
@@ -1597,41 +1804,56 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
     SPB_CUDA(cudaMemsetAsync(q.cnt[1 - q.cur], 0, s->ncells * sizeof(int), st));
     SPB_CUDA(cudaMemsetAsync(q.ocnt + (1 - q.cur), 0, sizeof(int), st));
   }
-  const size_t psm = push_smem<TX, TY, TZ, MINB>(), dsm = deposit_smem<TX, TY, TZ>();
+  const bool exact = s->d.deterministic != 0;
+  const size_t psm = push_smem<TX, TY, TZ, MINB>(), dsm = deposit_smem<TX, TY, TZ>(false, exact);
+  auto *const kdep = exact ? k_deposit<TX, TY, TZ, false, true> : k_deposit<TX, TY, TZ, false, false>;
   static bool attr = false;
   if (!attr) {
     SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, false, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)deposit_smem<TX, TY, TZ>(false, false)));
+    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, false, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)deposit_smem<TX, TY, TZ>(false, true)));
     attr = true;
   }
   const CycleParams P = make_params(s);
   const int ntiles = s->nt[0] * s->nt[1] * s->nt[2];
-  static int pocc = 0, docc = 0;   // resident CTAs per SM
+  static int pocc = 0, docc[2] = {0, 0};   // resident CTAs per SM
   if (!pocc) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, false>,
-                                                      SIM_TPB,
-                                                      psm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, false>,
-                                                      dep_tpb<TX, TY, TZ>(),
-                                                      dsm) != cudaSuccess) {
+                                                      SIM_TPB, psm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &docc[0], k_deposit<TX, TY, TZ, false, false>, dep_tpb<TX, TY, TZ>(),
+            deposit_smem<TX, TY, TZ>(false, false)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &docc[1], k_deposit<TX, TY, TZ, false, true>, dep_tpb<TX, TY, TZ>(),
+            deposit_smem<TX, TY, TZ>(false, true)) != cudaSuccess) {
       cudaGetLastError();
       pocc = MINB;
-      docc = 1;
+      docc[0] = docc[1] = 1;
     }
     pocc = std::max(pocc, 1);
-    docc = std::max(docc, 1);
+    docc[0] = std::max(docc[0], 1);
+    docc[1] = std::max(docc[1], 1);
   }
   const int pctas = std::min(ntiles, s->d.ctas > 0 ? s->d.ctas : pocc * num_sms());
-  const int dctas = std::min(ntiles, docc * num_sms());
+  const int dctas = std::min(ntiles, docc[exact ? 1 : 0] * num_sms());
   EvCycle ev{record_event(s, st), nullptr, nullptr};
   k_push<TX, TY, TZ, MINB, false><<<pctas, SIM_TPB, psm, st>>>(s->fmap, P, JobTable{},
                                                                NoMaps{});
   SPB_CUDA(cudaGetLastError());
   ev.m = record_event(s, st);
-  k_deposit<TX, TY, TZ, false><<<dctas, dep_tpb<TX, TY, TZ>(), dsm, st>>>(P, JobTable{});
+  kdep<<<dctas, dep_tpb<TX, TY, TZ>(), dsm, st>>>(P, JobTable{});
   SPB_CUDA(cudaGetLastError());
+  if (exact) {
+    k_scale_moments<<<2 * num_sms(), 256, 0, st>>>(P);
+    SPB_CUDA(cudaGetLastError());
+    g_launches++;
+    s->launches++;
+  }
   ev.e = record_event(s, st);
   if (ev.b && ev.m && ev.e) s->ev_cycle.push_back(ev);
   g_launches += 2;
@@ -1792,6 +2014,26 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
   q.total = total;
   q.n = n;
   q.cur = 0;
+  // the deterministic deposit's grid: Q = 2^(ceil(log2 T) - 38) with
+  // T = max|q| x max(1, 16 vmax^2) (see exact_terms)
+  q.quantum = 1.0;
+  if (n > 0 && s->d.deterministic) {
+    unsigned *bounds = reinterpret_cast<unsigned *>(s->scan_tmp);   // free until the next scan
+    unsigned h[2] = {0, 0};
+    SPB_CUDA(cudaMemsetAsync(bounds, 0, 2 * sizeof(unsigned), st));
+    k_species_bounds<<<blocks_for(n, 256), 256, 0, st>>>(src[6], src[3], src[4], src[5], n,
+                                                         bounds);
+    SPB_CUDA(cudaGetLastError());
+    SPB_CUDA(cudaMemcpyAsync(h, bounds, sizeof(h), cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+    g_launches++;
+    s->launches++;
+    float qmax, vmax;
+    std::memcpy(&qmax, &h[0], sizeof(float));
+    std::memcpy(&vmax, &h[1], sizeof(float));
+    const double T = std::max((double)qmax, 1e-300) * std::max(1.0, 16.0 * (double)vmax * vmax);
+    q.quantum = std::ldexp(1.0, (int)std::ceil(std::log2(T)) - 38);
+  }
   return SPB_OK;
 }
 
@@ -1892,11 +2134,11 @@ int launch_jobs_t(spb_sim *const *sims, int n, JobBuffers &B, cudaStream_t st) {
   if (!pocc) {
     SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, true>,
+    SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, true, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, true>,
                                                       SIM_TPB, psm) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, true>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&docc, k_deposit<TX, TY, TZ, true, false>,
                                                       dep_tpb<TX, TY, TZ>(), dsm) != cudaSuccess) {
       cudaGetLastError();
       pocc = MINB;
@@ -1930,7 +2172,7 @@ int launch_jobs_t(spb_sim *const *sims, int n, JobBuffers &B, cudaStream_t st) {
   k_push<TX, TY, TZ, MINB, true><<<pctas, SIM_TPB, psm, st>>>(CUtensorMap{}, CycleParams{}, J,
                                                               maps);
   SPB_CUDA(cudaGetLastError());
-  k_deposit<TX, TY, TZ, true><<<dctas, dep_tpb<TX, TY, TZ>(), dsm, st>>>(CycleParams{}, J);
+  k_deposit<TX, TY, TZ, true, false><<<dctas, dep_tpb<TX, TY, TZ>(), dsm, st>>>(CycleParams{}, J);
   SPB_CUDA(cudaGetLastError());
   g_launches += 3;
   for (int j = 0; j < n; ++j) {
@@ -2482,6 +2724,10 @@ extern "C" int spb_sim_check(spb_sim *s, void *stream) {
     SPB_CUDA(cudaMemset(s->d_err, 0, sizeof(int)));
     if (h & ERRBIT_TIMEOUT) return fail(SPB_ERR_TIMEOUT, "a staged field tile never arrived (bounded wait)");
     if (h & ERRBIT_SMEM_ALIGN) return fail(SPB_ERR_UNSUPPORTED, "shared memory not 128-byte aligned for TMA");
+    if (h & ERRBIT_INEXACT)
+      return fail(SPB_ERR_CAPACITY,
+                  "a deterministic deposit sum left its exact range (the moments are accurate "
+                  "but not guaranteed bitwise reproducible)");
     if (h & ERRBIT_LOST)
       return fail(SPB_ERR_CAPACITY, "a cell's bucket and the overflow list were both full: particles lost");
     return fail(SPB_ERR_OUT_OF_GRID, "a particle left the node array and was clamped");

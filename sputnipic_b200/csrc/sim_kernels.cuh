@@ -51,6 +51,8 @@ struct SpeciesDev {
   double *mom;         // [10][nodes]
   int ocap;
   float qomdt2;        // qom * (dt/2) / c
+  double quantum;      // deterministic deposit: the grid every term is
+                       // rounded down to (a power of two; see deposit_tile_exact)
 };
 
 struct CycleParams {

@@ -24,7 +24,7 @@ def _stream(stream):
 
 class Simulation:
     def __init__(self, wl, tile=(8, 4, 4), resort_every=4, ctas=0, species=None, variant=0,
-                 bucket_slots=0, graph=False):
+                 bucket_slots=0, graph=False, deterministic=False):
         self.lib = _lib.load()
         self.wl = wl
         species = list(range(len(wl.species))) if species is None else list(species)
@@ -42,6 +42,7 @@ class Simulation:
         d.resort_every, d.ctas, d.variant = resort_every, ctas, variant
         d.bucket_slots = bucket_slots
         d.graph = 1 if graph else 0
+        d.deterministic = 1 if deterministic else 0
         h = ctypes.c_void_p()
         _lib.check(self.lib.spb_sim_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h

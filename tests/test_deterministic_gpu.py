@@ -1,0 +1,96 @@
+"""The precision form's deterministic mode (spb_sim_desc.deterministic).
+
+Particles reach their buckets through atomics, so their order inside a
+bucket, the overflow lists and the FP64 atomics differ from run to run. In the
+deterministic mode every deposit term is rounded down to a power-of-two grid
+and summed exactly, and a particle's push is the same whichever path serves it
+(staged tile or L2, bucket or overflow list), so:
+  - two runs from the same inputs give bitwise identical moments and the same
+    particles (compared as sorted multisets), over many cycles with CUDA
+    graphs, forced overflows and re-layouts;
+  - the moments still match the FP64 oracle (relative L2 <= 1e-5 per moment,
+    the precision form's bar) and the default mode's moments (1e-6).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from sputnipic_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+
+def run(torch, wl, fields, cycles, deterministic, bucket_slots=0, resort_every=2, graph=True):
+    from sputnipic_b200.device import gen_particles
+    from sputnipic_b200.sim import Simulation
+    sim = Simulation(wl, resort_every=resort_every, graph=graph, deterministic=deterministic,
+                     bucket_slots=bucket_slots)
+    sim.set_fields(fields)
+    for s in range(len(wl.species)):
+        sim.load_species(s, gen_particles(wl, s))
+    sim.cycle(cycles)
+    assert sim.check() == 0
+    mom = [sim.moments(s).cpu().numpy() for s in range(len(wl.species))]
+    parts = []
+    for s in range(len(wl.species)):
+        p = sim.particles(s)
+        a = np.stack([p[k].cpu().numpy().view(np.uint32) for k in "xyzuvwq"], axis=1)
+        parts.append(a[np.lexsort(a.T[::-1])])
+    overflow = [sim.overflow(s) for s in range(len(wl.species))]
+    sim.close()
+    return mom, parts, overflow
+
+
+@pytest.mark.parametrize("bucket_slots", [0, 96])
+def test_two_runs_bitwise_identical(cuda, bucket_slots):
+    """Uneven species (125, 125, 12.5, 12.5 ppc) on a 64x32x32 GEM grid, 12
+    cycles with graphs and overflow checks every 2 cycles; bucket_slots=96
+    fixes every bucket below the 125-particle mean, so many particles go
+    through the overflow lists (pushed from L2, deposited entry by entry)."""
+    torch = cuda
+    from sputnipic_b200.device import gen_fields
+    wl = W.batching_gem(nxc=64, nyc=32, nzc=32, Lx=10.0, Ly=5.0, Lz=5.0)
+    fields = gen_fields(wl)
+    m1, p1, o1 = run(torch, wl, fields, 12, True, bucket_slots)
+    m2, p2, o2 = run(torch, wl, fields, 12, True, bucket_slots)
+    if bucket_slots:
+        assert min(o1) > 0 and min(o2) > 0          # the overflow paths were used
+    for s in range(len(wl.species)):
+        assert np.array_equal(m1[s].view(np.uint64), m2[s].view(np.uint64)), s
+        assert np.array_equal(p1[s], p2[s]), s
+        assert np.abs(m1[s]).max() > 0
+
+
+def test_deterministic_moments_match_oracle_and_default(cuda):
+    """One cycle of the small GEM configuration: the deterministic moments
+    against the FP64 oracle and against the default deposit."""
+    torch = cuda
+    from sputnipic_b200.sim import Simulation
+    wl = W.small_gem(E_amp=1e-3)
+    fields = W.gem_fields(wl)
+    parts = [W.gem_particles(wl, s) for s in range(4)]
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    got = {}
+    for det in (False, True):
+        sim = Simulation(wl, resort_every=10**6, deterministic=det)
+        sim.set_fields([T(f) for f in fields])
+        for s, p in enumerate(parts):
+            sim.load_species(s, {k: T(p[k]) for k in "xyzuvwq"})
+        sim.cycle(1)
+        assert sim.check() == 0
+        got[det] = [sim.moments(s).cpu().numpy() for s in range(4)]
+        sim.close()
+    orc64 = oracle.CpuOracle("restated", 64)
+    setup = oracle.setup_from(wl)
+    F64 = [f.astype(np.float64) for f in fields]
+    for s in range(4):
+        p = {k: parts[s][k].astype(np.float64) for k in "xyzuvwq"}
+        orc64.mover_pc(setup, F64, p, wl.species[s].qom)
+        mom = [np.zeros(wl.nodes) for _ in range(10)]
+        orc64.interp_p2g(setup, p, mom)
+        ref = np.stack(mom)
+        for det, bar in ((True, 1e-5), (False, 1e-5)):
+            err = np.linalg.norm(got[det][s] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+            assert (err <= bar).all(), (s, det, err)
+        diff = np.linalg.norm(got[True][s] - got[False][s], axis=1) / np.linalg.norm(ref, axis=1)
+        assert (diff <= 1e-6).all(), (s, diff)

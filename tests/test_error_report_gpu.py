@@ -117,3 +117,79 @@ def test_error_report_small_gem(cuda):
         assert plain["moments"][name]["rel_l2"] <= 2e-4, name
     for k in "xyz":
         assert prec["particles"][k]["max_abs"] <= 1e-5, k
+
+
+@pytest.mark.parametrize("preset", ["gem", "dense"])
+def test_error_report_full_size_slab(cuda, preset):
+    """The precision form at the full sizes of the GEM (4 x 65.5M particles,
+    128x64x64) and dense (4 x 134M, 256x128x128) workloads, one cycle,
+    against the FP64 oracle on the first SLABS x-slabs of cells:
+      - moments: the full run's moments on the node planes x = 3..SLABS-1,
+        which in one cycle only the slabs' particles reach, against the FP64
+        oracle's deposit of the slabs' particles;
+      - particles: the slabs' particles loaded alone (each with a unique
+        charge as its tag, so that the bucket order can be undone) and
+        pushed one cycle, against the FP64 oracle's push of the same
+        particles.
+    `pytest -s` prints the table (same keys as the small-GEM report). Bars:
+    relative L2 <= 1e-5 per moment, positions <= 1e-5 absolute (domain
+    units), velocities <= 1e-5 relative to the largest."""
+    torch = cuda
+    from sputnipic_b200.device import gen_fields, gen_particles
+    from sputnipic_b200.sim import Simulation
+    SLABS = 6
+    wl = W.PRESETS[preset]()
+    ns = len(wl.species)
+    orc64 = oracle.CpuOracle("restated", 64)
+    setup = oracle.setup_from(wl)
+    fields = gen_fields(wl)
+    F64 = [f.cpu().numpy().astype(np.float64) for f in fields]
+    plane = wl.nyc * wl.nzc
+    sim = Simulation(wl, resort_every=10**6)
+    sim.set_fields(fields)
+    slab = []
+    for s in range(ns):
+        p = gen_particles(wl, s, with_cell=True)
+        sel = (p["cell"] // plane) < SLABS
+        slab.append({k: p[k][sel].contiguous() for k in "xyzuvwq"})
+        sim.load_species(s, {k: p[k] for k in "xyzuvwq"})
+        del p, sel
+        torch.cuda.empty_cache()
+    sim.cycle(1)
+    assert sim.check() == 0
+    keep = np.arange(wl.nodes).reshape(wl.nxn, wl.nyn, wl.nzn)[3:SLABS].ravel()
+    got_m = [sim.moments(s).cpu().numpy()[:, keep] for s in range(ns)]
+    sim.close()
+    torch.cuda.empty_cache()
+    # the slabs alone, tagged
+    tag = Simulation(wl, resort_every=10**6)
+    tag.set_fields(fields)
+    for s in range(ns):
+        d = dict(slab[s])
+        d["q"] = torch.arange(d["x"].numel(), dtype=torch.float32, device="cuda")
+        tag.load_species(s, d)
+    tag.cycle(1)
+    assert tag.check() == 0
+    ref_m, ref_p, got_p = [], [], []
+    for s in range(ns):
+        p = {k: slab[s][k].cpu().numpy().astype(np.float64) for k in "xyzuvwq"}
+        orc64.mover_pc(setup, F64, p, wl.species[s].qom)
+        mom = [np.zeros(wl.nodes) for _ in range(10)]
+        orc64.interp_p2g(setup, p, mom)
+        ref_m.append(np.stack(mom)[:, keep])
+        ref_p.append(p)
+        g = {k: v.cpu().numpy() for k, v in tag.particles(s).items()}
+        order = np.argsort(g["q"])
+        assert np.array_equal(g["q"][order], np.arange(len(order), dtype=np.float32))
+        got_p.append({k: g[k][order] for k in "xyzuvw"})
+    tag.close()
+    torch.cuda.empty_cache()
+    rep = {"moments": moment_errors(got_m, ref_m), "particles": particle_errors(got_p, ref_p)}
+    n_slab = sum(len(p["x"]) for p in ref_p)
+    print(json.dumps({"config": f"{wl.name}, {ns} species x {wl.species_count(0):,} particles, "
+                                f"1 cycle; first {SLABS} x-slabs ({n_slab:,} particles), node "
+                                f"planes 3..{SLABS - 1}", "precision": rep}))
+    for name in MOMENTS:
+        assert rep["moments"][name]["rel_l2"] <= 1e-5, name
+    for k in "xyzuvw":
+        assert rep["particles"][k]["max_abs"] <= 1e-5, k
