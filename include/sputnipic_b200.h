@@ -298,8 +298,10 @@ typedef struct spb_sim_desc {
                                buffer-parity pattern; not while timing */
   int deterministic;        /* 1: bitwise reproducible moments. Every deposit
                                term is rounded down to a power-of-two grid
-                               (2^-38 of the species' largest |q| x
-                               max(1, 16 |v|max^2) at load) and summed exactly
+                               (2^-38 of the species' largest possible term of
+                               that moment at load: |q|max for rhon, |q|max x
+                               4 |v|max for J, |q|max x 16 |v|max^2 for the
+                               pressures) and summed exactly
                                in FP64, so the moments do not depend on the
                                particles' order in their buckets or on the
                                order of the atomics; the push gives every
@@ -405,6 +407,15 @@ typedef struct spb_serve_desc {
   long long reserve_bytes;  /* device memory the library's pool maps up front
                                (0: none), so that admitting jobs maps nothing;
                                spb_release_cached_memory gives it back */
+  double extra_budget;      /* after a step's launch of every admitted job,
+                               further launches give jobs with cycles left
+                               more cycles, the cheapest jobs first (cost of a
+                               cycle: particles + 4 x cells), while the added
+                               cost stays within this fraction of the first
+                               launch's (at most 7 further launches): small
+                               jobs then finish in a few steps instead of being
+                               paced by the largest. 0: 1.0; negative: one
+                               cycle per job and step */
 } spb_serve_desc;
 
 typedef struct spb_job_desc {
@@ -428,9 +439,11 @@ void spb_serve_destroy(spb_serve *srv);
  * queue (status not PENDING). Returns the job id (>= 0) or -status. */
 long spb_serve_submit(spb_serve *srv, const spb_job_desc *job, const float *const fields[6],
                       const float *const *parts, const long *counts, int on_device);
-/* Admits the queued jobs that fit (in order of arrival), runs one cycle of
- * every admitted job, retires the jobs that reached their cycle count, and
- * synchronises. Returns the number of jobs still admitted, or -status. */
+/* Runs one cycle of every admitted job (and more for the cheap ones, see
+ * extra_budget) while admitting the queued jobs that fit (in order of
+ * arrival; they upload on a stream of their own and join the next step),
+ * retires the jobs that reached their cycle count, and synchronises.
+ * Returns the number of jobs admitted, or -status. */
 int spb_serve_step(spb_serve *srv);
 /* SPB_JOB_*, or -1 for an unknown id. */
 int spb_serve_status(const spb_serve *srv, long id);

@@ -164,7 +164,8 @@ class HatDesc(ctypes.Structure):
 class ServeDesc(ctypes.Structure):
     """spb_serve_desc of include/sputnipic_b200.h."""
     _fields_ = [("tile", c_int * 3), ("hbm_budget", ctypes.c_longlong), ("max_jobs", c_int),
-                ("check_every", c_int), ("reserve_bytes", ctypes.c_longlong)]
+                ("check_every", c_int), ("reserve_bytes", ctypes.c_longlong),
+                ("extra_budget", c_double)]
 
 
 class JobDesc(ctypes.Structure):

@@ -2,12 +2,18 @@
 // particle jobs, each a precision-form simulation of its own grid, admitted by
 // free HBM and stepped together in one launch per kernel (spb::launch_jobs).
 //
-// Scheduling. Jobs queue in order of arrival. A step first admits queued jobs
-// while the next one's estimated footprint fits the budget and the launch has
-// room (first come, first served: a large job at the head waits rather than
-// being overtaken), then runs one cycle of every admitted job, then retires
-// the jobs that reached their cycle count. A job that can never fit (larger
-// than the whole budget) fails with SPB_ERR_CAPACITY instead of blocking.
+// Scheduling. Jobs queue in order of arrival. A step launches one cycle of
+// every admitted job, then further launches for the jobs with cycles left,
+// cheapest first, within a cost budget relative to the first launch (so a
+// small job is not paced by the largest one), all asynchronous; meanwhile it
+// admits queued jobs while the next one's estimated footprint fits the budget
+// and the launch has room (first come, first served: a large job at the head
+// waits rather than being overtaken), uploading them on a stream of their own
+// so that the upload overlaps the launches; it then waits for both and
+// retires the jobs that reached their cycle count. A job that can never fit
+// (larger than the whole budget) fails with SPB_ERR_CAPACITY instead of
+// blocking.
+#include <algorithm>
 #include <chrono>
 #include <deque>
 #include <map>
@@ -68,11 +74,15 @@ double seconds_since(Clock::time_point t0) {
 
 }  // namespace
 
+constexpr int SERVE_LAUNCHES = 8;   // launches per step at most
+
 struct spb_serve {
   spb_serve_desc d{};
   int device = 0;
-  cudaStream_t st = nullptr;
-  JobBuffers buf;
+  cudaStream_t st = nullptr;       // the jobs' cycles
+  cudaStream_t adm = nullptr;      // admissions (uploads of new jobs)
+  cudaEvent_t adm_done = nullptr;
+  JobBuffers buf[SERVE_LAUNCHES];
   long long budget = 0, used = 0;
   long next_id = 0;
   long steps = 0;
@@ -122,14 +132,21 @@ int admit(spb_serve *s, ServeJob *j) {
   for (int i = 0; i < j->d.ns; ++i) sd.qom[i] = j->d.qom[i];
   sd.resort_every = 1 << 30;   // the engine checks overflow lists itself
   if (int rc = spb_sim_create(&sd, &j->sim)) return rc;
-  if (int rc = spb_sim_set_fields(j->sim, j->fields, j->on_device, s->st)) return rc;
+  if (int rc = spb_sim_set_fields(j->sim, j->fields, j->on_device, s->adm)) return rc;
   for (int i = 0; i < j->d.ns; ++i) {
     const float *const *p = j->parts.data() + 7 * i;
     if (int rc = spb_sim_load_species(j->sim, i, p[0], p[1], p[2], p[3], p[4], p[5], p[6],
-                                      j->counts[i], j->on_device, s->st))
+                                      j->counts[i], j->on_device, s->adm))
       return rc;
   }
   return SPB_OK;
+}
+
+// Estimated cost of one cycle of a job (particles + 4 x cells).
+double cycle_cost(const ServeJob *j) {
+  double n = 0;
+  for (long c : j->counts) n += (double)c;
+  return n + 4.0 * (double)j->d.nxc * j->d.nyc * j->d.nzc;
 }
 
 }  // namespace
@@ -152,7 +169,10 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
   auto s = std::make_unique<spb_serve>();
   s->d = d;
   SPB_CUDA(cudaGetDevice(&s->device));
+  if (d.extra_budget == 0.0) d.extra_budget = 1.0;
   SPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  SPB_CUDA(cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking));
+  SPB_CUDA(cudaEventCreateWithFlags(&s->adm_done, cudaEventDisableTiming));
   SPB_CUDA(cudaMallocHost(&s->h_ovf, (size_t)SERVE_MAX_JOBS * SPB_SIM_MAX_SPECIES * sizeof(int)));
   if (d.hbm_budget > 0) {
     s->budget = d.hbm_budget;
@@ -171,8 +191,11 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
 extern "C" void spb_serve_destroy(spb_serve *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
+  if (s->adm) cudaStreamSynchronize(s->adm);
   s->jobs.clear();
   if (s->st) cudaStreamDestroy(s->st);
+  if (s->adm) cudaStreamDestroy(s->adm);
+  if (s->adm_done) cudaEventDestroy(s->adm_done);
   cudaFreeHost(s->h_ovf);
   delete s;
 }
@@ -219,30 +242,41 @@ extern "C" int spb_serve_step(spb_serve *s) {
     s->phase_s[phase] += std::chrono::duration<double>(t - tp).count();
     tp = t;
   };
-  // admit in order of arrival while the head fits
-  while (!s->pending.empty() && (int)s->active.size() < s->d.max_jobs) {
-    ServeJob *j = s->pending.front();
-    if (j->bytes > s->budget) {   // can never fit: fail it rather than block the queue
+  // admit in order of arrival while the head fits, uploading on the
+  // admission stream; the engine's stream then waits for the uploads
+  auto admit_pending = [&](std::vector<ServeJob *> &joined) -> int {
+    while (!s->pending.empty() && (int)(s->active.size() + joined.size()) < s->d.max_jobs) {
+      ServeJob *j = s->pending.front();
+      if (j->bytes > s->budget) {   // can never fit: fail it rather than block the queue
+        s->pending.pop_front();
+        fail_job(s, j, fail(SPB_ERR_CAPACITY, "job larger than the engine's HBM budget"));
+        continue;
+      }
+      if (s->used + j->bytes > s->budget) break;
       s->pending.pop_front();
-      fail_job(s, j, fail(SPB_ERR_CAPACITY, "job larger than the engine's HBM budget"));
-      continue;
+      j->state = SPB_JOB_ACTIVE;
+      s->used += j->bytes;
+      j->t[1] = seconds_since(s->t0);
+      if (int rc = admit(s, j)) {
+        fail_job(s, j, rc);
+        continue;
+      }
+      joined.push_back(j);
     }
-    if (s->used + j->bytes > s->budget) break;
-    s->pending.pop_front();
-    j->state = SPB_JOB_ACTIVE;
-    s->used += j->bytes;
-    j->t[1] = seconds_since(s->t0);
-    if (int rc = admit(s, j)) {
-      fail_job(s, j, rc);
-      continue;
-    }
-    s->active.push_back(j);
+    SPB_CUDA(cudaEventRecord(s->adm_done, s->adm));
+    SPB_CUDA(cudaStreamWaitEvent(s->st, s->adm_done, 0));
+    return SPB_OK;
+  };
+  std::vector<ServeJob *> joined;
+  const bool idle = s->active.empty();
+  if (idle) {   // nothing running: the new jobs run in this step
+    if (int rc = admit_pending(joined)) return -rc;
+    s->active.swap(joined);
+    lap(0);
   }
-  lap(0);
-  if (s->active.empty()) return 0;
   // overflow lists past their threshold: re-lay out those jobs (one
-  // synchronisation for all)
-  if (s->steps > 0 && s->steps % s->d.check_every == 0) {
+  // synchronisation for all; the engine's stream is idle between steps)
+  if (!idle && s->steps > 0 && s->steps % s->d.check_every == 0) {
     int k = 0;
     for (ServeJob *j : s->active)
       for (const SimSpecies &q : j->sim->sp)
@@ -259,17 +293,55 @@ extern "C" int spb_serve_step(spb_serve *s) {
     }
   }
   lap(1);
-  std::vector<spb_sim *> sims;
-  sims.reserve(s->active.size());
-  for (ServeJob *j : s->active) sims.push_back(j->sim);
-  if (int rc = launch_jobs(sims.data(), (int)sims.size(), s->buf, s->st)) return -rc;
+  // this step's launches (asynchronous): one cycle of every admitted job,
+  // then further cycles for the jobs with cycles left, cheapest first, while
+  // the added cost stays within extra_budget of the first launch's
+  const std::vector<ServeJob *> ran = s->active;
+  if (!ran.empty()) {
+    std::vector<spb_sim *> sims;
+    sims.reserve(ran.size());
+    double first = 0.0;
+    for (ServeJob *j : ran) {
+      sims.push_back(j->sim);
+      first += cycle_cost(j);
+      j->cycles++;
+    }
+    if (int rc = launch_jobs(sims.data(), (int)sims.size(), s->buf[0], s->st)) return -rc;
+    if (s->d.extra_budget > 0.0) {
+      std::vector<std::pair<double, ServeJob *>> cand;
+      for (ServeJob *j : ran) cand.emplace_back(cycle_cost(j), j);
+      std::stable_sort(cand.begin(), cand.end(),
+                       [](const std::pair<double, ServeJob *> &a,
+                          const std::pair<double, ServeJob *> &b) { return a.first < b.first; });
+      double budget = s->d.extra_budget * first;
+      for (int L = 1; L < SERVE_LAUNCHES && budget > 0.0; ++L) {
+        sims.clear();
+        double spent = 0.0;
+        for (auto &c : cand)
+          if (c.second->cycles < c.second->d.ncycles && spent + c.first <= budget) {
+            sims.push_back(c.second->sim);
+            spent += c.first;
+            c.second->cycles++;
+          }
+        if (sims.empty()) break;
+        if (int rc = launch_jobs(sims.data(), (int)sims.size(), s->buf[L], s->st)) return -rc;
+        budget -= spent;
+      }
+    }
+    s->steps++;
+  }
+  lap(2);
+  // while the launches run: admit what fits; those jobs join the next step
+  if (!idle) {
+    if (int rc = admit_pending(joined)) return -rc;
+    lap(0);
+  }
   SPB_CUDA(cudaStreamSynchronize(s->st));
-  s->steps++;
   lap(2);
   // retire the jobs that reached their cycle count
   std::vector<ServeJob *> still;
-  for (ServeJob *j : s->active) {
-    if (++j->cycles < j->d.ncycles) {
+  for (ServeJob *j : ran) {
+    if (j->cycles < j->d.ncycles) {
       still.push_back(j);
       continue;
     }
@@ -281,6 +353,7 @@ extern "C" int spb_serve_step(spb_serve *s) {
       j->state = SPB_JOB_DONE;
     }
   }
+  still.insert(still.end(), joined.begin(), joined.end());
   s->active.swap(still);
   lap(3);
   return (int)s->active.size();

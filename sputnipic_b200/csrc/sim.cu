@@ -864,16 +864,23 @@ __device__ __noinline__ void deposit_global(const CycleParams &P, const SpeciesD
 // The deterministic deposit. Every one of a particle's 80 terms W_node x mf
 // (W = q x the trilinear weight in FP32, mf = 1, u, v, w, uu, uv, uw, vv, vw,
 // ww in FP32) is formed exactly in FP64 (a product of two floats) and rounded
-// down to a multiple of the species' quantum Q, a power of two: a fused
+// down to a multiple of its moment's quantum Q, a power of two: a fused
 // multiply-add rounding toward -infinity into an accumulator that holds
 // M + S with M = 1.5 x 2^52 x Q, whose unit in the last place is exactly Q
 // while |S| < 2^51 Q. Every partial sum is then a multiple of Q below 2^53 Q,
 // so every later FP64 addition (across lanes, cells, tiles and the global
 // atomics) is exact and the moments do not depend on the order of the
 // particles in their buckets or of the atomics. Q = 2^(ceil(log2 T) - 38)
-// with T = max|q| x max(1, 16 max(u^2, v^2, w^2)) over the loaded species:
-// 2^-38 T resolution, 2^13 T headroom per cell and 2^15 T per node. The
-// moments are the sums times invVOL, applied once at the end.
+// with T the species' largest possible term of that moment at load: max|q|
+// for rhon, max|q| x 4 vmax for Jx..Jz, max|q| x 16 vmax^2 for pxx..pzz
+// (vmax the largest velocity component): 2^-38 T resolution (the downward
+// rounding's bias over a node's N terms, N 2^-39 T, stays far below the
+// size of a cancelling sum, ~sqrt(N) of its terms), 2^13 T headroom per cell
+// and 2^15 T per node. The moments are the sums times invVOL, applied once
+// at the end.
+__device__ __forceinline__ double exact_quantum(const SpeciesDev &S, int m) {
+  return S.quantum[m == 0 ? 0 : (m < 4 ? 1 : 2)];
+}
 __device__ __forceinline__ double exact_offset(double quantum) {
   return 6755399441055744.0 * quantum;   // 1.5 * 2^52 * Q
 }
@@ -907,7 +914,6 @@ __device__ __noinline__ void deposit_global_exact(const CycleParams &P, const Sp
   const long nodes = (long)P.nxn * P.nyn * P.nzn;
   const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
   const long n0 = (long)(cx + 1) * sx + (long)(cy + 1) * sy + (cz + 1);
-  const double M = exact_offset(S.quantum);
   float W[8], mf[10];
   exact_terms(a, b, W, mf);
 #pragma unroll 1
@@ -916,6 +922,7 @@ __device__ __noinline__ void deposit_global_exact(const CycleParams &P, const Sp
     const double Wd = (double)W[node];
 #pragma unroll
     for (int m = 0; m < 10; ++m) {
+      const double M = exact_offset(exact_quantum(S, m));
       const double t = __fma_rd(Wd, (double)mf[m], M) - M;
       if (t != 0.0) atomicAdd(S.mom + m * nodes + n, t);
     }
@@ -1092,7 +1099,8 @@ __device__ __forceinline__ void deposit_tile_exact(const CycleParams &P, int til
   const int c0x = tx * TX, c0y = ty * TY, c0z = tz * TZ;
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
-    const double M = exact_offset(S.quantum);
+    const double M[3] = {exact_offset(S.quantum[0]), exact_offset(S.quantum[1]),
+                         exact_offset(S.quantum[2])};
     const float4 *rec = S.rout;
     int cnt = 0;
     if (own) {
@@ -1103,7 +1111,7 @@ __device__ __forceinline__ void deposit_tile_exact(const CycleParams &P, int til
     }
     double acc[80];
 #pragma unroll
-    for (int i = 0; i < 80; ++i) acc[i] = M;
+    for (int i = 0; i < 80; ++i) acc[i] = M[(i % 10) == 0 ? 0 : ((i % 10) < 4 ? 1 : 2)];
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, a1 = a, b1 = a;
     if (cnt > 0) ld_rec(rec, a, b);
     if (cnt > 1) ld_rec(rec + 2, a1, b1);
@@ -1125,11 +1133,12 @@ __device__ __forceinline__ void deposit_tile_exact(const CycleParams &P, int til
       b1 = nb;
     }
     if (own) {
-      const double lo = 4503599627370496.0 * S.quantum, hi = 2.0 * lo;   // 2^52 Q, 2^53 Q
 #pragma unroll
       for (int i = 0; i < 80; ++i) {
-        inexact |= (acc[i] < lo) | (acc[i] >= hi);
-        sCell[i * TC + tid] = acc[i] - M;
+        const int k = (i % 10) == 0 ? 0 : ((i % 10) < 4 ? 1 : 2);
+        const double lo = 4503599627370496.0 * S.quantum[k];   // 2^52 Q; 2^53 Q above
+        inexact |= (acc[i] < lo) | (acc[i] >= 2.0 * lo);
+        sCell[i * TC + tid] = acc[i] - M[k];
       }
     }
     __syncthreads();
@@ -1255,35 +1264,32 @@ __global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(),
       deposit_tile_exact<TX, TY, TZ>(P1, tile, reinterpret_cast<double *>(smem_raw), inexact);
     if (inexact) atomicOr(P1.err, ERRBIT_INEXACT);
     deposit_overflow<TX, TY, TZ, true>(P1);
-    return;
-  }
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  } else {
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      if constexpr (MULTI) {
+        const int job = job_of(J, tile);
+        if (job != cur_job) {
+          __syncthreads();   // every thread is done with the staged parameters
+          load_params(sP, J.params + job);
+          cur_job = job;
+        }
+        deposit_tile<TX, TY, TZ>(*sP, tile - J.tile_base[job], sCell);
+      } else {
+        deposit_tile<TX, TY, TZ>(P1, tile, sCell);
+      }
+    }
     if constexpr (MULTI) {
-      const int job = job_of(J, tile);
-      if (job != cur_job) {
+      for (int job = 0; job < J.njobs; ++job) {
         __syncthreads();   // every thread is done with the staged parameters
         load_params(sP, J.params + job);
-        cur_job = job;
+        deposit_overflow<TX, TY, TZ, false>(*sP);
       }
-      deposit_tile<TX, TY, TZ>(*sP, tile - J.tile_base[job], sCell);
     } else {
-      deposit_tile<TX, TY, TZ>(P1, tile, sCell);
+      deposit_overflow<TX, TY, TZ, false>(P1);
     }
-  }
-  if constexpr (MULTI) {
-    for (int job = 0; job < J.njobs; ++job) {
-      __syncthreads();   // every thread is done with the staged parameters
-      load_params(sP, J.params + job);
-      deposit_overflow<TX, TY, TZ, false>(*sP);
-    }
-  } else {
-    deposit_overflow<TX, TY, TZ, false>(P1);
   }
 }
 
-// Zeroes every job's write-side fill counters and overflow counter and its
-// moments before a multi-job cycle (one launch instead of three memsets per
-// job and species).
 // The deterministic deposit's moments are unscaled sums: times invVOL, once.
 __global__ void k_scale_moments(const __grid_constant__ CycleParams P) {
   const long n = 10L * P.nxn * P.nyn * P.nzn;
@@ -1312,6 +1318,9 @@ __global__ void k_species_bounds(const float *__restrict__ q, const float *__res
   }
 }
 
+// Zeroes every job's write-side fill counters and overflow counter and its
+// moments before a multi-job cycle (one launch instead of three memsets per
+// job and species).
 __global__ void k_zero_jobs(const __grid_constant__ JobTable J) {
   const long stride = (long)gridDim.x * blockDim.x;
   const long t0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -1787,7 +1796,7 @@ CycleParams make_params(spb_sim *s) {
     D.mom = q.mom;
     D.ocap = q.ocap;
     D.qomdt2 = (float)(q.qom * (0.5 * s->d.dt) / s->d.c);
-    D.quantum = q.quantum;
+    for (int k = 0; k < 3; ++k) D.quantum[k] = q.quantum[k];
   }
   return P;
 }
@@ -2014,9 +2023,9 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
   q.total = total;
   q.n = n;
   q.cur = 0;
-  // the deterministic deposit's grid: Q = 2^(ceil(log2 T) - 38) with
-  // T = max|q| x max(1, 16 vmax^2) (see exact_terms)
-  q.quantum = 1.0;
+  // the deterministic deposit's grids: Q = 2^(ceil(log2 T) - 38) with T the
+  // largest term of rhon, Jx..Jz, pxx..pzz (see exact_terms)
+  q.quantum[0] = q.quantum[1] = q.quantum[2] = 1.0;
   if (n > 0 && s->d.deterministic) {
     unsigned *bounds = reinterpret_cast<unsigned *>(s->scan_tmp);   // free until the next scan
     unsigned h[2] = {0, 0};
@@ -2031,8 +2040,10 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
     float qmax, vmax;
     std::memcpy(&qmax, &h[0], sizeof(float));
     std::memcpy(&vmax, &h[1], sizeof(float));
-    const double T = std::max((double)qmax, 1e-300) * std::max(1.0, 16.0 * (double)vmax * vmax);
-    q.quantum = std::ldexp(1.0, (int)std::ceil(std::log2(T)) - 38);
+    const double qm = std::max((double)qmax, 1e-300), vm = std::max((double)vmax, 1e-30);
+    const double T[3] = {qm, qm * 4.0 * vm, qm * 16.0 * vm * vm};
+    for (int k = 0; k < 3; ++k)
+      q.quantum[k] = std::ldexp(1.0, (int)std::ceil(std::log2(T[k])) - 38);
   }
   return SPB_OK;
 }

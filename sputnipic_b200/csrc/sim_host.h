@@ -29,7 +29,7 @@ struct SimSpecies {
   long long total = 0;          // record slots of the layout
   int cur = 0;                  // the buffer set holding the particles
   double *mom = nullptr;        // [10][nodes]
-  double quantum = 1.0;         // deterministic deposit grid (set at load)
+  double quantum[3] = {1.0, 1.0, 1.0};   // deterministic deposit grids (set at load)
 };
 
 using EvPair = std::pair<cudaEvent_t, cudaEvent_t>;

@@ -51,8 +51,9 @@ struct SpeciesDev {
   double *mom;         // [10][nodes]
   int ocap;
   float qomdt2;        // qom * (dt/2) / c
-  double quantum;      // deterministic deposit: the grid every term is
-                       // rounded down to (a power of two; see deposit_tile_exact)
+  double quantum[3];   // deterministic deposit: the grid every term of rhon,
+                       // of Jx..Jz and of pxx..pzz is rounded down to (powers
+                       // of two; see exact_terms)
 };
 
 struct CycleParams {

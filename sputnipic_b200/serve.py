@@ -50,13 +50,14 @@ class Finished:
 
 class Server:
     def __init__(self, tile=(4, 4, 4), hbm_budget=0, max_jobs=64, check_every=4,
-                 reserve_bytes=0):
+                 reserve_bytes=0, extra_budget=0.0):
         self.lib = _lib.load()
         d = _lib.ServeDesc()
         for a in range(3):
             d.tile[a] = tile[a]
         d.hbm_budget, d.max_jobs, d.check_every = int(hbm_budget), max_jobs, check_every
         d.reserve_bytes = int(reserve_bytes)
+        d.extra_budget = float(extra_budget)
         h = ctypes.c_void_p()
         _lib.check(self.lib.spb_serve_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h
@@ -229,7 +230,51 @@ def device_jobs(configs):
     return jobs
 
 
-def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), rates=None):
+def plain_job_seconds(job) -> float:
+    """Wall seconds of one job run alone through the plain path (the
+    reference's precision types on device arrays, spb_grid_*): grid context,
+    fields, a copy of the particles, then per cycle mover_PC for every species,
+    zeroed moments and interpP2G for every species, as the reference's CPU
+    driver steps them (src/sputniPIC_CPU.cpp:232-256), synchronised at the end."""
+    import torch
+
+    from .device import GridContext, push_params
+    wl = job.wl
+    species = job.species or list(range(len(job.parts)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx = GridContext(wl)
+    ctx.set_fields(job.fields)
+    parts = [{k: p[k].clone() for k in "xyzuvwq"} for p in job.parts]
+    pushes = [push_params(wl, s) for s in species]
+    mom = torch.zeros(len(parts), 10, wl.nodes, device="cuda")
+    for _ in range(job.ncycles):
+        for p, push in zip(parts, pushes):
+            ctx.mover(p, push)
+        mom.zero_()
+        for i, p in enumerate(parts):
+            ctx.p2g(p, mom[i])
+    rc = ctx.check()
+    t = time.perf_counter() - t0
+    ctx.close()
+    if rc:
+        raise RuntimeError(f"plain job status {rc}")
+    return t
+
+
+def fifo_latencies(arrivals, service):
+    """Latencies of jobs served one at a time in order of arrival (a single
+    server, no overlap): each starts when it has arrived and the previous one
+    has finished. Returns (latencies, finish time of the last job)."""
+    t, lat = 0.0, []
+    for a, d in zip(arrivals, service):
+        t = max(t, a) + d
+        lat.append(t - a)
+    return lat, t
+
+
+def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), rates=None,
+                   extra_budget=0.0):
     """Poisson streams of `njobs` jobs drawn from a seeded mix of
     configurations, at `rate` jobs/s or at each of `rates`. Every
     configuration is also run alone (its single-job latency). Returns per
@@ -241,15 +286,18 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
     pool = device_jobs(configs)
     alone = []
     for job in pool:
-        srv = Server(tile=tile)
+        srv = Server(tile=tile, extra_budget=extra_budget)
         done, _ = run_stream(srv, [job], [0.0])
         srv.close()
         assert done[0].status == DONE
         alone.append(done[0].latency)
+    # the baseline: every configuration alone through the plain path (warm)
+    plain_job_seconds(pool[0])
+    plain = [plain_job_seconds(job) for job in pool]
     # warm-up burst of a full launch's worth of jobs (every configuration,
     # repeated), so the device memory pool has grown to a saturated engine's
     # footprint before the timed streams
-    srv = Server(tile=tile)
+    srv = Server(tile=tile, extra_budget=extra_budget)
     burst = [pool[i % len(pool)] for i in range(max(len(pool), 64))]
     run_stream(srv, burst, [0.0] * len(burst))
     srv.close()
@@ -261,7 +309,7 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         arrivals = np.cumsum(rng.exponential(1.0 / r, size=njobs))
         arrivals -= arrivals[0]
         jobs = [pool[i] for i in pick]
-        srv = Server(tile=tile)
+        srv = Server(tile=tile, extra_budget=extra_budget)
         done, wall = run_stream(srv, jobs, list(arrivals))
         stats = srv.stats()
         stats["release_s"] = srv.release_s
@@ -270,19 +318,31 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         lat = np.array([d.latency for d in ok])
         slow = np.array([d.latency / alone[index[id(d.job)]] for d in ok])
         work = sum(d.job.particles() * d.job.ncycles for d in ok)
+        plat, pend = fifo_latencies(list(arrivals), [plain[i] for i in pick])
         sweep.append({
             "rate_jobs_per_s": r, "jobs": njobs, "completed": len(ok),
             "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
                            "p99": 1e3 * float(np.percentile(lat, 99))},
             "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
                                   "p99": float(np.percentile(slow, 99))},
-            "throughput_particle_cycles_per_s": work / wall, "wall_s": wall, "engine": stats})
+            "throughput_particle_cycles_per_s": work / wall, "wall_s": wall, "engine": stats,
+            "plain_one_at_a_time": {
+                "latency_ms": {"p50": 1e3 * float(np.percentile(plat, 50)),
+                               "p99": 1e3 * float(np.percentile(plat, 99))},
+                "throughput_particle_cycles_per_s":
+                    sum(jobs[k].particles() * jobs[k].ncycles for k in range(njobs)) / pend}})
     release_cached_memory()
     out = dict(sweep[0])
     out.update({
         "single_job_latency_ms": {"p50": 1e3 * float(np.percentile(alone, 50)),
                                   "p99": 1e3 * float(np.percentile(alone, 99))},
         "p99_over_single_job_p99": sweep[0]["latency_ms"]["p99"] / (1e3 * float(np.percentile(alone, 99))),
+        "extra_budget": extra_budget or 1.0,
+        "plain_alone_ms": {"p50": 1e3 * float(np.percentile(plain, 50)),
+                           "p99": 1e3 * float(np.percentile(plain, 99))},
+        "baseline": ("plain_one_at_a_time: the same stream served one job at a time through the "
+                     "plain path (each configuration's wall time alone, measured; FIFO queue "
+                     "over the same arrivals)"),
         "mix": f"{n_configs} configurations: grids {list(SERVING_GRIDS)} "
                f"(weights {list(SERVING_GRID_WEIGHTS)}), ppc from {list(SERVING_PPC)} "
                "(capped at 5M particles per species), 2 or 4 species, 1-50 cycles, "

@@ -95,4 +95,4 @@ def test_deterministic_moments_match_oracle_and_default(cuda):
             assert (err[det] <= 1e-5).all(), (s, det, err[det])
         # exact sums of the same FP32 terms: no less accurate than the default
         # deposit's FP32 cell sums
-        assert err[True].max() <= err[False].max() + 1e-9, (s, err[True], err[False])
+        assert err[True].max() <= err[False].max() + 1e-8, (s, err[True], err[False])
