@@ -301,7 +301,9 @@ typedef struct spb_sim_desc {
                                (2^-38 of the species' largest possible term of
                                that moment at load: |q|max for rhon, |q|max x
                                4 |v|max for J, |q|max x 16 |v|max^2 for the
-                               pressures) and summed exactly
+                               pressures; the rounding's average loss,
+                               half a grid step per term, is added back) and
+                               summed exactly
                                in FP64, so the moments do not depend on the
                                particles' order in their buckets or on the
                                order of the atomics; the push gives every
