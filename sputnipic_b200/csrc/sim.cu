@@ -338,95 +338,24 @@ __device__ __forceinline__ Field6 field_at(const CycleParams &P, const float *__
   return F;
 }
 
-// The eight node records (E, B) of one cell, node i = a*4 + b*2 + c with
-// a/b/c = 1 the upper node on x/y/z: the start cell's, kept in registers for
-// the later NiterMover iterations (push with REUSE).
-struct CellNodes {
-  float4 a[8];
-  float2 b[8];
-};
-
-template <int TX, int TY, int TZ>
-__device__ __forceinline__ void nodes_staged(const float *__restrict__ sF, int n0, CellNodes &N) {
-  using T = Tile<TX, TY, TZ>;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int n = n0 + ((i >> 2) * T::BY + ((i >> 1) & 1)) * T::BZ + (i & 1);
-    N.a[i] = *reinterpret_cast<const float4 *>(sF + 8 * n);
-    N.b[i] = *reinterpret_cast<const float2 *>(sF + 8 * n + 4);
-  }
-}
-
-// The same from HBM/L2, with gather_global's clamps.
-__device__ __forceinline__ void nodes_global(const CycleParams &P, int gx, int gy, int gz,
-                                             CellNodes &N) {
-  const long sy = P.nzn, sx = (long)P.nyn * P.nzn;
-  const int hx = min(max(gx, -1), P.nxc), hy = min(max(gy, -1), P.nyc);
-  const int hz = min(max(gz, -1), P.nzc);
-  const long n0 = (long)(hx + 1) * sx + (long)(hy + 1) * sy + (hz + 1);
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const long n = n0 + (i >> 2) * sx + ((i >> 1) & 1) * sy + (i & 1);
-    N.a[i] = __ldg(reinterpret_cast<const float4 *>(P.fields8 + 8 * n));
-    N.b[i] = __ldg(reinterpret_cast<const float2 *>(P.fields8 + 8 * n + 4));
-  }
-}
-
-// Trilinear interpolation of a cell's node records held in registers: the
-// same operations in the same order as the staged gather.
-__device__ __forceinline__ Field6 combine(const CellNodes &N, float fx, float fy, float fz) {
-  const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
-  Field6 F[2];
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      const float wab = __fmul_rn(wx[a], wy[b]);
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const int i = a * 4 + b * 2 + c;
-        if (b == 0 && c == 0)
-          F[a] = first_node(__fmul_rn(wab, wz[c]), N.a[i], N.b[i]);
-        else
-          acc_node(F[a], __fmul_rn(wab, wz[c]), N.a[i], N.b[i]);
-      }
-    }
-  return {__fadd2_rn(F[0].exy, F[1].exy), __fadd2_rn(F[0].ezbx, F[1].ezbx),
-          __fadd2_rn(F[0].byz, F[1].byz)};
-}
-
 // mover_PC for one particle in cell units (src/Mover.cpp:33-157). n0c is the
 // tile node of the particle's start cell (the first gather is there, at the
 // stored offsets), or -1 when the start cell is not known to be staged. All
 // 32 lanes of the warp must call (the gathers vote: lanes whose cell lies
-// past the staged halo re-gather from HBM/L2). P.niter >= 1. With REUSE the
-// start cell's node records stay in registers, and a later iteration in
-// which every lane of the warp is still in its start cell interpolates from
-// them instead of gathering again (the results are the same either way).
-template <int TX, int TY, int TZ, bool REUSE = false>
+// past the staged halo re-gather from HBM/L2). P.niter >= 1.
+template <int TX, int TY, int TZ>
 __device__ __forceinline__ void push(const CycleParams &P, const float *__restrict__ sF, int c0x,
                                      int c0y, int c0z, int n0c, float qomdt2, int &cx, int &cy,
                                      int &cz, float &ox, float &oy, float &oz, float &u, float &v,
                                      float &w, int &bad) {
   float dx, dy, dz;   // predicted displacement in cells
   float up, vp, wp;
-  CellNodes N;
-  const int scx = cx, scy = cy, scz = cz;
   {
     // the first iteration gathers at the stored position, in the start cell
     bool inbox = true;
     int n0 = n0c;
     if (n0c < 0) n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, cx, cy, cz, inbox);
-    Field6 F;
-    if constexpr (REUSE) {
-      nodes_staged<TX, TY, TZ>(sF, n0, N);
-      if (__any_sync(0xffffffffu, !inbox)) {
-        if (!inbox) nodes_global(P, cx, cy, cz, N);
-      }
-      F = combine(N, ox, oy, oz);
-    } else {
-      F = field_at<TX, TY, TZ>(P, sF, n0, inbox, cx, cy, cz, ox, oy, oz);
-    }
+    const Field6 F = field_at<TX, TY, TZ>(P, sF, n0, inbox, cx, cy, cz, ox, oy, oz);
     boris(P, F, qomdt2, u, v, w, up, vp, wp, dx, dy, dz);
   }
 #pragma unroll 1
@@ -441,14 +370,9 @@ __device__ __forceinline__ void push(const CycleParams &P, const float *__restri
       truncate_below(gy, fy);
       truncate_below(gz, fz);
     }
-    Field6 F;
-    if (REUSE && __all_sync(0xffffffffu, (gx == scx) & (gy == scy) & (gz == scz))) {
-      F = combine(N, fx, fy, fz);
-    } else {
-      bool inbox;
-      const int n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, gx, gy, gz, inbox);
-      F = field_at<TX, TY, TZ>(P, sF, n0, inbox, gx, gy, gz, fx, fy, fz);
-    }
+    bool inbox;
+    const int n0 = tile_node<TX, TY, TZ>(c0x, c0y, c0z, gx, gy, gz, inbox);
+    const Field6 F = field_at<TX, TY, TZ>(P, sF, n0, inbox, gx, gy, gz, fx, fy, fz);
     boris(P, F, qomdt2, u, v, w, up, vp, wp, dx, dy, dz);
   }
   u = __fmaf_rn(2.0f, up, -u);
@@ -633,7 +557,7 @@ struct PushWarp {
 // copies the cells' records into a two-half ring (bulk copies, one per cell
 // piece; a half's barrier closes after its last piece is armed); a half is
 // refilled as soon as its last slot has been read.
-template <int TX, int TY, int TZ, int RH, bool REUSE>
+template <int TX, int TY, int TZ, int RH>
 __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const float *sF,
                                           PushWarp &W) {
   using T = Tile<TX, TY, TZ>;
@@ -728,7 +652,7 @@ __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const 
       int cx = c0x + lx, cy = c0y + ly, cz = c0z + lz;
       float ox = a.x, oy = a.y, oz = a.z, u = b.x, v = b.y, w = b.z;
       int pbad = 0;
-      push<TX, TY, TZ, REUSE>(P, sF, c0x, c0y, c0z, n0c, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
+      push<TX, TY, TZ>(P, sF, c0x, c0y, c0z, n0c, S.qomdt2, cx, cy, cz, ox, oy, oz, u, v, w,
                        pbad);
       W.bad |= valid ? pbad : 0;
       const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
@@ -799,7 +723,7 @@ __device__ __forceinline__ void report(const CycleParams &P, PushWarp &W) {
 // cell. Afterwards the CTAs push the overflow entries (gathers from L2).
 // MULTI = false: one job, parameters P1 and field map fmap. MULTI = true: the
 // jobs of table J, each tile's job parameters staged in shared memory.
-template <int TX, int TY, int TZ, int MINB, bool MULTI, bool REUSE = false>
+template <int TX, int TY, int TZ, int MINB, bool MULTI>
 __global__ void __launch_bounds__(SIM_TPB, MINB)
     k_push(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P1,
            const __grid_constant__ JobTable J, const __grid_constant__ MapsOf<MULTI> M) {
@@ -885,10 +809,10 @@ __global__ void __launch_bounds__(SIM_TPB, MINB)
         load_params(sP, J.params + job);
         cur_job = job;
       }
-      push_tile<TX, TY, TZ, RH, REUSE>(*sP, local, sF, W);
+      push_tile<TX, TY, TZ, RH>(*sP, local, sF, W);
       report(*sP, W);
     } else {
-      push_tile<TX, TY, TZ, RH, REUSE>(P1, local, sF, W);
+      push_tile<TX, TY, TZ, RH>(P1, local, sF, W);
     }
     // every warp is done with this field stage (and the staged parameters)
     // before they are refilled
@@ -1883,7 +1807,7 @@ CycleParams make_params(spb_sim *s) {
 namespace {
 
 // One cycle: zero the moments and the write-side counters, push, deposit.
-template <int TX, int TY, int TZ, int MINB, bool REUSE = false>
+template <int TX, int TY, int TZ, int MINB>
 int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   for (auto &q : s->sp) {
     if (!q.rec[0]) return fail(SPB_ERR_INVALID, "spb_sim_cycle: a species was never loaded");
@@ -1896,7 +1820,7 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   auto *const kdep = exact ? k_deposit<TX, TY, TZ, false, true> : k_deposit<TX, TY, TZ, false, false>;
   static bool attr = false;
   if (!attr) {
-    SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, false, REUSE>,
+    SPB_CUDA(cudaFuncSetAttribute(k_push<TX, TY, TZ, MINB, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
     SPB_CUDA(cudaFuncSetAttribute(k_deposit<TX, TY, TZ, false, false>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1910,7 +1834,7 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   const int ntiles = s->nt[0] * s->nt[1] * s->nt[2];
   static int pocc = 0, docc[2] = {0, 0};   // resident CTAs per SM
   if (!pocc) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, false, REUSE>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, k_push<TX, TY, TZ, MINB, false>,
                                                       SIM_TPB, psm) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &docc[0], k_deposit<TX, TY, TZ, false, false>, dep_tpb<TX, TY, TZ>(),
@@ -1929,7 +1853,7 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   const int pctas = std::min(ntiles, s->d.ctas > 0 ? s->d.ctas : pocc * num_sms());
   const int dctas = std::min(ntiles, docc[exact ? 1 : 0] * num_sms());
   EvCycle ev{record_event(s, st), nullptr, nullptr};
-  k_push<TX, TY, TZ, MINB, false, REUSE><<<pctas, SIM_TPB, psm, st>>>(s->fmap, P, JobTable{},
+  k_push<TX, TY, TZ, MINB, false><<<pctas, SIM_TPB, psm, st>>>(s->fmap, P, JobTable{},
                                                                       NoMaps{});
   SPB_CUDA(cudaGetLastError());
   ev.m = record_event(s, st);
@@ -1953,7 +1877,6 @@ template <int TX, int TY, int TZ>
 int launch_cycle(spb_sim *s, cudaStream_t st) {
   switch (s->d.variant) {
     case 1: return launch_cycle_v<TX, TY, TZ, 2>(s, st);
-    case 3: return launch_cycle_v<TX, TY, TZ, 2, true>(s, st);
     case 2: return launch_cycle_v<TX, TY, TZ, 4>(s, st);
     default: return launch_cycle_v<TX, TY, TZ, 3>(s, st);
   }
