@@ -313,6 +313,14 @@ typedef struct spb_sim_desc {
                                cell with 80 FP64 sums: slower than the default
                                deposit. spb_sim_check reports SPB_ERR_CAPACITY
                                if a sum ever left its exact range. */
+  int fused;                /* 1: each cycle is one persistent cooperative
+                               launch (the batching form): every CTA pushes a
+                               tile, then deposits the tile it pushed
+                               ceil(R/G) steps earlier once the 27 tiles around
+                               it are pushed, so the deposit overlaps the
+                               push; overflow entries are pushed and deposited
+                               after two grid barriers. Not with
+                               deterministic. */
 } spb_sim_desc;
 
 /* Whether a tile shape has an instantiated kernel. */

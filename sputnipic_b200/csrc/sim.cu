@@ -475,17 +475,22 @@ __device__ __forceinline__ void flush(const SpeciesDev &S, const Pending &p, con
 
 // Issues the counter updates of a pushed slot and stages its records. All 32
 // lanes call, after the previous slot's flush.
+// `far`: the particle goes to the overflow list whatever its bucket's room
+// (the fused cycle's particles that left their tile's neighbourhood; every
+// lane of a destination group has the same value).
 __device__ __forceinline__ void issue_slot(const SpeciesDev &S, Pending &p, float4 *stage,
-                                          int nkey, bool valid, float4 a, float4 b, int lane) {
+                                          int nkey, bool valid, float4 a, float4 b, int lane,
+                                          bool far = false) {
   const unsigned peers = __match_any_sync(FULL, valid ? nkey : -1);
   p.leader = __ffs(peers) - 1;
   p.rank = __popc(peers & ((1u << lane) - 1u));
   p.slot0 = 0;
-  if (valid && lane == p.leader) p.slot0 = atomicAdd(S.cout + nkey, __popc(peers));
+  const bool place = valid && !far;
+  if (place && lane == p.leader) p.slot0 = atomicAdd(S.cout + nkey, __popc(peers));
   p.key = nkey;
   p.valid = valid;
-  p.dbase = valid ? __ldg(S.base + nkey) : 0;
-  p.dend = valid ? __ldg(S.base + nkey + 1) : 0;
+  p.dbase = place ? __ldg(S.base + nkey) : 0;
+  p.dend = place ? __ldg(S.base + nkey + 1) : 0;
   stage[lane] = a;
   stage[32 + lane] = b;
 }
@@ -557,7 +562,14 @@ struct PushWarp {
 // copies the cells' records into a two-half ring (bulk copies, one per cell
 // piece; a half's barrier closes after its last piece is armed); a half is
 // refilled as soon as its last slot has been read.
-template <int TX, int TY, int TZ, int RH>
+// Whether a destination tile coordinate d tiles away on an axis of n tiles
+// (periodic or not) lies outside the source tile's neighbourhood.
+__device__ __forceinline__ bool far_axis(int d, int n, int periodic) {
+  if (periodic && n > 2) d = d == n - 1 ? -1 : (d == 1 - n ? 1 : d);
+  return d < -1 || d > 1;
+}
+
+template <int TX, int TY, int TZ, int RH, bool FUSED = false>
 __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const float *sF,
                                           PushWarp &W) {
   using T = Tile<TX, TY, TZ>;
@@ -656,10 +668,15 @@ __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const 
                        pbad);
       W.bad |= valid ? pbad : 0;
       const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
+      bool far = false;
+      if constexpr (FUSED)
+        far = far_axis(cx / TX - tx, P.ntx, P.periodic[0]) |
+              far_axis(cy / TY - ty, P.nty, P.periodic[1]) |
+              far_axis(cz / TZ - tz, P.ntz, P.periodic[2]);
       flush(S, pend, W.wrec, lane, W.lost);   // the previous slot's counters are back
       __syncwarp();
       issue_slot(S, pend, W.wrec, nkey, valid, make_float4(ox, oy, oz, a.w),
-                 make_float4(u, v, w, 0.f), lane);
+                 make_float4(u, v, w, 0.f), lane, far);
       // last slot of half h read by every lane: refill it
       if ((rv + 32) % RH == 0 && pv < total) {
         __syncwarp();
@@ -674,7 +691,9 @@ __device__ __forceinline__ void push_tile(const CycleParams &P, int tile, const 
 // The overflow entries of every species of job P: pushed with gathers from
 // L2 (the staged-tile origin is placed out of reach, so every gather takes
 // the global path). sF is any valid staged buffer. All threads call.
-template <int TX, int TY, int TZ>
+// TO_LIST: every pushed entry goes to the new overflow list (the fused cycle
+// has deposited the buckets already).
+template <int TX, int TY, int TZ, bool TO_LIST = false>
 __device__ __forceinline__ void push_overflow(const CycleParams &P, const float *sF, PushWarp &W) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int s = 0; s < P.ns; ++s) {
@@ -697,9 +716,14 @@ __device__ __forceinline__ void push_overflow(const CycleParams &P, const float 
       W.bad |= valid ? pbad : 0;
       const int nkey = tile_key<TX, TY, TZ>(cx, cy, cz, P.nty, P.ntz);
       if (valid) {
-        const int slot = atomicAdd(S.cout + nkey, 1);
-        W.lost |= put_at(S, nkey, S.base[nkey], S.base[nkey + 1], slot,
-                         make_float4(ox, oy, oz, a.w), make_float4(u, v, w, 0.f));
+        if (TO_LIST) {
+          W.lost |= put_at(S, nkey, 0, 0, 0, make_float4(ox, oy, oz, a.w),
+                           make_float4(u, v, w, 0.f));
+        } else {
+          const int slot = atomicAdd(S.cout + nkey, 1);
+          W.lost |= put_at(S, nkey, S.base[nkey], S.base[nkey + 1], slot,
+                           make_float4(ox, oy, oz, a.w), make_float4(u, v, w, 0.f));
+        }
       }
     }
   }
@@ -946,6 +970,22 @@ __device__ __forceinline__ void ld_rec(const float4 *p, float4 &a, float4 &b) {
       : "l"(p));
 }
 
+// The same through L2 only (coherent with records written by other CTAs of
+// the same launch, which the fused cycle deposits).
+__device__ __forceinline__ void ld_rec_cg(const float4 *p, float4 &a, float4 &b) {
+  asm("ld.global.cg.L2::256B.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
+template <bool COH>
+__device__ __forceinline__ void ld_record(const float4 *p, float4 &a, float4 &b) {
+  if constexpr (COH)
+    ld_rec_cg(p, a, b);
+  else
+    ld_rec(p, a, b);
+}
+
 // Per-warp quota of the deposit (all 32 lanes call with their cell's count):
 // lanes sum at most Q particles of their own cell, one particle per lane per
 // step; the excess of the cells above Q is summed by the whole warp, 32
@@ -976,11 +1016,15 @@ __device__ __forceinline__ int deposit_quota(int cnt) {
 // Each node of the tile then adds up the totals of its (up to 8) cells in the
 // tile and one FP64 atomic per node and moment adds the sum into the moments.
 // All threads call.
-template <int TX, int TY, int TZ>
+// NT: the CTA's threads (at least one per cell); COH: coherent loads of the
+// counters and records (the fused cycle, where other CTAs of the launch wrote
+// them).
+template <int TX, int TY, int TZ, int NT = dep_tpb<TX, TY, TZ>(), bool COH = false>
 __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, float *sCell) {
   using T = Tile<TX, TY, TZ>;
   constexpr int NX = TX + 1, NY = TY + 1, NZ = TZ + 1, NB = NX * NY * NZ;
-  constexpr int TC = T::TC, NT = dep_tpb<TX, TY, TZ>();
+  constexpr int TC = T::TC;
+  static_assert(NT >= TC && NT % 32 == 0, "one thread per cell, whole warps");
   const int tid = threadIdx.x;
   const bool own = tid < TC;
   const long nodes = (long)P.nxn * P.nyn * P.nzn;
@@ -993,7 +1037,7 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
     if (own) {
       const int key = tile * TC + tid;
       const long long b0 = S.base[key];
-      cnt = (int)min((long long)S.cout[key], S.base[key + 1] - b0);
+      cnt = (int)min((long long)(COH ? __ldcg(S.cout + key) : S.cout[key]), S.base[key + 1] - b0);
       rec += 2 * b0;
     }
     // quota: each lane sums at most Q particles of its own cell; the rest of
@@ -1005,14 +1049,14 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
 #pragma unroll
     for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, a1 = a, b1 = a;
-    if (n1 > 0) ld_rec(rec, a, b);
-    if (n1 > 1) ld_rec(rec + 2, a1, b1);
+    if (n1 > 0) ld_record<COH>(rec, a, b);
+    if (n1 > 1) ld_record<COH>(rec + 2, a1, b1);
 #pragma unroll 1
     for (int k = 0; k < trips; ++k) {
       // two records in flight while this one is summed; lanes past their
       // count add zero terms
       float4 na = a1, nb = b1;
-      if (k + 2 < n1) ld_rec(rec + 2 * (k + 2), na, nb);
+      if (k + 2 < n1) ld_record<COH>(rec + 2 * (k + 2), na, nb);
       add_terms(acc, k < n1 ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, 0);
       a = a1;
       b = b1;
@@ -1047,7 +1091,7 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
         for (int o = Q; o < hc; o += 32) {
           const int i = o + lane;
           float4 ha = make_float4(0.f, 0.f, 0.f, 0.f), hb = ha;
-          if (i < hc) ld_rec(hrec + 2 * i, ha, hb);
+          if (i < hc) ld_record<COH>(hrec + 2 * i, ha, hb);
           add_terms(acc, i < hc ? ha.w : 0.0f, ha.x, ha.y, ha.z, hb.x, hb.y, hb.z, lane);
         }
         float r[5];
@@ -1174,7 +1218,7 @@ __device__ __forceinline__ void deposit_tile_exact(const CycleParams &P, int til
 // warp in FP32 (warp_sum80) and added with one FP64 atomic per node and
 // moment; the remaining entries deposit one by one (deposit_global). Called
 // by whole warps.
-template <int TX, int TY, int TZ, bool EXACT>
+template <int TX, int TY, int TZ, bool EXACT, bool COH = false>
 __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
   const int lane = threadIdx.x & 31;
   const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
@@ -1188,16 +1232,16 @@ __device__ __forceinline__ void deposit_overflow(const CycleParams &P) {
   const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
   for (int s = 0; s < P.ns; ++s) {
     const SpeciesDev &S = P.sp[s];
-    const long on = min(*S.ocout, S.ocap);
+    const long on = min(COH ? __ldcg(S.ocout) : *S.ocout, S.ocap);
     for (long base = gwarp * 32; base < on; base += nwarps * 32) {
       const long i = base + lane;
       bool valid = i < on;
       int key = -1;
       float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
       if (valid) {
-        key = S.okout[i];
-        a = S.oout[2 * i];
-        b = S.oout[2 * i + 1];
+        key = COH ? __ldcg(S.okout + i) : S.okout[i];
+        a = COH ? __ldcg(S.oout + 2 * i) : S.oout[2 * i];
+        b = COH ? __ldcg(S.oout + 2 * i + 1) : S.oout[2 * i + 1];
       }
       if constexpr (EXACT) {   // every entry on its own, exactly
         if (valid) {
@@ -1290,6 +1334,240 @@ __global__ void __launch_bounds__(dep_tpb<TX, TY, TZ>(),
       deposit_overflow<TX, TY, TZ, false>(P1);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// the fused cycle: push and deposit in one persistent cooperative launch
+// ---------------------------------------------------------------------------
+
+// Per-cycle device state of the fused cycle (zeroed before every cycle).
+struct FusedAux {
+  int *done;        // [ntiles] 1 once a tile's particles are pushed
+  unsigned *bar;    // [2] arrivals at the two grid barriers
+  int lag;          // waves between a tile's push and its deposit
+};
+
+constexpr long long GRID_WAIT_CYCLES = 4000000000LL;   // ~2 s: bounded waits
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_acquire_u(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident): thread 0 of
+// each CTA arrives and waits, bounded; false for every thread if it gave up.
+__device__ __forceinline__ bool grid_barrier(unsigned *count) {
+  __threadfence();
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    atomicAdd(count, 1u);
+    const long long t0 = clock64();
+    while (ld_acquire_u(count) < gridDim.x) {
+      if (clock64() - t0 > GRID_WAIT_CYCLES) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+  }
+  ok = __syncthreads_and(ok);
+  __threadfence();
+  return ok != 0;
+}
+
+// Launch order of the tiles: on a periodic axis of n > 2 tiles the order
+// folds (0, n-1, 1, n-2, ...) so that a tile's wrap-around neighbour comes
+// next to it; every neighbour is then at most 2 positions away per axis.
+__host__ __device__ __forceinline__ int unfold_pos(int f, int n, int periodic) {
+  if (!periodic || n <= 2) return f;
+  return (f & 1) ? n - 1 - (f >> 1) : (f >> 1);
+}
+__device__ __forceinline__ int tile_of_order(const CycleParams &P, int o) {
+  const int fz = o % P.ntz, fy = (o / P.ntz) % P.nty, fx = o / (P.ntz * P.nty);
+  return (unfold_pos(fx, P.ntx, P.periodic[0]) * P.nty + unfold_pos(fy, P.nty, P.periodic[1])) *
+             P.ntz +
+         unfold_pos(fz, P.ntz, P.periodic[2]);
+}
+
+// Shared memory of the fused cycle: the push's field stages, then its record
+// staging and ring or the deposit's per-cell sums (whichever is larger; the
+// two are used at different times), then the barriers.
+template <int TX, int TY, int TZ, int MINB>
+__host__ __device__ constexpr size_t fused_rec_bytes() {
+  return (size_t)(SIM_NW * 64 + SIM_NW * 2 * ring_half<MINB>() * 2) * 16 >
+                 (size_t)Tile<TX, TY, TZ>::TC * 80 * 4
+             ? (size_t)(SIM_NW * 64 + SIM_NW * 2 * ring_half<MINB>() * 2) * 16
+             : (size_t)Tile<TX, TY, TZ>::TC * 80 * 4;
+}
+template <int TX, int TY, int TZ, int MINB>
+__host__ __device__ constexpr size_t fused_smem() {
+  return 2 * (size_t)Tile<TX, TY, TZ>::SF * 4 + fused_rec_bytes<TX, TY, TZ, MINB>() +
+         (2 + 2 * SIM_NW) * sizeof(uint64_t);
+}
+
+// Thread 0 waits (bounded) until every neighbour of `tile` (itself included,
+// wrapping on periodic axes) is pushed; false for every thread if it gave up.
+__device__ __forceinline__ bool wait_neighbours(const CycleParams &P, const int *done, int tile) {
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    const int tz = tile % P.ntz, ty = (tile / P.ntz) % P.nty, tx = tile / (P.ntz * P.nty);
+    const long long t0 = clock64();
+    for (int dx = -1; dx <= 1 && ok; ++dx)
+      for (int dy = -1; dy <= 1 && ok; ++dy)
+        for (int dz = -1; dz <= 1 && ok; ++dz) {
+          int n[3] = {tx + dx, ty + dy, tz + dz};
+          const int N[3] = {P.ntx, P.nty, P.ntz};
+          bool skip = false;
+          for (int a = 0; a < 3; ++a) {
+            if (n[a] >= 0 && n[a] < N[a]) continue;
+            if (!P.periodic[a]) skip = true;
+            n[a] = (n[a] + N[a]) % N[a];
+          }
+          if (skip) continue;
+          const int *f = done + (n[0] * P.nty + n[1]) * P.ntz + n[2];
+          while (ld_acquire(f) == 0) {
+            if (clock64() - t0 > GRID_WAIT_CYCLES) {
+              ok = 0;
+              break;
+            }
+            __nanosleep(64);
+          }
+        }
+  }
+  ok = __syncthreads_and(ok);
+  __threadfence();
+  return ok != 0;
+}
+
+// The fused cycle (the batching form's one launch per cycle), all species.
+// Persistent CTAs, all resident (cooperative launch), take the tiles in the
+// launch order above: at step k a CTA pushes its k-th tile (as k_push does:
+// TMA-staged fields, record ring, particles written into their new cells'
+// buckets) and publishes it, then deposits its tile from lag steps earlier
+// (as k_deposit does, with coherent loads) once the 27 tiles around it are
+// published, whose pushes are the only ones that write into its buckets. The
+// push keeps the SM's shared-memory pipe busy and the deposit its arithmetic
+// and load units, so the two phases overlap across the CTAs of an SM. A
+// pushed particle that left its tile's neighbourhood goes to the overflow
+// list. Then, after a grid barrier, the entries of the previous overflow list
+// are pushed into the new overflow list, and after a second barrier every
+// entry of the new list is deposited. lag = ceil(R / G) with R the largest
+// launch-order distance between neighbouring tiles and G the CTAs, so that a
+// CTA only ever waits for pushes of steps up to its own: no cycle of waits.
+// Every wait is bounded (an error bit, then the CTA stops).
+template <int TX, int TY, int TZ, int MINB>
+__global__ void __launch_bounds__(SIM_TPB, MINB)
+    k_cycle(const __grid_constant__ CUtensorMap fmap, const __grid_constant__ CycleParams P,
+            const __grid_constant__ FusedAux X) {
+  using T = Tile<TX, TY, TZ>;
+  constexpr int RH = ring_half<MINB>();
+  static_assert(T::TC % SIM_NW == 0 && T::TC / SIM_NW <= 32,
+                "cells per warp must fit a warp's lanes");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float *sF0 = reinterpret_cast<float *>(smem_raw);                 // 2 stages x SF
+  float4 *sRec = reinterpret_cast<float4 *>(sF0 + 2 * T::SF);       // NW x 64 staged records
+  float4 *sBuf = sRec + SIM_NW * 64;                                // NW x 2 x RH records
+  uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(sRec) +
+                                               fused_rec_bytes<TX, TY, TZ, MINB>());   // 2 + 2 NW
+  // the deposit's per-cell sums reuse the record staging and ring (idle
+  // between two tiles' pushes; the field stages stay untouched)
+  float *sCell = reinterpret_cast<float *>(sRec);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  PushWarp W;
+  W.wrec = sRec + warp * 64;
+  W.ring = sBuf + warp * 2 * RH * 2;
+  W.cbar = bar + 2 + warp * 2;
+  if (smem_addr(sF0) & 127u) {
+    if (tid == 0) atomicOr(P.err, ERRBIT_SMEM_ALIGN);
+    return;
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+  }
+  if (lane == 0) {
+    mbar_init(W.cbar, 1);
+    mbar_init(W.cbar + 1, 1);
+  }
+  __syncthreads();
+
+  const int ntiles = P.ntx * P.nty * P.ntz;
+  const int G = gridDim.x;
+  const unsigned box_bytes = (unsigned)(T::BN * 8 * sizeof(float));
+  auto issue = [&](int tile, int stage) {   // thread 0
+    const int z = tile % P.ntz, y = (tile / P.ntz) % P.nty, x = tile / (P.ntz * P.nty);
+    fence_proxy_async();
+    mbar_expect_tx(bar + stage, box_bytes);
+    tma_load_4d(sF0 + stage * T::SF, &fmap, 0, z * TZ, y * TY, x * TX, bar + stage);
+  };
+  const int first = blockIdx.x;
+  if (tid == 0 && first < ntiles) issue(tile_of_order(P, first), 0);
+  int it = 0;   // tiles pushed by this CTA
+  for (int k = 0;; ++k) {
+    const int o = first + k * G;                // order index pushed at this step
+    const int od = first + (k - X.lag) * G;     // order index deposited at this step
+    if (o >= ntiles && od >= ntiles) break;
+    if (o < ntiles) {
+      const int stage = it & 1;
+      if (tid == 0 && o + G < ntiles) issue(tile_of_order(P, o + G), stage ^ 1);
+      const bool arrived = mbar_wait_bounded(bar + stage, (it >> 1) & 1);
+      if (__syncthreads_or(!arrived)) {
+        if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+        mbar_wait_bounded(bar + stage, (it >> 1) & 1);
+        mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
+        return;
+      }
+      const int tile = tile_of_order(P, o);
+      push_tile<TX, TY, TZ, RH, true>(P, tile, sF0 + stage * T::SF, W);
+      if (__syncthreads_or(W.dead)) {
+        if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+        for (int b = 0; b < 2; ++b)
+          if (W.inflight & (1u << b)) mbar_wait_bounded(W.cbar + b, (W.phase >> b) & 1u);
+        if (o + G < ntiles) mbar_wait_bounded(bar + (stage ^ 1), ((it + 1) >> 1) & 1);
+        return;
+      }
+      // publish: every thread's stores, then the flag
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(X.done + tile, 1);
+      ++it;
+    }
+    if (od >= 0 && od < ntiles) {
+      const int tile = tile_of_order(P, od);
+      if (!wait_neighbours(P, X.done, tile)) {
+        if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+        if (o + G < ntiles) mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1);
+        return;
+      }
+      deposit_tile<TX, TY, TZ, SIM_TPB, true>(P, tile, sCell);
+      // the next tile's bulk copies overwrite the sums written here
+      fence_proxy_async();
+      __syncthreads();
+    }
+  }
+  report(P, W);
+  if (!grid_barrier(X.bar)) {
+    if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+    return;
+  }
+  push_overflow<TX, TY, TZ, true>(P, sF0, W);
+  report(P, W);
+  if (!grid_barrier(X.bar + 1)) {
+    if (tid == 0) atomicOr(P.err, ERRBIT_TIMEOUT);
+    return;
+  }
+  deposit_overflow<TX, TY, TZ, false, true>(P);
 }
 
 // The deterministic deposit's moments are unscaled sums: times invVOL, once.
@@ -1873,8 +2151,62 @@ int launch_cycle_v(spb_sim *s, cudaStream_t st) {
   return SPB_OK;
 }
 
+// The fused cycle: zeroing (moments, write-side counters, the tiles' flags
+// and the barrier counters), then k_cycle as one cooperative launch of every
+// CTA that fits on the device at once.
+template <int TX, int TY, int TZ>
+int launch_cycle_fused(spb_sim *s, cudaStream_t st) {
+  constexpr int MINB = 2;
+  for (auto &q : s->sp) {
+    if (!q.rec[0]) return fail(SPB_ERR_INVALID, "spb_sim_cycle: a species was never loaded");
+    SPB_CUDA(cudaMemsetAsync(q.mom, 0, 10 * s->nodes * sizeof(double), st));
+    SPB_CUDA(cudaMemsetAsync(q.cnt[1 - q.cur], 0, s->ncells * sizeof(int), st));
+    SPB_CUDA(cudaMemsetAsync(q.ocnt + (1 - q.cur), 0, sizeof(int), st));
+  }
+  const int ntiles = s->nt[0] * s->nt[1] * s->nt[2];
+  SPB_CUDA(cudaMemsetAsync(s->fused_done, 0, (ntiles + 2) * sizeof(int), st));
+  const size_t sm = fused_smem<TX, TY, TZ, MINB>();
+  static int occ = -1;
+  if (occ < 0) {
+    SPB_CUDA(cudaFuncSetAttribute(k_cycle<TX, TY, TZ, MINB>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    SPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cycle<TX, TY, TZ, MINB>,
+                                                           SIM_TPB, sm));
+  }
+  if (occ < 1) return fail(SPB_ERR_UNSUPPORTED, "fused cycle: the kernel does not fit an SM");
+  const int G = occ * num_sms();
+  // largest launch-order distance between neighbouring tiles (folded
+  // periodic axes: 2 positions)
+  int step[3];
+  for (int a = 0; a < 3; ++a) step[a] = (s->d.periodic[a] && s->nt[a] > 2) ? 2 : 1;
+  const long R = (long)step[0] * s->nt[1] * s->nt[2] + (long)step[1] * s->nt[2] + step[2];
+  const FusedAux X{s->fused_done, reinterpret_cast<unsigned *>(s->fused_done + ntiles),
+                   (int)std::max<long>(1, ceil_div(R, G))};
+  const CycleParams P = make_params(s);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)G);
+  cfg.blockDim = dim3(SIM_TPB);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  EvCycle ev{record_event(s, st), nullptr, nullptr};
+  SPB_CUDA(cudaLaunchKernelEx(&cfg, k_cycle<TX, TY, TZ, MINB>, s->fmap, P, X));
+  ev.m = record_event(s, st);
+  ev.e = record_event(s, st);
+  if (ev.b && ev.m && ev.e) s->ev_cycle.push_back(ev);
+  g_launches += 1;
+  s->launches += 1;
+  for (auto &q : s->sp) q.cur = 1 - q.cur;
+  return SPB_OK;
+}
+
 template <int TX, int TY, int TZ>
 int launch_cycle(spb_sim *s, cudaStream_t st) {
+  if (s->d.fused) return launch_cycle_fused<TX, TY, TZ>(s, st);
   switch (s->d.variant) {
     case 1: return launch_cycle_v<TX, TY, TZ, 2>(s, st);
     case 2: return launch_cycle_v<TX, TY, TZ, 4>(s, st);
@@ -2284,6 +2616,9 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
   if (d->niter < 1 || !(d->dt > 0) || !(d->c != 0))
     return fail(SPB_ERR_INVALID, "spb_sim_create: bad NiterMover, dt or c");
   if (d->bucket_slots < 0) return fail(SPB_ERR_INVALID, "spb_sim_create: bucket_slots < 0");
+  if (d->fused && d->deterministic)
+    return fail(SPB_ERR_UNSUPPORTED,
+                "spb_sim_create: the fused cycle has no deterministic deposit (use one of them)");
   int tile[3] = {d->tile[0], d->tile[1], d->tile[2]};
   if (!tile[0] || !tile[1] || !tile[2]) {
     tile[0] = 8;
@@ -2328,6 +2663,11 @@ extern "C" int spb_sim_create(const spb_sim_desc *d, spb_sim **out) {
       dmalloc(&s->counts, s->ncells * sizeof(int)) != cudaSuccess ||
       dmalloc(&s->lcap, s->ncells * sizeof(long long)) != cudaSuccess ||
       dmalloc(&s->offset, (s->ncells + 1) * sizeof(long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail(SPB_ERR_ALLOC, "spb_sim_create: device allocation failed"));
+  }
+  if (d->fused && dmalloc(&s->fused_done, (s->nt[0] * s->nt[1] * s->nt[2] + 2) * sizeof(int)) !=
+                      cudaSuccess) {
     cudaGetLastError();
     return bail(fail(SPB_ERR_ALLOC, "spb_sim_create: device allocation failed"));
   }
@@ -2493,6 +2833,7 @@ extern "C" void spb_sim_destroy(spb_sim *s) {
   dfree(s->counts);
   dfree(s->lcap);
   dfree(s->offset);
+  dfree(s->fused_done);
   delete s;
 }
 

@@ -69,6 +69,7 @@ struct spb_sim {
   int *counts = nullptr;          // [ncells] particles per cell
   long long *lcap = nullptr;      // [ncells] capacities / clamped counts
   long long *offset = nullptr;    // [ncells + 1] readback offsets
+  int *fused_done = nullptr;      // fused cycle: [tiles] pushed flags + 2 barrier counters
   CUtensorMap fmap{};
   bool fields_set = false;
   int cycles_since_check = 0;
