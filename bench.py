@@ -274,7 +274,8 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
         tune = autotune(wl, fields, parts)
         args.tile, args.variant = list(tune["tile"]), tune["variant"]
     sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort, variant=args.variant,
-                     graph=not args.no_graph)
+                     graph=not args.no_graph, fused=args.fused,
+                     deterministic=args.deterministic)
     sim.set_fields(fields)
     for s, p in enumerate(parts):
         sim.load_species(s, p)
@@ -458,7 +459,12 @@ def run_ours(args, rank, world, local_rank):
                                    "one mover + 10-moment deposit cycle",
                        "form": "precision (per-cell buckets of fp32 offsets, charge and "
                                "velocities; fp32 push; fp32 per-cell register sums -> "
-                               "fp64 moments)",
+                               "fp64 moments)" + ("; fused cycle" if args.fused else "")
+                               + ("; deterministic deposit" if args.deterministic else ""),
+                       "step": "the driver's cycle: new fields (six device arrays uploaded "
+                               "and packed), mover + deposit of every species, applyBCids "
+                               "per species" + (", moment all-reduce over the ranks"
+                                                if world > 1 else ""),
                        "tile": list(args.tile), "overflow_check_every": args.resort,
                        "cuda_graph": not args.no_graph,
                        "push_variant": args.variant, "buckets": prec["buckets"],
@@ -479,22 +485,49 @@ def run_ours(args, rank, world, local_rank):
 
 def measure_batching(torch, rank):
     """The batching form: 4 species of uneven counts (65.5M, 65.5M, 6.55M,
-    6.55M) on the GEM grid, 20 cycles from the loaded state, tile shape, push
-    residency and overflow-check interval k in {1, 2, 4, 8} picked by the
-    autotuner (sputnipic_b200.sim.autotune_batching)."""
+    6.55M) on the GEM grid, 20 cycles from the loaded state with CUDA graphs.
+    The two-launch cycle with tile shape, push residency and overflow-check
+    interval k in {1, 2, 4, 8} picked by the autotuner
+    (sputnipic_b200.sim.autotune_batching); then, at the chosen tile shape and
+    interval, the fused cycle (one persistent launch per cycle) and the
+    deterministic deposit, timed the same way. `value` is the fastest."""
     from sputnipic_b200.device import gen_fields, gen_particles
-    from sputnipic_b200.sim import autotune_batching
+    from sputnipic_b200.sim import Simulation, autotune_batching
     wl = R.rank_workload(W.batching_gem(), rank)
     fields = gen_fields(wl)
     parts = [gen_particles(wl, s) for s in range(len(wl.species))]
+    n = sum(p["x"].numel() for p in parts)
     tune = autotune_batching(wl, fields, parts, cycles=wl.cycles)
+    modes = {"two_launch": {"ms_per_cycle": tune["ms"] / tune["cycles"],
+                            "particles_per_s": tune["particles_per_s"]}}
+    st = torch.cuda.current_stream()
+    for name, kw in (("fused", {"fused": True}), ("deterministic", {"deterministic": True})):
+        sim = Simulation(wl, tile=tuple(tune["tile"]), resort_every=tune["check_every"],
+                         graph=True, **kw)
+        sim.set_fields(fields)
+        for s, p in enumerate(parts):
+            sim.load_species(s, p)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(st)
+        sim.cycle(wl.cycles, stream=st)
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        rc = sim.check()
+        sim.close()
+        if rc:
+            raise RuntimeError(f"batching {name} status {rc}")
+        ms = ev[0].elapsed_time(ev[1])
+        modes[name] = {"ms_per_cycle": ms / wl.cycles,
+                       "particles_per_s": n * wl.cycles / (ms * 1e-3)}
     del parts, fields
     torch.cuda.empty_cache()
+    best = max(modes, key=lambda k: modes[k]["particles_per_s"])
     counts = [wl.species_count(s) for s in range(len(wl.species))]
     return {"workload": f"{wl.name}: species of {', '.join(f'{c:,}' for c in counts)} "
                         f"particles, {wl.cycles} cycles, CUDA graphs",
-            "value": tune["particles_per_s"], "unit": UNIT,
-            "ms_per_cycle": tune["ms"] / tune["cycles"], "tile": tune["tile"],
+            "value": modes[best]["particles_per_s"], "unit": UNIT, "mode": best,
+            "ms_per_cycle": modes[best]["ms_per_cycle"], "modes": modes, "tile": tune["tile"],
             "push_variant": tune["variant"], "check_every": tune["check_every"],
             "intervals": tune["intervals"], "tile_trials": tune["tile_trials"]}
 
@@ -661,6 +694,10 @@ def main():
                     help="push kernel residency: 0 three CTAs per SM, 1 two, 2 four")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the tile shape and push variant first (timed on this workload)")
+    ap.add_argument("--fused", action="store_true",
+                    help="precision form: the fused cycle (one persistent launch per cycle)")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="precision form: the deterministic deposit")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each cycle directly instead of replaying a CUDA graph")
     ap.add_argument("--no-serving", action="store_true",
