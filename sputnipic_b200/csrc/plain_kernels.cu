@@ -408,12 +408,15 @@ __device__ __forceinline__ Particle smem_particle(const GroupSmem &S, int j) {
   return Particle{S.p[0][j], S.p[1][j], S.p[2][j], S.p[3][j], S.p[4][j], S.p[5][j], S.p[6][j]};
 }
 
+// perm (may be null): the particles in cell order (k_p2g_scatter), so that a
+// chunk holds whole cells whatever the order of the arrays.
 template <bool ACC>
 __global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
     GeomDev g, const float *__restrict__ x, const float *__restrict__ y,
     const float *__restrict__ z, const float *__restrict__ u, const float *__restrict__ v,
     const float *__restrict__ w, const float *__restrict__ q, long n,
-    const __grid_constant__ DepTarget T, int *__restrict__ err) {
+    const unsigned *__restrict__ perm, const __grid_constant__ DepTarget T,
+    int *__restrict__ err) {
   __shared__ GroupSmem S;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long base = (long)blockIdx.x * GP_CHUNK;
@@ -430,8 +433,9 @@ __global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
     const bool valid = j < cnt;
     int key = -1;
     if (valid) {
+      const long i = perm ? (long)perm[base + j] : base + j;
 #pragma unroll
-      for (int a = 0; a < 7; ++a) S.p[a][j] = src[a][base + j];
+      for (int a = 0; a < 7; ++a) S.p[a][j] = src[a][i];
       const int ix = clamp_cell(cell_floor(S.p[0][j], g.xStart, g.invdx, g.nxn), g.nxn, bad);
       const int iy = clamp_cell(cell_floor(S.p[1][j], g.yStart, g.invdy, g.nyn), g.nyn, bad);
       const int iz = clamp_cell(cell_floor(S.p[2][j], g.zStart, g.invdz, g.nzn), g.nzn, bad);
@@ -538,6 +542,108 @@ __global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
       if (i >= lo && i < hi) dep_add<ACC>(T, node, mbase + i, r[i]);
   }
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
+// The plain deposit's cell sort: a counting sort of (cell, index) pairs by
+// the deposit's own cell (the node-space floor cell of src/Mover.cpp:399-401).
+// Keys and per-cell counts (one atomic per distinct cell of a warp) ...
+__global__ void __launch_bounds__(TPB) k_p2g_keys(GeomDev g, const float *__restrict__ x,
+                                                  const float *__restrict__ y,
+                                                  const float *__restrict__ z, long n,
+                                                  unsigned *__restrict__ key,
+                                                  unsigned *__restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  int ignored = 0;   // the deposit flags cells off the node array
+  for (long base = (long)blockIdx.x * TPB; base < n; base += (long)gridDim.x * TPB) {
+    const long i = base + threadIdx.x;
+    const bool valid = i < n;
+    unsigned k = 0xffffffffu;
+    if (valid) {
+      const int ix = clamp_cell(cell_floor(x[i], g.xStart, g.invdx, g.nxn), g.nxn, ignored);
+      const int iy = clamp_cell(cell_floor(y[i], g.yStart, g.invdy, g.nyn), g.nyn, ignored);
+      const int iz = clamp_cell(cell_floor(z[i], g.zStart, g.invdz, g.nzn), g.nzn, ignored);
+      k = (unsigned)((ix * g.nyn + iy) * g.nzn + iz);
+      key[i] = k;
+    }
+    const unsigned peers = __match_any_sync(FULL, k);
+    if (valid && lane == __ffs(peers) - 1) atomicAdd(count + k, (unsigned)__popc(peers));
+  }
+}
+
+// ... an exclusive scan of the counts into the cells' first positions (three
+// passes over blocks of P2S_B) ...
+constexpr int P2S_B = 1024;
+__device__ __forceinline__ unsigned p2s_block_scan(unsigned v, unsigned *ws, unsigned &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned xs = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(FULL, xs, o);
+    if (lane >= o) xs += t;
+  }
+  if (lane == 31) ws[warp] = xs;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned s = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(FULL, s, o);
+      if (lane >= o) s += t;
+    }
+    ws[lane] = s;
+  }
+  __syncthreads();
+  const unsigned pre = warp ? ws[warp - 1] : 0u;
+  total = ws[31];
+  __syncthreads();
+  return pre + xs - v;
+}
+
+__global__ void __launch_bounds__(P2S_B) k_p2s_scan_blocks(const unsigned *in, long m,
+                                                           unsigned *out, unsigned *bsum) {
+  __shared__ unsigned ws[32];
+  const long i = blockIdx.x * (long)P2S_B + threadIdx.x;
+  unsigned total;
+  const unsigned ex = p2s_block_scan(i < m ? in[i] : 0u, ws, total);
+  if (i < m) out[i] = ex;
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(P2S_B) k_p2s_scan_sums(unsigned *bsum, int nb) {
+  __shared__ unsigned ws[32];
+  unsigned carry = 0;
+  for (int b = 0; b < nb; b += P2S_B) {
+    const int i = b + threadIdx.x;
+    unsigned total;
+    const unsigned ex = p2s_block_scan(i < nb ? bsum[i] : 0u, ws, total);
+    if (i < nb) bsum[i] = ex + carry;
+    carry += total;
+  }
+}
+
+__global__ void __launch_bounds__(P2S_B) k_p2s_scan_add(unsigned *out, long m,
+                                                        const unsigned *bsum) {
+  const long i = blockIdx.x * (long)P2S_B + threadIdx.x;
+  if (i < m) out[i] += bsum[blockIdx.x];
+}
+
+// ... and every index at its cell's next free position (cursor: the first
+// positions, advanced; the order inside a cell is the atomics').
+__global__ void __launch_bounds__(TPB) k_p2g_scatter(const unsigned *__restrict__ key, long n,
+                                                     unsigned *__restrict__ cursor,
+                                                     unsigned *__restrict__ perm) {
+  const int lane = threadIdx.x & 31;
+  for (long base = (long)blockIdx.x * TPB; base < n; base += (long)gridDim.x * TPB) {
+    const long i = base + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned k = valid ? key[i] : 0xffffffffu;
+    const unsigned peers = __match_any_sync(FULL, k);
+    const int leader = __ffs(peers) - 1;
+    unsigned first = 0;
+    if (valid && lane == leader) first = atomicAdd(cursor + k, (unsigned)__popc(peers));
+    first = __shfl_sync(FULL, first, leader);
+    if (valid) perm[first + __popc(peers & ((1u << lane) - 1u))] = (unsigned)i;
+  }
 }
 
 __global__ void __launch_bounds__(TPB) k_pack_fields(const float *__restrict__ ex,
@@ -699,6 +805,9 @@ __global__ void __launch_bounds__(TPB) k_bc_fold(Moments10 M, int nxn, int nyn, 
 
 inline unsigned blocks_for(long n) { return (unsigned)ceil_div(n, TPB); }
 
+// Deposits of at least this many particles sort them by cell first.
+constexpr long P2S_MIN = 65536;
+
 }  // namespace
 
 int launch_pack_fields(const float *const f[6], float4 *eb4, float2 *eb2, long nodes,
@@ -808,10 +917,40 @@ int launch_plain_p2g_into(const GeomDev &g, const float *x, const float *y, cons
   if (n <= 0) return SPB_OK;
   const DepTarget T = target(acc, mom);
   const unsigned chunks = (unsigned)ceil_div(n, GP_CHUNK);
+  // the particles in cell order first (above P2S_MIN; scratch from the
+  // device's pool, skipped if it cannot be had)
+  unsigned *scratch = nullptr, *perm = nullptr;
+  const long nodes = (long)g.nxn * g.nyn * g.nzn;
+  if (n >= P2S_MIN) {
+    const long nb = ceil_div(nodes, P2S_B);
+    keep_pool_memory();
+    const size_t words = (size_t)2 * n + 2 * nodes + nb;
+    if (cudaMallocAsync(reinterpret_cast<void **>(&scratch), words * sizeof(unsigned), s) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      scratch = nullptr;
+    }
+    if (scratch) {
+      unsigned *key = scratch, *pm = scratch + n, *count = pm + n, *first = count + nodes;
+      unsigned *bsum = first + nodes;
+      SPB_CUDA(cudaMemsetAsync(count, 0, nodes * sizeof(unsigned), s));
+      const unsigned blocks = (unsigned)std::min<long>(ceil_div(n, TPB), 148L * 16);
+      k_p2g_keys<<<blocks, TPB, 0, s>>>(g, x, y, z, n, key, count);
+      k_p2s_scan_blocks<<<(unsigned)nb, P2S_B, 0, s>>>(count, nodes, first, bsum);
+      k_p2s_scan_sums<<<1, P2S_B, 0, s>>>(bsum, (int)nb);
+      k_p2s_scan_add<<<(unsigned)nb, P2S_B, 0, s>>>(first, nodes, bsum);
+      k_p2g_scatter<<<blocks, TPB, 0, s>>>(key, n, first, pm);
+      SPB_CUDA(cudaGetLastError());
+      g_launches += 5;
+      perm = pm;
+    }
+  }
   if (acc)
-    k_plain_p2g_grouped<true><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
+    k_plain_p2g_grouped<true><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, perm, T, err);
   else
-    k_plain_p2g_grouped<false><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
+    k_plain_p2g_grouped<false><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, perm, T,
+                                                         err);
+  if (scratch) cudaFreeAsync(scratch, s);
   SPB_CUDA(cudaGetLastError());
   g_launches++;
   return SPB_OK;
