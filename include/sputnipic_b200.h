@@ -449,12 +449,19 @@ void spb_serve_destroy(spb_serve *srv);
  * queue (status not PENDING). Returns the job id (>= 0) or -status. */
 long spb_serve_submit(spb_serve *srv, const spb_job_desc *job, const float *const fields[6],
                       const float *const *parts, const long *counts, int on_device);
-/* Runs one cycle of every admitted job (and more for the cheap ones, see
- * extra_budget) while admitting the queued jobs that fit (in order of
- * arrival; they upload on a stream of their own and join the next step),
- * retires the jobs that reached their cycle count, and synchronises.
- * Returns the number of jobs admitted, or -status. */
+/* Launches one cycle of every admitted job (and more for the cheap ones, see
+ * extra_budget) and, while they run, admits the queued jobs that fit (in
+ * order of arrival; they upload on a stream of their own and join the next
+ * step). It waits for the previous step's launches, not its own, so the host
+ * prepares the next step while the device runs this one; a job whose last
+ * cycle is launched finishes (DONE, or FAILED with its error) once its work
+ * has completed, seen at a later step, or at this one when nothing else is
+ * left to run. Returns the number of jobs admitted and not yet finished, or
+ * -status. */
 int spb_serve_step(spb_serve *srv);
+/* Ids of the jobs that finished (DONE or FAILED) since the last call, at
+ * most max of them, oldest first; returns how many (or -status). */
+int spb_serve_finished(spb_serve *srv, long *ids, int max);
 /* SPB_JOB_*, or -1 for an unknown id. */
 int spb_serve_status(const spb_serve *srv, long id);
 /* Status code of a failed job (why it failed). */

@@ -277,6 +277,7 @@ def load():
     _proto(lib, "spb_serve_destroy", None, [P])
     _proto(lib, "spb_serve_submit", c_long, [P, R(JobDesc), P, P, P, c_int])
     _proto(lib, "spb_serve_step", c_int, [P])
+    _proto(lib, "spb_serve_finished", c_int, [P, ctypes.POINTER(c_long), c_int])
     _proto(lib, "spb_serve_status", c_int, [P, c_long])
     _proto(lib, "spb_serve_error", c_int, [P, c_long])
     _proto(lib, "spb_serve_result", c_int, [P, c_long, c_int] + [P] * 8 + [c_int])

@@ -38,12 +38,15 @@ struct ServeJob {
   int on_device = 0;
   long long bytes = 0;                // estimated footprint, held while admitted
   spb_sim *sim = nullptr;
-  int cycles = 0;
+  int cycles = 0;                     // cycles launched
   int state = SPB_JOB_PENDING;
   int error = SPB_OK;
   double t[3] = {-1.0, -1.0, -1.0};   // submitted, admitted, finished
+  cudaEvent_t done = nullptr;         // recorded after the job's last launch
   ~ServeJob() {
-    if (sim) spb_sim_destroy(sim);
+    // a released job's work is complete (its event was seen, or it never ran)
+    if (sim) spb::sim_free(sim, false);
+    if (done) cudaEventDestroy(done);
   }
 };
 
@@ -75,6 +78,7 @@ double seconds_since(Clock::time_point t0) {
 }  // namespace
 
 constexpr int SERVE_LAUNCHES = 8;   // launches per step at most
+constexpr int SERVE_ERR_SLOTS = 4096;   // pinned error words of jobs finishing
 
 struct spb_serve {
   spb_serve_desc d{};
@@ -90,7 +94,12 @@ struct spb_serve {
   int *h_ovf = nullptr;   // pinned: overflow counters of the admitted jobs' species
   Clock::time_point t0;
   std::deque<ServeJob *> pending;
-  std::vector<ServeJob *> active;
+  std::vector<ServeJob *> active;      // cycles left to launch
+  std::vector<ServeJob *> finishing;   // every cycle launched, not yet seen complete
+  std::vector<long> finished;          // ids done or failed since spb_serve_finished
+  int *h_err = nullptr;                // pinned: finishing jobs' error words (by id)
+  cudaEvent_t step_done[2] = {nullptr, nullptr};
+  bool step_pending[2] = {false, false};
   std::map<long, std::unique_ptr<ServeJob>> jobs;   // every job not yet released
 };
 
@@ -110,6 +119,31 @@ void fail_job(spb_serve *s, ServeJob *j, int status) {
   j->state = SPB_JOB_FAILED;
   j->error = status;
   j->t[2] = seconds_since(s->t0);
+  s->finished.push_back(j->id);
+}
+
+// Finishing jobs whose last launch has completed: done, or failed with their
+// error word's status. wait: block until every one has completed.
+int retire(spb_serve *s, bool wait) {
+  std::vector<ServeJob *> still;
+  for (ServeJob *j : s->finishing) {
+    const cudaError_t e = wait ? cudaEventSynchronize(j->done) : cudaEventQuery(j->done);
+    if (e == cudaErrorNotReady) {
+      still.push_back(j);
+      continue;
+    }
+    if (e != cudaSuccess) return fail_cuda(e, "serving: job completion");
+    const int rc = spb::sim_status(s->h_err[j->id % SERVE_ERR_SLOTS]);
+    if (rc) {
+      fail_job(s, j, rc);
+    } else {
+      j->state = SPB_JOB_DONE;
+      j->t[2] = seconds_since(s->t0);
+      s->finished.push_back(j->id);
+    }
+  }
+  s->finishing.swap(still);
+  return SPB_OK;
 }
 
 // Creates the job's simulation and uploads its fields and particles.
@@ -174,6 +208,8 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
   SPB_CUDA(cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking));
   SPB_CUDA(cudaEventCreateWithFlags(&s->adm_done, cudaEventDisableTiming));
   SPB_CUDA(cudaMallocHost(&s->h_ovf, (size_t)SERVE_MAX_JOBS * SPB_SIM_MAX_SPECIES * sizeof(int)));
+  SPB_CUDA(cudaMallocHost(&s->h_err, (size_t)SERVE_ERR_SLOTS * sizeof(int)));
+  for (auto &e : s->step_done) SPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   if (d.hbm_budget > 0) {
     s->budget = d.hbm_budget;
   } else {
@@ -196,7 +232,10 @@ extern "C" void spb_serve_destroy(spb_serve *s) {
   if (s->st) cudaStreamDestroy(s->st);
   if (s->adm) cudaStreamDestroy(s->adm);
   if (s->adm_done) cudaEventDestroy(s->adm_done);
+  for (cudaEvent_t e : s->step_done)
+    if (e) cudaEventDestroy(e);
   cudaFreeHost(s->h_ovf);
+  cudaFreeHost(s->h_err);
   delete s;
 }
 
@@ -258,6 +297,7 @@ extern "C" int spb_serve_step(spb_serve *s) {
       s->used += j->bytes;
       j->t[1] = seconds_since(s->t0);
       if (int rc = admit(s, j)) {
+        cudaStreamSynchronize(s->adm);   // nothing of the failed job may still run
         fail_job(s, j, rc);
         continue;
       }
@@ -267,16 +307,18 @@ extern "C" int spb_serve_step(spb_serve *s) {
     SPB_CUDA(cudaStreamWaitEvent(s->st, s->adm_done, 0));
     return SPB_OK;
   };
+  if (int rc = retire(s, false)) return -rc;
+  lap(3);
   std::vector<ServeJob *> joined;
   const bool idle = s->active.empty();
-  if (idle) {   // nothing running: the new jobs run in this step
+  if (idle) {   // nothing to launch: the new jobs run in this step
     if (int rc = admit_pending(joined)) return -rc;
     s->active.swap(joined);
     lap(0);
   }
   // overflow lists past their threshold: re-lay out those jobs (one
-  // synchronisation for all; the engine's stream is idle between steps)
-  if (!idle && s->steps > 0 && s->steps % s->d.check_every == 0) {
+  // synchronisation for all)
+  if (!s->active.empty() && s->steps > 0 && s->steps % s->d.check_every == 0) {
     int k = 0;
     for (ServeJob *j : s->active)
       for (const SimSpecies &q : j->sim->sp)
@@ -328,35 +370,58 @@ extern "C" int spb_serve_step(spb_serve *s) {
         budget -= spent;
       }
     }
+    // the jobs whose last cycle is launched: their error words come back
+    // and an event marks their completion
+    std::vector<ServeJob *> still;
+    for (ServeJob *j : ran) {
+      if (j->cycles < j->d.ncycles) {
+        still.push_back(j);
+        continue;
+      }
+      if (!j->done) SPB_CUDA(cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming));
+      SPB_CUDA(cudaMemcpyAsync(s->h_err + j->id % SERVE_ERR_SLOTS, j->sim->d_err, sizeof(int),
+                               cudaMemcpyDeviceToHost, s->st));
+      SPB_CUDA(cudaEventRecord(j->done, s->st));
+      s->finishing.push_back(j);
+    }
+    s->active.swap(still);
     s->steps++;
   }
   lap(2);
   // while the launches run: admit what fits; those jobs join the next step
   if (!idle) {
     if (int rc = admit_pending(joined)) return -rc;
+    s->active.insert(s->active.end(), joined.begin(), joined.end());
     lap(0);
   }
-  SPB_CUDA(cudaStreamSynchronize(s->st));
-  lap(2);
-  // retire the jobs that reached their cycle count
-  std::vector<ServeJob *> still;
-  for (ServeJob *j : ran) {
-    if (j->cycles < j->d.ncycles) {
-      still.push_back(j);
-      continue;
-    }
-    const int rc = spb_sim_check(j->sim, s->st);
-    j->t[2] = seconds_since(s->t0);
-    if (rc) {
-      fail_job(s, j, rc);
-    } else {
-      j->state = SPB_JOB_DONE;
-    }
+  // at most one step in flight beyond this one: wait for the previous step's
+  // launches, not for this step's, so the host prepares the next step while
+  // the GPU runs this one
+  const int cur = (int)(s->steps & 1);
+  if (!ran.empty()) {
+    if (s->step_pending[cur ^ 1]) SPB_CUDA(cudaEventSynchronize(s->step_done[cur ^ 1]));
+    SPB_CUDA(cudaEventRecord(s->step_done[cur], s->st));
+    s->step_pending[cur ^ 1] = false;
+    s->step_pending[cur] = true;
+  } else {
+    // nothing launched: wait for whatever is still finishing
+    SPB_CUDA(cudaStreamSynchronize(s->st));
+    s->step_pending[0] = s->step_pending[1] = false;
   }
-  still.insert(still.end(), joined.begin(), joined.end());
-  s->active.swap(still);
+  lap(2);
+  // with nothing else to launch or admit, wait for the finishing jobs (there
+  // is no next step to prepare meanwhile)
+  if (int rc = retire(s, ran.empty() || (s->active.empty() && s->pending.empty()))) return -rc;
   lap(3);
-  return (int)s->active.size();
+  return (int)(s->active.size() + s->finishing.size());
+}
+
+extern "C" int spb_serve_finished(spb_serve *s, long *ids, int max) {
+  if (!s || (max > 0 && !ids)) return -fail(SPB_ERR_INVALID, "spb_serve_finished: bad arguments");
+  const int n = std::min<int>(max, (int)s->finished.size());
+  for (int i = 0; i < n; ++i) ids[i] = s->finished[i];
+  s->finished.erase(s->finished.begin(), s->finished.begin() + n);
+  return n;
 }
 
 extern "C" int spb_serve_stats(const spb_serve *s, double out[5]) {

@@ -2814,14 +2814,23 @@ int run_cycle(spb_sim *s, const TileImpl *ti, cudaStream_t st) {
 
 }  // namespace
 
-extern "C" void spb_sim_destroy(spb_sim *s) {
+namespace spb {
+// Frees a simulation. sync: wait for the whole device first (queued work may
+// still read the memory returned); the serving engine passes false for jobs
+// whose work it knows to be complete.
+void sim_free(spb_sim *s, bool sync);
+}  // namespace spb
+
+extern "C" void spb_sim_destroy(spb_sim *s) { spb::sim_free(s, true); }
+
+void spb::sim_free(spb_sim *s, bool sync) {
   if (!s) return;
   drop_graphs(s);
   if (s->gstream) cudaStreamDestroy(s->gstream);
   for (cudaEvent_t e : s->gev)
     if (e) cudaEventDestroy(e);
   drain(s, nullptr, nullptr, nullptr, nullptr, nullptr);
-  cudaDeviceSynchronize();   // no queued work may still read the memory returned below
+  if (sync) cudaDeviceSynchronize();   // no queued work may still read the memory returned below
   for (auto &q : s->sp) {
     free_buckets(q);
     dfree(q.mom);
@@ -3069,13 +3078,10 @@ extern "C" int spb_sim_particles(spb_sim *s, int species, float *x, float *y, fl
   return rc;
 }
 
-extern "C" int spb_sim_check(spb_sim *s, void *stream) {
-  if (!s) return fail(SPB_ERR_INVALID, "spb_sim_check: null simulation");
-  SPB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
-  int h = 0;
-  SPB_CUDA(cudaMemcpy(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+namespace spb {
+// The status of a simulation's error word (0: SPB_OK).
+int sim_status(int h) {
   if (h) {
-    SPB_CUDA(cudaMemset(s->d_err, 0, sizeof(int)));
     if (h & ERRBIT_TIMEOUT) return fail(SPB_ERR_TIMEOUT, "a staged field tile never arrived (bounded wait)");
     if (h & ERRBIT_SMEM_ALIGN) return fail(SPB_ERR_UNSUPPORTED, "shared memory not 128-byte aligned for TMA");
     if (h & ERRBIT_INEXACT)
@@ -3087,4 +3093,14 @@ extern "C" int spb_sim_check(spb_sim *s, void *stream) {
     return fail(SPB_ERR_OUT_OF_GRID, "a particle left the node array and was clamped");
   }
   return SPB_OK;
+}
+}  // namespace spb
+
+extern "C" int spb_sim_check(spb_sim *s, void *stream) {
+  if (!s) return fail(SPB_ERR_INVALID, "spb_sim_check: null simulation");
+  SPB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  int h = 0;
+  SPB_CUDA(cudaMemcpy(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) SPB_CUDA(cudaMemset(s->d_err, 0, sizeof(int)));
+  return spb::sim_status(h);
 }

@@ -100,4 +100,10 @@ void pool_reserve(long long bytes);
 // each of zeroing, push and deposit; flips their buffer sets.
 int launch_jobs(spb_sim *const *sims, int n, JobBuffers &buf, cudaStream_t st);
 
+// Frees a simulation; sync = false when no queued work still uses it.
+void sim_free(spb_sim *s, bool sync);
+// The status (SPB_OK or SPB_ERR_*, recorded for spb_last_error) of a
+// simulation's device error word.
+int sim_status(int word);
+
 }  // namespace spb

@@ -103,9 +103,24 @@ class Server:
         n = self.lib.spb_serve_step(self.h)
         if n < 0:
             _lib.check(-n)
-        for jid in [j for j in self._inputs if self.status(j) != PENDING]:
-            del self._inputs[jid]   # admitted (or failed): inputs no longer read
+        self._steps = getattr(self, "_steps", 0) + 1
+        if self._steps % 8 == 0 or n == 0:
+            # admitted (or failed) jobs' inputs are no longer read
+            for jid in [j for j in self._inputs if self.status(j) != PENDING]:
+                del self._inputs[jid]
         return n
+
+    def finished(self) -> list:
+        """Ids of the jobs that finished (done or failed) since the last call."""
+        out = []
+        buf = (ctypes.c_long * 256)()
+        while True:
+            k = self.lib.spb_serve_finished(self.h, buf, 256)
+            if k < 0:
+                _lib.check(-k)
+            out.extend(buf[:k])
+            if k < 256:
+                return out
 
     def status(self, jid: int) -> int:
         return self.lib.spb_serve_status(self.h, jid)
@@ -175,10 +190,9 @@ def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
             time.sleep(min(idle_sleep, max(0.0, arrivals[i] - now)))
             continue
         server.step()
-        for jid, idx in list(live.items()):
+        for jid in server.finished():
+            idx = live[jid]
             st = server.status(jid)
-            if st not in (DONE, FAILED):
-                continue
             job = jobs[idx]
             res = {}
             if st == DONE and idx in keep:

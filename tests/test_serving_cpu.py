@@ -17,11 +17,13 @@ class FakeJob:
 
 class FakeServer:
     """Admits at most `slots` jobs; each step advances every admitted job one
-    cycle. Records the step at which each job was submitted and finished."""
+    cycle. Records the step at which each job was submitted and finished, and
+    reports the newly finished ids (finished())."""
 
     def __init__(self, slots=2):
         self.slots, self.t0, self.jobs, self.order, self.steps = slots, time.perf_counter(), {}, [], 0
         self.next_id = 0
+        self.newly_done = []
 
     def submit(self, job):
         jid = self.next_id
@@ -39,13 +41,19 @@ class FakeServer:
                 j["state"] = serve.ACTIVE
                 j["t"][1] = time.perf_counter() - self.t0
                 active.append(j)
-        for j in active:
-            j["left"] -= 1
-            if j["left"] == 0:
-                j["state"] = serve.DONE
-                j["t"][2] = time.perf_counter() - self.t0
+        for jid, j in self.jobs.items():
+            if j in active:
+                j["left"] -= 1
+                if j["left"] == 0:
+                    j["state"] = serve.DONE
+                    j["t"][2] = time.perf_counter() - self.t0
+                    self.newly_done.append(jid)
         self.steps += 1
         return sum(1 for j in self.jobs.values() if j["state"] == serve.ACTIVE)
+
+    def finished(self):
+        out, self.newly_done = self.newly_done, []
+        return out
 
     def status(self, jid):
         return self.jobs[jid]["state"] if jid in self.jobs else -1
