@@ -613,21 +613,47 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
             dropin.setZeroSpeciesDensities(ids[s])
             dropin.interpP2G(P[s], ids[s], grd, raise_on_error=True)
 
+    def timed(steps):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        return R.max_over_ranks(time.perf_counter() - t0, dist)
+
     for _ in range(max(1, args.warmup)):
         step()
     steps = max(2, min(args.steps, 5))
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    t = R.max_over_ranks(time.perf_counter() - t0, dist)
+    t = timed(steps)
+    out = {"value": R.aggregate_rate(sum(n), world, steps, t), "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
+           "ms_per_step": 1e3 * t / steps,
+           "path": "spb_mover_PC + spb_interpP2G on reference structs, COPY residency, "
+                   "pinned host arrays; timed on the host clock"}
+    # the same calls with the particles kept in HBM (spb_set_residency): every
+    # step still uploads each species' fields and moments and reads the
+    # moments back; the particles went up once, before the timed steps
     dropin.release_all()
-    return {"value": R.aggregate_rate(sum(n), world, steps, t), "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "steps": steps, "ms_per_step": 1e3 * t / steps,
-            "path": "spb_mover_PC + spb_interpP2G on reference structs, COPY residency, "
-                    "pinned host arrays; timed on the host clock"}
+    if dropin.set_residency(True) == 0:
+        try:
+            for _ in range(max(1, args.warmup)):
+                step()
+            steps_d = max(2, min(args.steps, 10))
+            td = timed(steps_d)
+            for s in range(ns):
+                dropin.sync_particles_to_host(P[s])
+        finally:
+            dropin.set_residency(False)
+        out["device_residency"] = {
+            "value": R.aggregate_rate(sum(n), world, steps_d, td), "unit": UNIT,
+            "h2d_bytes_per_step": ns * (24 * nodes + 40 * nodes),
+            "d2h_bytes_per_step": ns * 40 * nodes, "steps": steps_d,
+            "ms_per_step": 1e3 * td / steps_d,
+            "path": "the same calls in DEVICE residency: particles resident in HBM, per step each "
+                    "species' fields and moments uploaded and its moments read back"}
+    dropin.release_all()
+    return out
 
 
 def launch_ranks(n: int) -> int:

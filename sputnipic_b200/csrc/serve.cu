@@ -43,6 +43,7 @@ struct ServeJob {
   int error = SPB_OK;
   double t[3] = {-1.0, -1.0, -1.0};   // submitted, admitted, finished
   cudaEvent_t done = nullptr;         // recorded after the job's last launch
+  long ovf_step = -1;                 // step whose overflow counters were copied back
   ~ServeJob() {
     // a released job's work is complete (its event was seen, or it never ran)
     if (sim) spb::sim_free(sim, false);
@@ -91,7 +92,7 @@ struct spb_serve {
   long next_id = 0;
   long steps = 0;
   double phase_s[4] = {0, 0, 0, 0};   // admit, overflow checks, launch + wait, retire
-  int *h_ovf = nullptr;   // pinned: overflow counters of the admitted jobs' species
+  int *h_ovf = nullptr;   // pinned: overflow counters of the jobs' species (by id)
   Clock::time_point t0;
   std::deque<ServeJob *> pending;
   std::vector<ServeJob *> active;      // cycles left to launch
@@ -207,7 +208,7 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
   SPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   SPB_CUDA(cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking));
   SPB_CUDA(cudaEventCreateWithFlags(&s->adm_done, cudaEventDisableTiming));
-  SPB_CUDA(cudaMallocHost(&s->h_ovf, (size_t)SERVE_MAX_JOBS * SPB_SIM_MAX_SPECIES * sizeof(int)));
+  SPB_CUDA(cudaMallocHost(&s->h_ovf, (size_t)SERVE_ERR_SLOTS * SPB_SIM_MAX_SPECIES * sizeof(int)));
   SPB_CUDA(cudaMallocHost(&s->h_err, (size_t)SERVE_ERR_SLOTS * sizeof(int)));
   for (auto &e : s->step_done) SPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   if (d.hbm_budget > 0) {
@@ -316,23 +317,18 @@ extern "C" int spb_serve_step(spb_serve *s) {
     s->active.swap(joined);
     lap(0);
   }
-  // overflow lists past their threshold: re-lay out those jobs (one
-  // synchronisation for all)
-  if (!s->active.empty() && s->steps > 0 && s->steps % s->d.check_every == 0) {
-    int k = 0;
-    for (ServeJob *j : s->active)
-      for (const SimSpecies &q : j->sim->sp)
-        SPB_CUDA(cudaMemcpyAsync(s->h_ovf + k++, q.ocnt + q.cur, sizeof(int),
-                                 cudaMemcpyDeviceToHost, s->st));
-    SPB_CUDA(cudaStreamSynchronize(s->st));
-    k = 0;
-    for (ServeJob *j : s->active) {
-      bool over = false;
-      for (size_t i = 0; i < j->sim->sp.size(); ++i)
-        over |= s->h_ovf[k++] > spb::relayout_threshold(j->sim->sp[i]);
-      if (over)
-        if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
-    }
+  // overflow lists past their threshold (counters copied back after an
+  // earlier check step, whose launches have completed by now): re-lay out
+  // those jobs, in stream order
+  for (ServeJob *j : s->active) {
+    if (j->ovf_step < 0 || s->steps < j->ovf_step + 2) continue;
+    const int *h = s->h_ovf + (j->id % SERVE_ERR_SLOTS) * SPB_SIM_MAX_SPECIES;
+    bool over = false;
+    for (size_t i = 0; i < j->sim->sp.size(); ++i)
+      over |= h[i] > spb::relayout_threshold(j->sim->sp[i]);
+    j->ovf_step = -1;
+    if (over)
+      if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
   }
   lap(1);
   // this step's launches (asynchronous): one cycle of every admitted job,
@@ -371,10 +367,19 @@ extern "C" int spb_serve_step(spb_serve *s) {
       }
     }
     // the jobs whose last cycle is launched: their error words come back
-    // and an event marks their completion
+    // and an event marks their completion; every check_every steps the
+    // others' overflow counters come back too
+    const bool check = s->steps % s->d.check_every == 0;
     std::vector<ServeJob *> still;
     for (ServeJob *j : ran) {
       if (j->cycles < j->d.ncycles) {
+        if (check && j->ovf_step < 0) {
+          int *h = s->h_ovf + (j->id % SERVE_ERR_SLOTS) * SPB_SIM_MAX_SPECIES;
+          for (size_t i = 0; i < j->sim->sp.size(); ++i)
+            SPB_CUDA(cudaMemcpyAsync(h + i, j->sim->sp[i].ocnt + j->sim->sp[i].cur, sizeof(int),
+                                     cudaMemcpyDeviceToHost, s->st));
+          j->ovf_step = s->steps;
+        }
         still.push_back(j);
         continue;
       }
