@@ -978,21 +978,6 @@ __device__ __forceinline__ void ld_rec_cg(const float4 *p, float4 &a, float4 &b)
       : "l"(p));
 }
 
-// Records per L2 prefetch of a bucket walk, and how far ahead of the walk's
-// loads the prefetches run (one to two such chunks).
-constexpr int PF_RECORDS = 8;
-
-// Asks L2 for records [i, min(i + n, cnt)) of a bucket without waiting: one
-// bulk prefetch, carried out by the SM's copy engine. Records are 32 bytes,
-// so the range starts and ends on the 16-byte boundaries it needs; a range
-// past the bucket's count is cut to it (nothing outside the bucket is read).
-__device__ __forceinline__ void prefetch_records(const float4 *rec, int i, int n, int cnt) {
-  const int e = min(i + n, cnt);
-  if (i < e)
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rec + 2 * i),
-                 "r"((e - i) * 32));
-}
-
 template <bool COH>
 __device__ __forceinline__ void ld_record(const float4 *p, float4 &a, float4 &b) {
   if constexpr (COH)
@@ -1064,14 +1049,12 @@ __device__ __forceinline__ void deposit_tile(const CycleParams &P, int tile, flo
 #pragma unroll
     for (int i = 0; i < 40; ++i) acc[i] = make_float2(0.f, 0.f);
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, a1 = a, b1 = a;
-    prefetch_records(rec, 0, 2 * PF_RECORDS, cnt);
     if (n1 > 0) ld_record<COH>(rec, a, b);
     if (n1 > 1) ld_record<COH>(rec + 2, a1, b1);
 #pragma unroll 1
     for (int k = 0; k < trips; ++k) {
-      // two records in flight while this one is summed, and L2 asked for
-      // the next one to two chunks; lanes past their count add zero terms
-      if (k > 0 && k % PF_RECORDS == 0) prefetch_records(rec, k + PF_RECORDS, PF_RECORDS, cnt);
+      // two records in flight while this one is summed; lanes past their
+      // count add zero terms
       float4 na = a1, nb = b1;
       if (k + 2 < n1) ld_record<COH>(rec + 2 * (k + 2), na, nb);
       add_terms(acc, k < n1 ? a.w : 0.0f, a.x, a.y, a.z, b.x, b.y, b.z, 0);
@@ -1176,12 +1159,10 @@ __device__ __forceinline__ void deposit_tile_exact(const CycleParams &P, int til
 #pragma unroll
     for (int i = 0; i < 80; ++i) acc[i] = M[(i % 10) == 0 ? 0 : ((i % 10) < 4 ? 1 : 2)];
     float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, a1 = a, b1 = a;
-    prefetch_records(rec, 0, 2 * PF_RECORDS, cnt);
     if (cnt > 0) ld_rec(rec, a, b);
     if (cnt > 1) ld_rec(rec + 2, a1, b1);
 #pragma unroll 1
     for (int k = 0; k < cnt; ++k) {
-      if (k > 0 && k % PF_RECORDS == 0) prefetch_records(rec, k + PF_RECORDS, PF_RECORDS, cnt);
       float4 na = a1, nb = b1;
       if (k + 2 < cnt) ld_rec(rec + 2 * (k + 2), na, nb);
       float W[8], mf[10];
