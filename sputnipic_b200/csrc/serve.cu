@@ -201,10 +201,10 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
     cudaGetLastError();
     return fail(SPB_ERR_NO_DEVICE, "no CUDA device");
   }
+  if (d.extra_budget == 0.0) d.extra_budget = 1.0;
   auto s = std::make_unique<spb_serve>();
   s->d = d;
   SPB_CUDA(cudaGetDevice(&s->device));
-  if (d.extra_budget == 0.0) d.extra_budget = 1.0;
   SPB_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   SPB_CUDA(cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking));
   SPB_CUDA(cudaEventCreateWithFlags(&s->adm_done, cudaEventDisableTiming));
