@@ -408,15 +408,14 @@ __device__ __forceinline__ Particle smem_particle(const GroupSmem &S, int j) {
   return Particle{S.p[0][j], S.p[1][j], S.p[2][j], S.p[3][j], S.p[4][j], S.p[5][j], S.p[6][j]};
 }
 
-// perm (may be null): the particles in cell order (k_p2g_scatter), so that a
-// chunk holds whole cells whatever the order of the arrays.
+// (Particles in the arrays' own order; cell-ordered input goes through
+// k_plain_p2g_runs instead.)
 template <bool ACC>
 __global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
     GeomDev g, const float *__restrict__ x, const float *__restrict__ y,
     const float *__restrict__ z, const float *__restrict__ u, const float *__restrict__ v,
     const float *__restrict__ w, const float *__restrict__ q, long n,
-    const unsigned *__restrict__ perm, const __grid_constant__ DepTarget T,
-    int *__restrict__ err) {
+    const __grid_constant__ DepTarget T, int *__restrict__ err) {
   __shared__ GroupSmem S;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long base = (long)blockIdx.x * GP_CHUNK;
@@ -433,7 +432,7 @@ __global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
     const bool valid = j < cnt;
     int key = -1;
     if (valid) {
-      const long i = perm ? (long)perm[base + j] : base + j;
+      const long i = base + j;
 #pragma unroll
       for (int a = 0; a < 7; ++a) S.p[a][j] = src[a][i];
       const int ix = clamp_cell(cell_floor(S.p[0][j], g.xStart, g.invdx, g.nxn), g.nxn, bad);
@@ -540,6 +539,166 @@ __global__ void __launch_bounds__(GP_TPB) k_plain_p2g_grouped(
 #pragma unroll
     for (int i = 0; i < 5; ++i)
       if (i >= lo && i < hi) dep_add<ACC>(T, node, mbase + i, r[i]);
+  }
+  if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
+}
+
+// The plain deposit over particles in cell order (a permutation from the cell
+// sort below). A CTA takes a chunk of RUN_CHUNK consecutive positions of the
+// permutation; while loading them it computes each particle's deposit cell
+// and its six node distances (xi0 = x - xn[ix-1], xi1 = xn[ix] - x, and so
+// on, src/Mover.cpp:399-410) once, into shared memory with u, v, w, q. Each
+// warp then takes an equal slice of the chunk: in the slice the particles of
+// one cell form runs, and a run of four or more is deposited as one group
+// (run_terms for both x halves, one warp reduction, 80 adds), shorter runs
+// particle by particle. A run that a slice or chunk boundary cuts is
+// deposited in parts.
+constexpr int RUN_TPB = 256;
+constexpr int RUN_PER_THREAD = 4;
+constexpr int RUN_CHUNK = RUN_TPB * RUN_PER_THREAD;
+static_assert(RUN_CHUNK == GP_CHUNK, "one grid size for both deposit kernels");
+
+struct RunSmem {
+  float d[10][RUN_CHUNK];   // xi0, xi1, eta0, eta1, zeta0, zeta1, u, v, w, q
+  int key[RUN_CHUNK];       // node-space cell
+};
+
+// half_terms from the stored node distances of particle j: the same 40
+// summands, bit for bit (each product in the reference's order; pairs of
+// independent products issued as one packed FP32x2 multiply).
+template <bool ADD>
+__device__ __forceinline__ void run_terms(const GeomDev &g, const RunSmem &S, int j,
+                                          float2 (&t)[20], int lane, int a) {
+  const bool pb = lane & 8, pc = lane & 4;
+  const float xi0 = S.d[0][j], xi1 = S.d[1][j], eta0 = S.d[2][j], eta1 = S.d[3][j];
+  const float zeta0 = S.d[4][j], zeta1 = S.d[5][j];
+  const float u = S.d[6][j], v = S.d[7][j], w = S.d[8][j], q = S.d[9][j];
+  const float xia = (a ^ ((lane >> 4) & 1)) ? xi1 : xi0;
+  const float eta[2] = {pb ? eta1 : eta0, pb ? eta0 : eta1};
+  const float2 zeta = pc ? make_float2(zeta1, zeta0) : make_float2(zeta0, zeta1);
+  const float2 uu_vv = __fmul2_rn(make_float2(u, v), make_float2(u, v));
+  const float2 uv_vw = __fmul2_rn(make_float2(u, v), make_float2(v, w));
+  const float2 uw_ww = __fmul2_rn(make_float2(u, w), make_float2(w, w));
+  // factor pairs (moment k, moment k + 5); rhon's (1 * wgt) * inv is the
+  // reference's wgt * inv exactly
+  const float2 f[5] = {make_float2(1.0f, uv_vw.x), make_float2(u, uw_ww.x),
+                       make_float2(v, uu_vv.y), make_float2(w, uv_vw.y),
+                       make_float2(uu_vv.x, uw_ww.y)};
+  const float2 inv = make_float2(g.invVOL, g.invVOL);
+  const float qx = q * xia;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const float qxe = qx * eta[b];
+    // ((q * xi * eta) * zeta) * invVOL for both z nodes
+    const float2 wgt = __fmul2_rn(__fmul2_rn(make_float2(qxe, qxe), zeta), inv);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float wc = c ? wgt.y : wgt.x;
+      const float2 w2 = make_float2(wc, wc);
+      float2 *o = t + (b * 2 + c) * 5;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float2 n = __fmul2_rn(__fmul2_rn(f[k], w2), inv);
+        o[k] = ADD ? __fadd2_rn(o[k], n) : n;
+      }
+    }
+  }
+}
+
+// deposit_lone from the stored node distances of particle j (all 32 lanes
+// call with the same j and key).
+template <bool ACC>
+__device__ __forceinline__ void run_lone(const GeomDev &g, const DepTarget &T, const RunSmem &S,
+                                         int j, int key) {
+  const int lane = threadIdx.x & 31;
+  const int sx = g.nyn * g.nzn, sy = g.nzn;
+  if (lane >= 24) return;
+  const int node = lane / 3, grp = lane % 3;
+  const int a = node >> 2, b = (node >> 1) & 1, c = node & 1;
+  const float inv = g.invVOL, u = S.d[6][j], v = S.d[7][j], w = S.d[8][j];
+  const float wgt = S.d[9][j] * S.d[a][j] * S.d[2 + b][j] * S.d[4 + c][j] * inv;
+  const float f0 = grp == 0 ? 1.0f : (grp == 1 ? u * u : v * w);
+  const float f1 = grp == 0 ? u : (grp == 1 ? u * v : w * w);
+  const float f2 = grp == 0 ? v : (grp == 1 ? u * w : 0.0f);
+  const float f3 = grp == 0 ? w : (grp == 1 ? v * v : 0.0f);
+  dep_add4<ACC>(T, key - a * sx - b * sy - c, grp, (f0 * wgt) * inv, (f1 * wgt) * inv,
+                (f2 * wgt) * inv, (f3 * wgt) * inv);
+}
+
+template <bool ACC>
+__global__ void __launch_bounds__(RUN_TPB, 3) k_plain_p2g_runs(
+    GeomDev g, const float *__restrict__ x, const float *__restrict__ y,
+    const float *__restrict__ z, const float *__restrict__ u, const float *__restrict__ v,
+    const float *__restrict__ w, const float *__restrict__ q, long n,
+    const unsigned *__restrict__ perm, const __grid_constant__ DepTarget T,
+    int *__restrict__ err) {
+  __shared__ RunSmem S;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long base = (long)blockIdx.x * RUN_CHUNK;
+  const int cnt = (int)min((long)RUN_CHUNK, n - base);
+  int bad = 0;
+#pragma unroll
+  for (int r = 0; r < RUN_PER_THREAD; ++r) {
+    const int j = tid + r * RUN_TPB;
+    if (j < cnt) {
+      const long i = perm[base + j];
+      const float px = x[i], py = y[i], pz = z[i];
+      const int ix = clamp_cell(cell_floor(px, g.xStart, g.invdx, g.nxn), g.nxn, bad);
+      const int iy = clamp_cell(cell_floor(py, g.yStart, g.invdy, g.nyn), g.nyn, bad);
+      const int iz = clamp_cell(cell_floor(pz, g.zStart, g.invdz, g.nzn), g.nzn, bad);
+      S.key[j] = (ix * g.nyn + iy) * g.nzn + iz;
+      S.d[0][j] = px - __ldg(g.xn + ix - 1);
+      S.d[1][j] = __ldg(g.xn + ix) - px;
+      S.d[2][j] = py - __ldg(g.yn + iy - 1);
+      S.d[3][j] = __ldg(g.yn + iy) - py;
+      S.d[4][j] = pz - __ldg(g.zn + iz - 1);
+      S.d[5][j] = __ldg(g.zn + iz) - pz;
+      S.d[6][j] = u[i];
+      S.d[7][j] = v[i];
+      S.d[8][j] = w[i];
+      S.d[9][j] = q[i];
+    }
+  }
+  __syncthreads();
+  const int sx = g.nyn * g.nzn, sy = g.nzn;
+  const int na = (lane >> 4) & 1, nb = (lane >> 3) & 1, nc = (lane >> 2) & 1;
+  const int mbase = 5 * ((lane >> 1) & 1);
+  const int lo = (lane & 1) ? 3 : 0, hi = (lane & 1) ? 5 : 3;
+  constexpr int PW = RUN_CHUNK / (RUN_TPB / 32);   // positions per warp
+  const int jend = min((warp + 1) * PW, cnt);
+#pragma unroll 1
+  for (int j = warp * PW; j < jend;) {
+    // the run of key S.key[j]: up to the first position with another key
+    const int key = S.key[j];
+    int e = jend;
+#pragma unroll 1
+    for (int b = j + 1; b < jend; b += 32) {
+      const int t = b + lane;
+      const unsigned m = __ballot_sync(FULL, t < jend && S.key[t] != key);
+      if (m) {
+        e = b + __ffs(m) - 1;
+        break;
+      }
+    }
+    const int c = e - j;
+    if (c <= 3) {
+      for (int m = 0; m < c; ++m) run_lone<ACC>(g, T, S, j + m, key);
+    } else {
+      float2 t[20];
+#pragma unroll
+      for (int i = 0; i < 20; ++i) t[i] = make_float2(0.0f, 0.0f);
+      for (int m = lane; m < c; m += 32) run_terms<true>(g, S, j + m, t, lane, 1);
+#pragma unroll
+      for (int i = 0; i < 20; ++i) t[i] = shfl_xor2(t[i], 16);
+      for (int m = lane; m < c; m += 32) run_terms<true>(g, S, j + m, t, lane, 0);
+      float r[5];
+      warp_sum80_tail(t, r, lane);
+      const int node = key - na * sx - nb * sy - nc;
+#pragma unroll
+      for (int i = 0; i < 5; ++i)
+        if (i >= lo && i < hi) dep_add<ACC>(T, node, mbase + i, r[i]);
+    }
+    j = e;
   }
   if (bad) atomicOr(err, ERRBIT_OUT_OF_GRID);
 }
@@ -945,11 +1104,14 @@ int launch_plain_p2g_into(const GeomDev &g, const float *x, const float *y, cons
       perm = pm;
     }
   }
-  if (acc)
-    k_plain_p2g_grouped<true><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, perm, T, err);
+  if (perm && acc)
+    k_plain_p2g_runs<true><<<chunks, RUN_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, perm, T, err);
+  else if (perm)
+    k_plain_p2g_runs<false><<<chunks, RUN_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, perm, T, err);
+  else if (acc)
+    k_plain_p2g_grouped<true><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
   else
-    k_plain_p2g_grouped<false><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, perm, T,
-                                                         err);
+    k_plain_p2g_grouped<false><<<chunks, GP_TPB, 0, s>>>(g, x, y, z, u, v, w, q, n, T, err);
   if (scratch) cudaFreeAsync(scratch, s);
   SPB_CUDA(cudaGetLastError());
   g_launches++;

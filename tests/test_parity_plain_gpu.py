@@ -368,6 +368,53 @@ def test_device_p2g_into_separate_moment_arrays(cuda, orc32, orc64, deposit_mode
     ctx.close()
 
 
+def test_device_p2g_clumped_shuffled_input(cuda, orc32, orc64, deposit_mode):
+    """spb_grid_p2g above the size where the deposit sorts its particles by
+    cell first (442K particles): a third of them in one cell (a run longer
+    than a CTA's chunk, split over warps and CTAs), the arrays in a seeded
+    random order. Nodes the clump does not reach: within the reordering
+    bound of the FP32 oracle. The clump's 8 nodes: a sequential FP32 sum of
+    147K terms is itself far from exact there (the reference code's own
+    result is up to 4 x 32 eps sum|terms| from the FP64 oracle), so they are
+    held to the FP64 oracle within 128 eps sum|terms|; a run deposited twice
+    or dropped would be off by 1/1150 of the node's value, over 50x that."""
+    torch = cuda
+    from sputnipic_b200.device import GridContext
+    wl = W.small_gem()
+    setup = oracle.setup_from(wl)
+    ctx = GridContext(wl)
+    ctx.set_fields([torch.from_numpy(f).cuda() for f in W.gem_fields(wl)])
+    a, b = W.gem_particles(wl, 0), W.gem_particles(wl, 1)
+    host = {k: np.concatenate([a[k], b[k]]) for k in "xyzuvwq"}
+    n = len(host["x"])
+    assert n > 400_000
+    rng = np.random.default_rng(5)
+    clump = rng.choice(n, n // 3, replace=False)
+    for k, c, d in (("x", 17, wl.dx), ("y", 9, wl.dy), ("z", 4, wl.dz)):
+        host[k][clump] = ((c + rng.uniform(0.05, 0.95, len(clump))) * d).astype(np.float32)
+    order = rng.permutation(n)
+    host = {k: np.ascontiguousarray(v[order]) for k, v in host.items()}
+    mom = torch.zeros(10, wl.nodes, device="cuda")
+    ctx.p2g({k: torch.from_numpy(v).cuda() for k, v in host.items()}, mom)
+    assert ctx.check() == 0
+    m32 = [np.zeros(wl.nodes, np.float32) for _ in range(10)]
+    orc32.interp_p2g(setup, host, m32)
+    m64 = [np.zeros(wl.nodes) for _ in range(10)]
+    orc64.interp_p2g(setup, {k: v.astype(np.float64) for k, v in host.items()}, m64)
+    absm = abs_moments(orc64, setup, wl, host)
+    gpu = mom.cpu().numpy().astype(np.float64)
+    clumped = np.zeros(wl.nodes, bool)
+    cell = {k: ((c + 0.5) * d) for k, c, d in (("x", 17, wl.dx), ("y", 9, wl.dy), ("z", 4, wl.dz))}
+    one = {k: np.array([cell[k] if k in cell else 1.0], np.float32) for k in "xyzuvwq"}
+    probe = abs_moments(orc64, setup, wl, one)
+    clumped[(probe != 0).any(axis=0)] = True
+    assert clumped.sum() == 8
+    check_moments(gpu[:, ~clumped], np.stack(m32)[:, ~clumped], absm[:, ~clumped])
+    err = np.abs(gpu[:, clumped] - np.stack(m64)[:, clumped])
+    assert (err <= 128 * EPS32 * absm[:, clumped]).all(), (err / (EPS32 * absm[:, clumped])).max()
+    ctx.close()
+
+
 @pytest.mark.parametrize("residency", ["copy", "device"])
 def test_interp_all_species_matches_driver_section(orc32, orc64, residency):
     """spb_interp_all_species against the reference driver's moment section
