@@ -301,7 +301,10 @@ typedef struct spb_sim_desc {
                                (2^-38 of the species' largest possible term of
                                that moment at load: |q|max for rhon, |q|max x
                                4 |v|max for J, |q|max x 16 |v|max^2 for the
-                               pressures; the rounding's average loss,
+                               pressures, |v|max the largest velocity
+                               component at load but at least c/8, so that a
+                               species loaded at rest keeps room for the
+                               velocities it gains; the rounding's average loss,
                                half a grid step per term, is added back) and
                                summed exactly
                                in FP64, so the moments do not depend on the
@@ -418,13 +421,14 @@ typedef struct spb_serve_desc {
                                (0: none), so that admitting jobs maps nothing;
                                spb_release_cached_memory gives it back */
   double extra_budget;      /* after a step's launch of every admitted job,
-                               further launches give jobs with cycles left
-                               more cycles, the cheapest jobs first (cost of a
-                               cycle: particles + 4 x cells), while the added
-                               cost stays within this fraction of the first
-                               launch's (at most 7 further launches): small
-                               jobs then finish in a few steps instead of being
-                               paced by the largest. 0: 1.0; negative: one
+                               up to 7 further launches: each gives one more
+                               cycle to every job with cycles left whose cost
+                               still fits (cost of a cycle: particles + 4 x
+                               cells; cheapest jobs first), while the added
+                               cost stays within this multiple of the first
+                               launch's. Once the largest job no longer fits,
+                               the smaller ones keep getting cycles, so they
+                               are not paced by it. 0: 1.0; negative: one
                                cycle per job and step */
 } spb_serve_desc;
 

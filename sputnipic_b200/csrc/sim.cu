@@ -897,7 +897,7 @@ __device__ __noinline__ void deposit_global(const CycleParams &P, const SpeciesD
 // particles in their buckets or of the atomics. Q = 2^(ceil(log2 T) - 38)
 // with T the species' largest possible term of that moment at load: max|q|
 // for rhon, max|q| x 4 vmax for Jx..Jz, max|q| x 16 vmax^2 for pxx..pzz
-// (vmax the largest velocity component): 2^-38 T resolution, 2^13 T headroom
+// (vmax the largest velocity component, at least c/8): 2^-38 T resolution, 2^13 T headroom
 // per cell and 2^15 T per node. Rounding down loses Q/2 per term on average,
 // which over a node's N terms would be N Q/2, comparable to a cancelling sum
 // (~sqrt(N) of its terms, each far below T): every term's Q/2 is added back
@@ -2374,7 +2374,12 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
     float qmax, vmax;
     std::memcpy(&qmax, &h[0], sizeof(float));
     std::memcpy(&vmax, &h[1], sizeof(float));
-    const double qm = std::max((double)qmax, 1e-300), vm = std::max((double)vmax, 1e-30);
+    // |v|max at least c/8, so that a species loaded at rest keeps room for
+    // the velocities it gains: a cell's sums have 2^13 T of room, so with 128
+    // particles in a cell its pressure terms may grow to 64 T (velocities to
+    // 8 x the bound) before a sum leaves its exact range
+    const double qm = std::max((double)qmax, 1e-300);
+    const double vm = std::max((double)vmax, std::max(s->d.c / 8.0, 1e-30));
     const double T[3] = {qm, qm * 4.0 * vm, qm * 16.0 * vm * vm};
     for (int k = 0; k < 3; ++k)
       q.quantum[k] = std::ldexp(1.0, (int)std::ceil(std::log2(T[k])) - 38);

@@ -96,3 +96,57 @@ def test_deterministic_moments_match_oracle_and_default(cuda):
         # exact sums of the same FP32 terms: no less accurate than the default
         # deposit's FP32 cell sums
         assert err[True].max() <= err[False].max() + 1e-8, (s, err[True], err[False])
+
+
+def test_species_loaded_at_rest_stays_exact(cuda):
+    """Every particle at rest when loaded (the velocity bound of the grids
+    falls back to c/8): six cycles of the small GEM configuration accelerate
+    them without any sum leaving its exact range, and two runs agree
+    bitwise."""
+    torch = cuda
+    wl = W.small_gem(E_amp=1e-3)
+    fields = [torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in W.gem_fields(wl)]
+    out = []
+    for _ in range(2):
+        from sputnipic_b200.sim import Simulation
+        sim = Simulation(wl, resort_every=2, graph=True, deterministic=True)
+        sim.set_fields(fields)
+        for s in range(len(wl.species)):
+            p = W.gem_particles(wl, s)
+            for k in "uvw":
+                p[k] = np.zeros_like(p[k])
+            sim.load_species(s, {k: torch.from_numpy(np.ascontiguousarray(p[k])).cuda()
+                                 for k in "xyzuvwq"})
+        sim.cycle(6)
+        assert sim.check() == 0
+        mom = [sim.moments(s).cpu().numpy() for s in range(len(wl.species))]
+        assert np.abs(mom[0][1:4]).max() > 0   # the electrons carry current
+        out.append(mom)
+        sim.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+@pytest.mark.parametrize("n, flagged", [(24000, True), (12000, False)])
+def test_cell_sum_past_exact_range_is_reported(cuda, n, flagged):
+    """n particles at rest near the lower corner of one cell, charge -1e-3
+    (max|q| = 1e-3, grid 2^-38 x 2^-9): that cell's rhon sum at the corner node
+    is about 0.86 n x 1e-3, against the exact range of 2^13 x 2^-9 = 16. 24,000
+    particles (about 20.6) leave it and spb_sim_check reports SPB_ERR_CAPACITY;
+    12,000 (about 10.3) stay inside."""
+    torch = cuda
+    from sputnipic_b200.sim import Simulation
+    wl = W.small_gem(E_amp=1e-3)
+    sim = Simulation(wl.with_(species=wl.species[:1]), resort_every=10**6, deterministic=True)
+    sim.set_fields([torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in W.gem_fields(wl)])
+    cell = (11, 7, 5)
+    d = {k: torch.full((n,), float((c + 0.05) * h), dtype=torch.float32, device="cuda")
+         for k, c, h in zip("xyz", cell, (wl.dx, wl.dy, wl.dz))}
+    for k in "uvw":
+        d[k] = torch.zeros(n, dtype=torch.float32, device="cuda")
+    d["q"] = torch.full((n,), -1e-3, dtype=torch.float32, device="cuda")
+    sim.load_species(0, d)
+    sim.cycle(1)
+    assert sim.check() == (8 if flagged else 0)   # SPB_ERR_CAPACITY
+    sim.close()
+

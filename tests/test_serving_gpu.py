@@ -125,6 +125,50 @@ def test_particles_in_mix_vs_fp64(cuda, orc64):
                 assert np.abs(got[k][order].astype(np.float64) - ref[k]).max() <= 1e-5 * scale
 
 
+def steps_to_finish(torch, specs, watch, **server_kw):
+    """Submits every spec at step 0 and steps until job `watch` is DONE.
+    Returns the steps taken and that job's results (species 0)."""
+    from sputnipic_b200.serve import DONE, Server
+    srv = Server(**server_kw)
+    jobs = [make_job(torch, wl, nc, sp) for wl, nc, sp in specs]
+    ids = [srv.submit(j) for j in jobs]
+    steps = 0
+    while srv.status(ids[watch]) != DONE:
+        srv.step()
+        steps += 1
+        assert steps < 200
+    wl = jobs[watch].wl
+    res = {k: v.cpu().numpy() for k, v in
+           srv.result(ids[watch], 0, jobs[watch].parts[0]["x"].numel(), wl.nodes).items()}
+    srv.close()
+    return steps, res
+
+
+def test_extra_cycles_for_cheap_jobs(cuda, orc64):
+    """A 40-cycle 16x8x8 job (16K particles) beside a 40-cycle 32x16x16 one
+    (884K). Each further launch of a step gives one more cycle to every job
+    with cycles left whose cost still fits the budget, cheapest first: with
+    the default budget (0, read as 1.0 x the first launch's cost) one such
+    launch fits both jobs (two cycles a step); with 8.0 all seven further
+    launches do (eight cycles a step); with extra cycles off (negative) each
+    job gets one cycle a step. The cheap job's moments are the same in all
+    three, within 1e-5 of the FP64 oracle."""
+    torch = cuda
+    cheap = W.small_gem(nxc=16, nyc=8, nzc=8, E_amp=1e-3, species=W.gem_species((8, 8, 8, 8)))
+    big = W.small_gem(E_amp=1e-3)
+    specs = [(big, 40, [0, 1, 2, 3]), (cheap, 40, [0, 1])]
+    steps, res = {}, {}
+    for budget in (0.0, 8.0, -1.0):
+        steps[budget], res[budget] = steps_to_finish(torch, specs, 1, extra_budget=budget)
+    assert steps[8.0] <= 7, steps
+    assert 20 <= steps[0.0] <= 22, steps
+    assert steps[-1.0] >= 40, steps
+    _, m64 = oracle_run(orc64, cheap, W.gem_particles(cheap, 0), cheap.species[0].qom, 40)
+    for budget in res:
+        assert (rel_l2(res[budget]["moments"], res[-1.0]["moments"]) <= 1e-5).all(), budget
+        assert (rel_l2(res[budget]["moments"], m64) <= 1e-5).all(), budget
+
+
 def test_admission_waits_for_budget(cuda):
     torch = cuda
     from sputnipic_b200.serve import ACTIVE, PENDING, Server
