@@ -2,8 +2,9 @@
 different grids and particle counts (spb_serve_* of libsputnipic_b200.so).
 
 A `Server` queues jobs as they arrive, admits them when their HBM footprint
-fits, and steps every admitted job one cycle per `step()` in one launch per
-kernel. `run_stream` is the request loop: it submits jobs at their arrival
+fits, and advances every admitted job at least one cycle per `step()` (one
+launch per kernel for all of them, and further launches that give cheap jobs
+more cycles within the engine's extra budget). `run_stream` is the request loop: it submits jobs at their arrival
 times (wall clock), steps while anything is queued or running, and reports
 each job's latency (submission to finish) and the aggregate throughput.
 See include/sputnipic_b200.h.
@@ -210,19 +211,23 @@ SERVING_GRID_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
 SERVING_PPC = (8, 27, 64, 125)
 
 
-def job_mix(n_configs=12, seed=0, max_particles_per_species=5_000_000, max_cycles=50):
+def job_mix(n_configs=12, seed=0, max_particles_per_species=5_000_000, max_cycles=50,
+            uniform=False):
     """Seeded mix of job configurations: grid, particles per cell, 2 or 4
-    species, 1..max_cycles cycles. Particles per cell are lowered where a
-    species would exceed the cap. Returns (workload, ncycles, species) tuples."""
+    species, 1..max_cycles cycles. Grids weighted SERVING_GRID_WEIGHTS and
+    particles per cell lowered where a species would exceed the cap, or, with
+    `uniform`, grids drawn uniformly and no cap. Returns (workload, ncycles,
+    species) tuples."""
     import numpy as np
 
     from . import workload as W
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n_configs):
-        g = SERVING_GRIDS[rng.choice(len(SERVING_GRIDS), p=SERVING_GRID_WEIGHTS)]
+        g = SERVING_GRIDS[rng.choice(len(SERVING_GRIDS), p=None if uniform else SERVING_GRID_WEIGHTS)]
         cells = g[0] * g[1] * g[2]
-        ppcs = [p for p in SERVING_PPC if p * cells <= max_particles_per_species] or [1]
+        cap = None if uniform else max_particles_per_species
+        ppcs = [p for p in SERVING_PPC if cap is None or p * cells <= cap] or [1]
         ppc = int(rng.choice(ppcs))
         ns = int(rng.choice((2, 4)))
         wl = W.small_gem(nxc=g[0], nyc=g[1], nzc=g[2], E_amp=1e-3, seed=int(rng.integers(1 << 30)),
@@ -288,7 +293,7 @@ def fifo_latencies(arrivals, service):
 
 
 def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), rates=None,
-                   extra_budget=0.0):
+                   extra_budget=0.0, uniform=False):
     """Poisson streams of `njobs` jobs drawn from a seeded mix of
     configurations, at `rate` jobs/s or at each of `rates`. Every
     configuration is also run alone (its single-job latency). Returns per
@@ -296,7 +301,7 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
     aggregate throughput in particle-cycles per second (the first rate's also
     at the top level)."""
     import numpy as np
-    configs = job_mix(n_configs, seed)
+    configs = job_mix(n_configs, seed, uniform=uniform)
     pool = device_jobs(configs)
     # warm-up: the engine's kernels for this tile shape loaded and configured
     # once, outside the single-job latencies
@@ -362,10 +367,13 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         "baseline": ("plain_one_at_a_time: the same stream served one job at a time through the "
                      "plain path (each configuration's wall time alone, measured; FIFO queue "
                      "over the same arrivals)"),
-        "mix": f"{n_configs} configurations: grids {list(SERVING_GRIDS)} "
-               f"(weights {list(SERVING_GRID_WEIGHTS)}), ppc from {list(SERVING_PPC)} "
-               "(capped at 5M particles per species), 2 or 4 species, 1-50 cycles, "
-               "frozen GEM fields; Poisson arrivals"})
+        "mix": (f"{n_configs} configurations: grids {list(SERVING_GRIDS)} drawn uniformly, ppc "
+                f"from {list(SERVING_PPC)}, 2 or 4 species, 1-50 cycles, frozen GEM fields; "
+                "Poisson arrivals" if uniform else
+                f"{n_configs} configurations: grids {list(SERVING_GRIDS)} "
+                f"(weights {list(SERVING_GRID_WEIGHTS)}), ppc from {list(SERVING_PPC)} "
+                "(capped at 5M particles per species), 2 or 4 species, 1-50 cycles, "
+                "frozen GEM fields; Poisson arrivals")})
     if rates:
         out["sweep"] = [{k: v for k, v in e.items() if k != "engine"} for e in sweep]
         for e in out["sweep"]:

@@ -95,3 +95,15 @@ def test_job_mix_is_seeded_and_capped():
         assert 1 <= ncycles <= 50 and len(species) in (2, 4)
         assert wl.species_count(0) <= 5_000_000
         assert wl.nxc % 4 == 0 and wl.nyc % 4 == 0 and wl.nzc % 4 == 0
+
+
+def test_uniform_job_mix_draws_grids_evenly_without_cap():
+    """The configuration's own mix: every grid about equally often, every
+    ppc on every grid (up to 65.5M particles per species)."""
+    mix = serve.job_mix(n_configs=400, seed=5, uniform=True)
+    grids = [(w.nxc, w.nyc, w.nzc) for w, _, _ in mix]
+    for g in serve.SERVING_GRIDS:
+        assert 0.18 <= grids.count(g) / len(grids) <= 0.32, g
+    big = [w for w, _, _ in mix if (w.nxc, w.nyc, w.nzc) == (128, 64, 64)]
+    assert max(w.species[0].ppc for w in big) == 125
+    assert max(w.species_count(0) for w, _, _ in mix) == 128 * 64 * 64 * 125
