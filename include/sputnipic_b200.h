@@ -351,11 +351,13 @@ int spb_sim_load_species(spb_sim *sim, int species, const float *x, const float 
  * slack. Overflow entries are pushed and deposited exactly in the meantime. */
 int spb_sim_cycle(spb_sim *sim, int ncycles, void *stream);
 /* Re-lay out every species now: buckets sized from the current counts, the
- * buckets and the overflow list copied into them (synchronises `stream`). */
+ * buckets and the overflow list copied into them (queued on `stream`; the
+ * buffer sets sized at the load hold any layout of the species). */
 int spb_sim_resort(spb_sim *sim, void *stream);
 /* Record slots of a species' bucket layout, summed over the cells (-1: bad
- * arguments). */
-long spb_sim_bucket_slots(const spb_sim *sim, int species);
+ * arguments; synchronises the device the first time after a load or
+ * re-layout). */
+long spb_sim_bucket_slots(spb_sim *sim, int species);
 /* Entries in a species' overflow list (synchronises `stream`; -1 on error). */
 long spb_sim_overflow(spb_sim *sim, int species, void *stream);
 /* FP64 moments of a species: 10*nodes doubles. */

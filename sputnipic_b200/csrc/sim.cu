@@ -2273,10 +2273,11 @@ int alloc_fixed(spb_sim *s, SimSpecies &q, int ocap) {
   return SPB_OK;
 }
 
-// Makes buffer set b hold at least `slots` records (1/16 headroom when it grows).
+// Makes buffer set b hold at least `slots` records (1/16 headroom when it
+// grows); waits for `st` only when it replaces a set queued work may read.
 int ensure_set(SimSpecies &q, int b, long long slots, cudaStream_t st) {
   if (q.slots[b] >= slots && q.rec[b]) return SPB_OK;
-  SPB_CUDA(cudaStreamSynchronize(st));
+  if (q.rec[b]) SPB_CUDA(cudaStreamSynchronize(st));
   free_set(q, b);
   const long long want = std::max<long long>(slots + slots / 16, 32);
   if (dmalloc(&q.rec[b], (size_t)want * 2 * sizeof(float4)) != cudaSuccess) {
@@ -2287,8 +2288,17 @@ int ensure_set(SimSpecies &q, int b, long long slots, cudaStream_t st) {
   return SPB_OK;
 }
 
-// base[0..ncells] = exclusive scan of v[0..ncells); returns base[ncells]
-// (synchronises the stream).
+// Record slots any layout of n particles can need: every cell's capacity is
+// at most count + count/2 + 16 rounded up to 4 (k_capacity), or the fixed
+// bucket size. Buffer sets of this size are allocated before the layout is
+// counted, so no load or re-layout waits for its counts on the host.
+long long slots_bound(const spb_sim *s, long n) {
+  const long long K = s->ncells;
+  return s->d.bucket_slots > 0 ? (long long)s->d.bucket_slots * K : (3LL * n) / 2 + 19 * K;
+}
+
+// base[0..ncells] = exclusive scan of v[0..ncells); with `total`, returns
+// base[ncells] (synchronises the stream).
 int scan_layout(spb_sim *s, const long long *v, long long *out, long long *total,
                 cudaStream_t st) {
   const long K = s->ncells;
@@ -2328,6 +2338,8 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
                                           : std::max<long>(65536, n / 32);
   if (ocap > (1L << 31) - 1) return fail(SPB_ERR_CAPACITY, "overflow list too large");
   if (int rc = alloc_fixed(s, q, (int)ocap)) return rc;
+  if (int rc = ensure_set(q, 0, slots_bound(s, n), st)) return rc;
+  if (int rc = ensure_set(q, 1, slots_bound(s, n), st)) return rc;
   SPB_CUDA(cudaMemsetAsync(s->counts, 0, s->ncells * sizeof(int), st));
   if (n > 0) {
     k_count_keys<TX, TY, TZ><<<blocks_for(n, 256), 256, 0, st>>>(g, s->nt[1], s->nt[2], src[0],
@@ -2340,10 +2352,7 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
   SPB_CUDA(cudaGetLastError());
   g_launches += 2;
   s->launches += 2;
-  long long total = 0;
-  if (int rc = scan_layout(s, s->lcap, q.base, &total, st)) return rc;
-  if (int rc = ensure_set(q, 0, total, st)) return rc;
-  if (int rc = ensure_set(q, 1, total, st)) return rc;
+  if (int rc = scan_layout(s, s->lcap, q.base, nullptr, st)) return rc;
   SPB_CUDA(cudaMemsetAsync(q.cnt[0], 0, s->ncells * sizeof(int), st));
   SPB_CUDA(cudaMemsetAsync(q.ocnt, 0, 2 * sizeof(int), st));
   if (n > 0) {
@@ -2354,7 +2363,7 @@ int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStre
     g_launches++;
     s->launches++;
   }
-  q.total = total;
+  q.total = -1;   // read back when asked for (spb_sim_bucket_slots)
   q.n = n;
   q.cur = 0;
   // the deterministic deposit's grids: Q = 2^(ceil(log2 T) - 38) with T the
@@ -2401,9 +2410,9 @@ int relayout(spb_sim *s, SimSpecies &q, cudaStream_t st) {
   SPB_CUDA(cudaGetLastError());
   g_launches += 3;
   s->launches += 3;
-  long long total = 0;
-  if (int rc = scan_layout(s, s->lcap, q.base2, &total, st)) return rc;
-  if (int rc = ensure_set(q, x, total, st)) return rc;
+  if (int rc = scan_layout(s, s->lcap, q.base2, nullptr, st)) return rc;
+  // the counts sum to the species' particles: the sets sized at the load hold it
+  if (int rc = ensure_set(q, x, slots_bound(s, q.n), st)) return rc;
   SPB_CUDA(cudaMemsetAsync(q.cnt[x], 0, K * sizeof(int), st));
   SPB_CUDA(cudaMemsetAsync(q.ocnt + x, 0, sizeof(int), st));
   k_relayout<<<blocks_for(K * 32, 256), 256, 0, st>>>(q.base, q.rec[c], q.cnt[c], K, q.orec[c],
@@ -2413,10 +2422,10 @@ int relayout(spb_sim *s, SimSpecies &q, cudaStream_t st) {
   g_launches++;
   s->launches++;
   std::swap(q.base, q.base2);
-  q.total = total;
+  q.total = -1;
   q.cur = x;
   // the other set is written by the next cycle: it must hold the new layout too
-  return ensure_set(q, c, total, st);
+  return ensure_set(q, c, slots_bound(s, q.n), st);
 }
 
 // Particles of buffer set `cur` into flat device arrays (dst[6], q, may be null).
@@ -2858,9 +2867,19 @@ extern "C" long spb_sim_count(const spb_sim *s, int species) {
 }
 extern "C" long spb_sim_launches(const spb_sim *s) { return s ? s->launches : 0; }
 
-extern "C" long spb_sim_bucket_slots(const spb_sim *s, int species) {
+extern "C" long spb_sim_bucket_slots(spb_sim *s, int species) {
   if (!s || species < 0 || species >= (int)s->sp.size()) return -1;
-  return (long)s->sp[species].total;
+  SimSpecies &q = s->sp[species];
+  if (q.total < 0 && q.base) {
+    long long t = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(&t, q.base + s->ncells, sizeof(t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    q.total = t;
+  }
+  return (long)std::max<long long>(q.total, 0);
 }
 
 extern "C" long spb_sim_overflow(spb_sim *s, int species, void *stream) {

@@ -26,7 +26,7 @@ struct SimSpecies {
   int *ocnt = nullptr;          // [2] overflow entry counters
   long long *base = nullptr;    // [ncells + 1] bucket layout of both buffer sets
   long long *base2 = nullptr;   // [ncells + 1] the next layout (re-layout)
-  long long total = 0;          // record slots of the layout
+  long long total = 0;          // record slots of the layout (-1: not read back yet)
   int cur = 0;                  // the buffer set holding the particles
   double *mom = nullptr;        // [10][nodes]
   double quantum[3] = {1.0, 1.0, 1.0};   // deterministic deposit grids (set at load)

@@ -43,10 +43,13 @@ class Finished:
     times: tuple            # (submitted, admitted, finished), engine seconds
     status: int
     results: dict = field(default_factory=dict)
+    late: float = 0.0       # seconds between the job's arrival and its submission
 
     @property
     def latency(self) -> float:
-        return self.times[2] - self.times[0]
+        """Arrival to finish: the engine's submission-to-finish time plus the
+        time the job waited for the request loop to submit it."""
+        return self.times[2] - self.times[0] + self.late
 
 
 class Server:
@@ -177,15 +180,18 @@ def release_cached_memory():
 
 def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
     """The request loop. jobs[i] arrives `arrivals[i]` seconds after the start
-    (sorted). Returns the finished jobs (with results for the indices in
-    `keep`) and the wall time of the whole stream."""
+    (sorted) and is submitted at the loop's first pass after that. Returns the
+    finished jobs (with results for the indices in `keep`; latencies count
+    from the arrival) and the wall time of the whole stream."""
     keep = set(keep or ())
     t0 = time.perf_counter()
-    i, live, done = 0, {}, []
+    i, live, done, late = 0, {}, [], {}
     while i < len(jobs) or live:
         now = time.perf_counter() - t0
         while i < len(jobs) and arrivals[i] <= now:
-            live[server.submit(jobs[i])] = i
+            jid = server.submit(jobs[i])
+            live[jid] = i
+            late[jid] = max(0.0, time.perf_counter() - t0 - arrivals[i])
             i += 1
         if not live:
             time.sleep(min(idle_sleep, max(0.0, arrivals[i] - now)))
@@ -200,7 +206,7 @@ def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
                 wl = job.wl
                 res = {s: server.result(jid, s, p["x"].numel(), wl.nodes)
                        for s, p in enumerate(job.parts)}
-            done.append(Finished(jid, job, server.times(jid), st, res))
+            done.append(Finished(jid, job, server.times(jid), st, res, late.pop(jid)))
             server.release(jid)
             del live[jid]
     return done, time.perf_counter() - t0
