@@ -424,7 +424,8 @@ def run_ours(args, rank, world, local_rank):
         # species) at a rate one GPU carries: about 9e8 particle-cycles a job
         lit = measure_stream(njobs=args.serve_jobs, rate=10.0, uniform=True)
         serving["uniform_mix_10_jobs_per_s"] = {
-            k: lit[k] for k in ("mix", "latency_ms", "single_job_latency_ms",
+            k: lit[k] for k in ("mix", "jobs", "completed", "failed", "failure_codes", "latency_ms",
+                                "single_job_latency_ms",
                                 "p99_over_single_job_p99", "slowdown_vs_alone",
                                 "throughput_particle_cycles_per_s", "plain_one_at_a_time",
                                 "plain_alone_ms")}

@@ -416,7 +416,8 @@ int spb_release_cached_memory(void);
 typedef struct spb_serve_desc {
   int tile[3];              /* tile shape of every job (0,0,0: 4x4x4) */
   long long hbm_budget;     /* bytes the admitted jobs may hold (0: 90% of the
-                               free device memory at creation) */
+                               device memory free at creation, counting what
+                               the device's memory pool holds unused) */
   int max_jobs;             /* jobs per launch (0 or above 64: 64) */
   int check_every;          /* steps between overflow checks (0: 4) */
   long long reserve_bytes;  /* device memory the library's pool maps up front

@@ -63,7 +63,7 @@ long long footprint(const spb_job_desc &d, const long *counts, int on_device) {
   for (int s = 0; s < d.ns; ++s) {
     const long long n = counts[s];
     nmax = std::max(nmax, n);
-    const long long slots = n + n / 4 + 20 * ncells;
+    const long long slots = (3 * n) / 2 + 19 * ncells;   // as the buckets are allocated
     const long long ocap = std::max<long long>(65536, n / 32);
     b += 2 * (slots + slots / 16) * 32 + 2 * ocap * 36 + 2 * ncells * 4 + 2 * (ncells + 1) * 8 +
          nodes * 80;
@@ -214,8 +214,18 @@ extern "C" int spb_serve_create(const spb_serve_desc *desc, spb_serve **out) {
   if (d.hbm_budget > 0) {
     s->budget = d.hbm_budget;
   } else {
+    // free device memory plus what the device's pool holds unused (the
+    // library's allocations come from it and keep freed memory there)
     size_t free_b = 0, total_b = 0;
     SPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    unsigned long long reserved = 0, used = 0;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used)
+      free_b += (size_t)(reserved - used);
+    cudaGetLastError();
     s->budget = (long long)(0.9 * (double)free_b);
   }
   if (d.reserve_bytes < 0) return fail(SPB_ERR_INVALID, "spb_serve_create: negative reserve");

@@ -44,6 +44,7 @@ class Finished:
     status: int
     results: dict = field(default_factory=dict)
     late: float = 0.0       # seconds between the job's arrival and its submission
+    error: int = 0          # status code of a failed job
 
     @property
     def latency(self) -> float:
@@ -129,6 +130,10 @@ class Server:
     def status(self, jid: int) -> int:
         return self.lib.spb_serve_status(self.h, jid)
 
+    def error(self, jid: int) -> int:
+        """Status code of a failed job (why it failed)."""
+        return self.lib.spb_serve_error(self.h, jid)
+
     def times(self, jid: int) -> tuple:
         t = (ctypes.c_double * 3)()
         _lib.check(self.lib.spb_serve_times(self.h, jid, t))
@@ -206,7 +211,8 @@ def run_stream(server: Server, jobs, arrivals, keep=None, idle_sleep=1e-4):
                 wl = job.wl
                 res = {s: server.result(jid, s, p["x"].numel(), wl.nodes)
                        for s, p in enumerate(job.parts)}
-            done.append(Finished(jid, job, server.times(jid), st, res, late.pop(jid)))
+            done.append(Finished(jid, job, server.times(jid), st, res, late.pop(jid),
+                                 server.error(jid) if st == FAILED else 0))
             server.release(jid)
             del live[jid]
     return done, time.perf_counter() - t0
@@ -314,6 +320,17 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
     srv = Server(tile=tile, extra_budget=extra_budget)
     run_stream(srv, [pool[0]], [0.0])
     srv.close()
+    # the baseline: every configuration alone through the plain path (warm;
+    # before the engine's pool grows, as its copies come from torch)
+    plain_job_seconds(pool[0])
+    plain = [plain_job_seconds(job) for job in pool]
+    # warm-up burst of a full launch's worth of jobs (every configuration,
+    # repeated), so the device memory pool has grown to a saturated engine's
+    # footprint before the single-job runs and the timed streams
+    srv = Server(tile=tile, extra_budget=extra_budget)
+    burst = [pool[i % len(pool)] for i in range(max(len(pool), 64))]
+    run_stream(srv, burst, [0.0] * len(burst))
+    srv.close()
     alone = []
     for job in pool:
         srv = Server(tile=tile, extra_budget=extra_budget)
@@ -321,16 +338,6 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         srv.close()
         assert done[0].status == DONE
         alone.append(done[0].latency)
-    # the baseline: every configuration alone through the plain path (warm)
-    plain_job_seconds(pool[0])
-    plain = [plain_job_seconds(job) for job in pool]
-    # warm-up burst of a full launch's worth of jobs (every configuration,
-    # repeated), so the device memory pool has grown to a saturated engine's
-    # footprint before the timed streams
-    srv = Server(tile=tile, extra_budget=extra_budget)
-    burst = [pool[i % len(pool)] for i in range(max(len(pool), 64))]
-    run_stream(srv, burst, [0.0] * len(burst))
-    srv.close()
     index = {id(j): k for k, j in enumerate(pool)}
     sweep = []
     for r in (rates or [rate]):
@@ -345,12 +352,14 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         stats["release_s"] = srv.release_s
         srv.close()
         ok = [d for d in done if d.status == DONE]
+        failed = len(done) - len(ok)
         lat = np.array([d.latency for d in ok])
         slow = np.array([d.latency / alone[index[id(d.job)]] for d in ok])
         work = sum(d.job.particles() * d.job.ncycles for d in ok)
         plat, pend = fifo_latencies(list(arrivals), [plain[i] for i in pick])
         sweep.append({
-            "rate_jobs_per_s": r, "jobs": njobs, "completed": len(ok),
+            "rate_jobs_per_s": r, "jobs": njobs, "completed": len(ok), "failed": failed,
+            "failure_codes": sorted({d.error for d in done if d.status != DONE}),
             "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
                            "p99": 1e3 * float(np.percentile(lat, 99))},
             "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
