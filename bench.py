@@ -25,6 +25,16 @@ Keys of the JSON line:
   cpu_baseline  the reference CPU code (oracle/_ref, else the restated port)
               timed on this host's cores over whole cycles of the same
               workload (one warm-up cycle, two timed)
+  plain       the plain drop-in (reference precision types) on device
+              arrays, per-kernel figures
+  serving     Poisson streams of independent frozen-field jobs through the
+              serving engine at 10, 50, 200 and 500 jobs/s (a weighted mix of
+              grids, a species capped at 5M particles), beside the same jobs
+              served one at a time through the plain path; and the
+              configuration's own mix (grids drawn uniformly, no cap) at 10
+              jobs/s (uniform_mix_10_jobs_per_s)
+  batching, hat_densities  the batching workload (uneven species, 20 cycles,
+              autotuned) and calculateHatDensities on the GEM grid
 The particle arrays (8.4 GB) are far larger than the 126 MB L2, so no L2
 flush is needed between steps.
 
