@@ -324,6 +324,13 @@ typedef struct spb_sim_desc {
                                push; overflow entries are pushed and deposited
                                after two grid barriers. Not with
                                deterministic. */
+  int overflow_per_mille;   /* overflow list entries per 1000 particles of a
+                               species, at least 65536 entries (0: about one
+                               per 32 particles; a fixed bucket_slots makes
+                               it one per particle). A species is re-laid out
+                               once its list passes 1/256 of its particles,
+                               so the default leaves 8x that for the cycles
+                               until the check that sees it */
 } spb_sim_desc;
 
 /* Whether a tile shape has an instantiated kernel. */
@@ -419,7 +426,10 @@ typedef struct spb_serve_desc {
                                device memory free at creation, counting what
                                the device's memory pool holds unused) */
   int max_jobs;             /* jobs per launch (0 or above 64: 64) */
-  int check_every;          /* steps between overflow checks (0: 4) */
+  int check_every;          /* a job's cycles between checks of its overflow
+                               lists (0: 4); a job gets further cycles in a
+                               step only while its last evaluated check is
+                               less than 2 x check_every cycles old */
   long long reserve_bytes;  /* device memory the library's pool maps up front
                                (0: none), so that admitting jobs maps nothing;
                                spb_release_cached_memory gives it back */

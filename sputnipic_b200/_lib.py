@@ -147,7 +147,7 @@ class SimDesc(ctypes.Structure):
                 ("ns", c_int), ("qom", c_double * 8), ("capacity", c_long * 8),
                 ("tile", c_int * 3), ("resort_every", c_int), ("ctas", c_int),
                 ("variant", c_int), ("bucket_slots", c_int), ("graph", c_int),
-                ("deterministic", c_int), ("fused", c_int)]
+                ("deterministic", c_int), ("fused", c_int), ("overflow_per_mille", c_int)]
 
 
 HAT_MAX_SPECIES = 16

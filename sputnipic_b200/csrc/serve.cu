@@ -29,6 +29,8 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+constexpr int SERVE_OVERFLOW_PER_MILLE = 125;   // jobs' overflow lists: n/8 entries
+
 struct ServeJob {
   long id = 0;
   spb_job_desc d{};
@@ -44,6 +46,8 @@ struct ServeJob {
   double t[3] = {-1.0, -1.0, -1.0};   // submitted, admitted, finished
   cudaEvent_t done = nullptr;         // recorded after the job's last launch
   long ovf_step = -1;                 // step whose overflow counters were copied back
+  int cycles_copied = 0;              // the job's cycles when they were copied
+  int cycles_checked = 0;             // cycles its last evaluated check (or re-layout) covers
   ~ServeJob() {
     // a released job's work is complete (its event was seen, or it never ran)
     if (sim) spb::sim_free(sim, false);
@@ -64,7 +68,7 @@ long long footprint(const spb_job_desc &d, const long *counts, int on_device) {
     const long long n = counts[s];
     nmax = std::max(nmax, n);
     const long long slots = (3 * n) / 2 + 19 * ncells;   // as the buckets are allocated
-    const long long ocap = std::max<long long>(65536, n / 32);
+    const long long ocap = std::max<long long>(65536, n * SERVE_OVERFLOW_PER_MILLE / 1000);
     b += 2 * (slots + slots / 16) * 32 + 2 * ocap * 36 + 2 * ncells * 4 + 2 * (ncells + 1) * 8 +
          nodes * 80;
   }
@@ -79,6 +83,8 @@ double seconds_since(Clock::time_point t0) {
 }  // namespace
 
 constexpr int SERVE_LAUNCHES = 8;   // launches per step at most
+constexpr int SERVE_ADMIT_MAX = 8;  // admissions per step at most
+constexpr double SERVE_ADMIT_SECONDS = 0.004;   // host time per step for admissions
 constexpr int SERVE_ERR_SLOTS = 4096;   // pinned error words of jobs finishing
 
 struct spb_serve {
@@ -166,6 +172,9 @@ int admit(spb_serve *s, ServeJob *j) {
   sd.ns = j->d.ns;
   for (int i = 0; i < j->d.ns; ++i) sd.qom[i] = j->d.qom[i];
   sd.resort_every = 1 << 30;   // the engine checks overflow lists itself
+  // its checks come back a few steps late: lists of n/8 entries leave 32x
+  // the re-layout threshold for the cycles in between
+  sd.overflow_per_mille = SERVE_OVERFLOW_PER_MILLE;
   if (int rc = spb_sim_create(&sd, &j->sim)) return rc;
   if (int rc = spb_sim_set_fields(j->sim, j->fields, j->on_device, s->adm)) return rc;
   for (int i = 0; i < j->d.ns; ++i) {
@@ -293,9 +302,17 @@ extern "C" int spb_serve_step(spb_serve *s) {
     tp = t;
   };
   // admit in order of arrival while the head fits, uploading on the
-  // admission stream; the engine's stream then waits for the uploads
+  // admission stream; the engine's stream then waits for the uploads. At
+  // most SERVE_ADMIT_MAX jobs or SERVE_ADMIT_SECONDS of host time per step
+  // (at least one job): the rest are admitted in the next steps, so a burst
+  // of arrivals does not hold the launches back while each job's memory is
+  // allocated and its layout queued
   auto admit_pending = [&](std::vector<ServeJob *> &joined) -> int {
-    while (!s->pending.empty() && (int)(s->active.size() + joined.size()) < s->d.max_jobs) {
+    const Clock::time_point t_adm = Clock::now();
+    int admitted = 0;
+    while (!s->pending.empty() && (int)(s->active.size() + joined.size()) < s->d.max_jobs &&
+           (admitted == 0 ||
+            (admitted < SERVE_ADMIT_MAX && seconds_since(t_adm) < SERVE_ADMIT_SECONDS))) {
       ServeJob *j = s->pending.front();
       if (j->bytes > s->budget) {   // can never fit: fail it rather than block the queue
         s->pending.pop_front();
@@ -313,6 +330,7 @@ extern "C" int spb_serve_step(spb_serve *s) {
         continue;
       }
       joined.push_back(j);
+      ++admitted;
     }
     SPB_CUDA(cudaEventRecord(s->adm_done, s->adm));
     SPB_CUDA(cudaStreamWaitEvent(s->st, s->adm_done, 0));
@@ -337,13 +355,18 @@ extern "C" int spb_serve_step(spb_serve *s) {
     for (size_t i = 0; i < j->sim->sp.size(); ++i)
       over |= h[i] > spb::relayout_threshold(j->sim->sp[i]);
     j->ovf_step = -1;
-    if (over)
+    j->cycles_checked = j->cycles_copied;
+    if (over) {
       if (int rc = spb_sim_resort(j->sim, s->st)) return -rc;
+      j->cycles_checked = j->cycles;   // the lists are empty again from here
+    }
   }
   lap(1);
   // this step's launches (asynchronous): one cycle of every admitted job,
   // then further cycles for the jobs with cycles left, cheapest first, while
-  // the added cost stays within extra_budget of the first launch's
+  // the added cost stays within extra_budget of the first launch's; a job
+  // gets further cycles only while its overflow lists were checked within
+  // the last 2 x check_every cycles (so that they cannot fill unseen)
   const std::vector<ServeJob *> ran = s->active;
   if (!ran.empty()) {
     std::vector<spb_sim *> sims;
@@ -366,7 +389,8 @@ extern "C" int spb_serve_step(spb_serve *s) {
         sims.clear();
         double spent = 0.0;
         for (auto &c : cand)
-          if (c.second->cycles < c.second->d.ncycles && spent + c.first <= budget) {
+          if (c.second->cycles < c.second->d.ncycles && spent + c.first <= budget &&
+              c.second->cycles - c.second->cycles_checked < 2 * s->d.check_every) {
             sims.push_back(c.second->sim);
             spent += c.first;
             c.second->cycles++;
@@ -377,18 +401,18 @@ extern "C" int spb_serve_step(spb_serve *s) {
       }
     }
     // the jobs whose last cycle is launched: their error words come back
-    // and an event marks their completion; every check_every steps the
-    // others' overflow counters come back too
-    const bool check = s->steps % s->d.check_every == 0;
+    // and an event marks their completion; the others' overflow counters
+    // come back every check_every of their cycles
     std::vector<ServeJob *> still;
     for (ServeJob *j : ran) {
       if (j->cycles < j->d.ncycles) {
-        if (check && j->ovf_step < 0) {
+        if (j->ovf_step < 0 && j->cycles - j->cycles_copied >= s->d.check_every) {
           int *h = s->h_ovf + (j->id % SERVE_ERR_SLOTS) * SPB_SIM_MAX_SPECIES;
           for (size_t i = 0; i < j->sim->sp.size(); ++i)
             SPB_CUDA(cudaMemcpyAsync(h + i, j->sim->sp[i].ocnt + j->sim->sp[i].cur, sizeof(int),
                                      cudaMemcpyDeviceToHost, s->st));
           j->ovf_step = s->steps;
+          j->cycles_copied = j->cycles;
         }
         still.push_back(j);
         continue;

@@ -2334,8 +2334,10 @@ SpeciesDev write_side(SimSpecies &q, int b, const long long *base) {
 template <int TX, int TY, int TZ>
 int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStream_t st) {
   const GridScalars g = scalars(s);
-  const long ocap = s->d.bucket_slots > 0 ? std::max<long>(65536, n)
-                                          : std::max<long>(65536, n / 32);
+  const long per = s->d.bucket_slots > 0      ? 1000
+                   : s->d.overflow_per_mille > 0 ? s->d.overflow_per_mille
+                                                 : 0;
+  const long ocap = std::max<long>(65536, per > 0 ? (long)((double)n * per / 1000.0) : n / 32);
   if (ocap > (1L << 31) - 1) return fail(SPB_ERR_CAPACITY, "overflow list too large");
   if (int rc = alloc_fixed(s, q, (int)ocap)) return rc;
   if (int rc = ensure_set(q, 0, slots_bound(s, n), st)) return rc;

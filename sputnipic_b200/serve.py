@@ -4,9 +4,10 @@ different grids and particle counts (spb_serve_* of libsputnipic_b200.so).
 A `Server` queues jobs as they arrive, admits them when their HBM footprint
 fits, and advances every admitted job at least one cycle per `step()` (one
 launch per kernel for all of them, and further launches that give cheap jobs
-more cycles within the engine's extra budget). `run_stream` is the request loop: it submits jobs at their arrival
-times (wall clock), steps while anything is queued or running, and reports
-each job's latency (submission to finish) and the aggregate throughput.
+more cycles within the engine's extra budget). `run_stream` is the request
+loop: it submits jobs at their arrival times (wall clock), steps while
+anything is queued or running, and reports each job's latency (arrival to
+finish) and the aggregate throughput.
 See include/sputnipic_b200.h.
 """
 from __future__ import annotations
@@ -360,6 +361,8 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         sweep.append({
             "rate_jobs_per_s": r, "jobs": njobs, "completed": len(ok), "failed": failed,
             "failure_codes": sorted({d.error for d in done if d.status != DONE}),
+            "failed_jobs": [{"config": index[id(d.job)], "code": d.error} for d in done
+                            if d.status != DONE],
             "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)),
                            "p99": 1e3 * float(np.percentile(lat, 99))},
             "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),

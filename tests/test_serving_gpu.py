@@ -150,8 +150,9 @@ def test_extra_cycles_for_cheap_jobs(cuda, orc64):
     with cycles left whose cost still fits the budget, cheapest first: with
     the default budget (0, read as 1.0 x the first launch's cost) one such
     launch fits both jobs (two cycles a step); with 8.0 all seven further
-    launches do (eight cycles a step); with extra cycles off (negative) each
-    job gets one cycle a step. The cheap job's moments are the same in all
+    launches do (eight cycles a step, one while a check of the job's
+    overflow lists is outstanding: 40 cycles in 9 steps); with extra cycles
+    off (negative) each job gets one cycle a step. The cheap job's moments are the same in all
     three, within 1e-5 of the FP64 oracle."""
     torch = cuda
     cheap = W.small_gem(nxc=16, nyc=8, nzc=8, E_amp=1e-3, species=W.gem_species((8, 8, 8, 8)))
@@ -160,7 +161,7 @@ def test_extra_cycles_for_cheap_jobs(cuda, orc64):
     steps, res = {}, {}
     for budget in (0.0, 8.0, -1.0):
         steps[budget], res[budget] = steps_to_finish(torch, specs, 1, extra_budget=budget)
-    assert steps[8.0] <= 7, steps
+    assert steps[8.0] <= 11, steps
     assert 20 <= steps[0.0] <= 22, steps
     assert steps[-1.0] >= 40, steps
     _, m64 = oracle_run(orc64, cheap, W.gem_particles(cheap, 0), cheap.species[0].qom, 40)
