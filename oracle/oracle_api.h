@@ -96,7 +96,7 @@ int orc_hat_densities(const orc_setup *s, double th, int ns, const double *qom,
 /* Number of OpenMP threads the library will use. */
 int orc_num_threads(void);
 
-/* sizeof(ORC_FP) of this build: 4 or 8. */
+/* sizeof(ORC_FP) of the loaded library: 4 (FP32 variant) or 8 (FP64 variant). */
 int orc_fp_bytes(void);
 
 #ifdef __cplusplus
