@@ -625,18 +625,23 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
     h2d = sum(52 * c for c in n) + ns * (24 * nodes + 40 * nodes)
     d2h = sum(24 * c for c in n) + ns * 40 * nodes
 
+    zero_s = [0.0]   # host seconds in the driver's setZeroSpeciesDensities
+
     def step():
         for s in range(ns):
             if dropin.mover_PC(P[s], field, grd, param) != 0:
                 raise RuntimeError(dropin.last_error())
         for s in range(ns):
+            z = time.perf_counter()
             dropin.setZeroSpeciesDensities(ids[s])
+            zero_s[0] += time.perf_counter() - z
             dropin.interpP2G(P[s], ids[s], grd, raise_on_error=True)
 
     def timed(steps):
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
+        zero_s[0] = 0.0
         t0 = time.perf_counter()
         for _ in range(steps):
             step()
@@ -649,8 +654,10 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
     out = {"value": R.aggregate_rate(sum(n), world, steps, t), "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
            "ms_per_step": 1e3 * t / steps,
+           "host_setzero_ms_per_step": 1e3 * zero_s[0] / steps,
            "path": "spb_mover_PC + spb_interpP2G on reference structs, COPY residency, "
-                   "pinned host arrays; timed on the host clock"}
+                   "pinned host arrays; timed on the host clock; the step includes the "
+                   "driver's own host-side setZeroSpeciesDensities (host_setzero_ms_per_step)"}
     # the same calls with the particles kept in HBM (spb_set_residency): every
     # step still uploads each species' fields and moments and reads the
     # moments back; the particles went up once, before the timed steps
@@ -670,6 +677,7 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
             "h2d_bytes_per_step": ns * (24 * nodes + 40 * nodes),
             "d2h_bytes_per_step": ns * 40 * nodes, "steps": steps_d,
             "ms_per_step": 1e3 * td / steps_d,
+            "host_setzero_ms_per_step": 1e3 * zero_s[0] / steps_d,
             "path": "the same calls in DEVICE residency: particles resident in HBM, per step each "
                     "species' fields and moments uploaded and its moments read back"}
     dropin.release_all()
