@@ -279,7 +279,10 @@ typedef struct spb_sim_desc {
   int periodic[3];          /* param->PERIODICX/Y/Z */
   int ns;                   /* species, 1..8 */
   double qom[SPB_SIM_MAX_SPECIES];
-  long capacity[SPB_SIM_MAX_SPECIES]; /* optional: particles to reserve for */
+  long capacity[SPB_SIM_MAX_SPECIES]; /* optional: particles a species' buffers
+                               are sized for at its first load (at least the
+                               loaded count), so that reloading it with up to
+                               that many particles reallocates nothing */
   int tile[3];              /* cells per tile (0,0,0: default 8x4x4) */
   int resort_every;         /* cycles between overflow checks (>= 1): a species
                                whose overflow list holds more than 1/256 of

@@ -2334,14 +2334,18 @@ SpeciesDev write_side(SimSpecies &q, int b, const long long *base) {
 template <int TX, int TY, int TZ>
 int build(spb_sim *s, SimSpecies &q, const float *const src[7], long n, cudaStream_t st) {
   const GridScalars g = scalars(s);
+  // the buffers hold max(n, the species' reserved capacity) particles
+  const long sidx = (long)(&q - s->sp.data());
+  const long nres = std::max<long>(n, sidx < SPB_SIM_MAX_SPECIES ? s->d.capacity[sidx] : 0);
   const long per = s->d.bucket_slots > 0      ? 1000
                    : s->d.overflow_per_mille > 0 ? s->d.overflow_per_mille
                                                  : 0;
-  const long ocap = std::max<long>(65536, per > 0 ? (long)((double)n * per / 1000.0) : n / 32);
+  const long ocap =
+      std::max<long>(65536, per > 0 ? (long)((double)nres * per / 1000.0) : nres / 32);
   if (ocap > (1L << 31) - 1) return fail(SPB_ERR_CAPACITY, "overflow list too large");
   if (int rc = alloc_fixed(s, q, (int)ocap)) return rc;
-  if (int rc = ensure_set(q, 0, slots_bound(s, n), st)) return rc;
-  if (int rc = ensure_set(q, 1, slots_bound(s, n), st)) return rc;
+  if (int rc = ensure_set(q, 0, slots_bound(s, nres), st)) return rc;
+  if (int rc = ensure_set(q, 1, slots_bound(s, nres), st)) return rc;
   SPB_CUDA(cudaMemsetAsync(s->counts, 0, s->ncells * sizeof(int), st));
   if (n > 0) {
     k_count_keys<TX, TY, TZ><<<blocks_for(n, 256), 256, 0, st>>>(g, s->nt[1], s->nt[2], src[0],

@@ -24,7 +24,8 @@ def _stream(stream):
 
 class Simulation:
     def __init__(self, wl, tile=(8, 4, 4), resort_every=4, ctas=0, species=None, variant=0,
-                 bucket_slots=0, graph=False, deterministic=False, fused=False):
+                 bucket_slots=0, graph=False, deterministic=False, fused=False, capacity=None,
+                 overflow_per_mille=0):
         self.lib = _lib.load()
         self.wl = wl
         species = list(range(len(wl.species))) if species is None else list(species)
@@ -44,6 +45,9 @@ class Simulation:
         d.graph = 1 if graph else 0
         d.deterministic = 1 if deterministic else 0
         d.fused = 1 if fused else 0
+        for i, c in enumerate(capacity or []):
+            d.capacity[i] = int(c)
+        d.overflow_per_mille = int(overflow_per_mille)
         h = ctypes.c_void_p()
         _lib.check(self.lib.spb_sim_create(ctypes.byref(d), ctypes.byref(h)))
         self.h = h

@@ -193,6 +193,40 @@ def test_relayout_keeps_particles_and_moments(cuda, orc64):
     sim.close()
 
 
+def test_reload_within_reserved_capacity(cuda, orc64):
+    """spb_sim_desc.capacity reserves a species' buffers at its first load:
+    half the particles loaded and run two cycles, then the whole set loaded
+    in their place and run three cycles, against three FP64 oracle cycles of
+    the whole set (moments and tagged particles)."""
+    torch = cuda
+    from sputnipic_b200.sim import Simulation
+    wl = W.small_gem()
+    fields = W.gem_fields(wl)
+    part = W.gem_particles(wl, 0)
+    n = len(part["x"])
+    sim = Simulation(wl, species=[0], resort_every=2, capacity=[n])
+    sim.set_fields([torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in fields])
+    half = {k: torch.from_numpy(np.ascontiguousarray(part[k][: n // 2])).cuda() for k in "xyzuvwq"}
+    sim.load_species(0, half)
+    sim.cycle(2)
+    assert sim.check() == 0 and sim.count(0) == n // 2
+    full = {k: torch.from_numpy(np.ascontiguousarray(part[k])).cuda() for k in "xyzuvwq"}
+    sim.load_species(0, full)
+    sim.cycle(3)
+    assert sim.check() == 0 and sim.count(0) == n
+    _, m64 = oracle64(orc64, wl, fields, part, wl.species[0].qom, ncycles=3)
+    assert (rel_l2(sim.moments(0).cpu().numpy(), m64) <= 1e-5).all()
+    full["q"] = torch.arange(n, dtype=torch.float32, device="cuda")
+    sim.load_species(0, full)
+    sim.cycle(3)
+    assert sim.check() == 0
+    tagged = dict(part)
+    tagged["q"] = np.arange(n, dtype=np.float32)
+    ref, _ = oracle64(orc64, wl, fields, tagged, wl.species[0].qom, ncycles=3)
+    compare_particles({k: v.cpu().numpy() for k, v in sim.particles(0).items()}, ref, wl)
+    sim.close()
+
+
 def test_bc_on_device_matches_oracle_bc(cuda, orc64):
     torch = cuda
     wl = W.small_gem()
