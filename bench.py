@@ -35,6 +35,8 @@ Keys of the JSON line:
               jobs/s (uniform_mix_10_jobs_per_s)
   batching, hat_densities  the batching workload (uneven species, 20 cycles,
               autotuned) and calculateHatDensities on the GEM grid
+  dense       the headline step on the dense variant (256x128x128 cells,
+              4 species x 134,217,728 particles)
 The particle arrays (8.4 GB) are far larger than the 126 MB L2, so no L2
 flush is needed between steps.
 
@@ -449,6 +451,10 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_batching:
         batching = measure_batching(torch, rank)
 
+    dense = None
+    if not args.no_dense:
+        dense = measure_dense(torch, stream, args, rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # whole cycles of the same workload on the host's cores: the pinned
@@ -498,9 +504,60 @@ def run_ours(args, rank, world, local_rank):
                 "value": plain["value"], "unit": UNIT, "ms_per_step": plain["ms_per_step"],
                 "kernels": plain["kernels"], "speedup_of_precision_form": value / plain["value"]},
             "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "hat_densities": hat,
-            "batching": batching,
+            "batching": batching, "dense": dense,
         }
         print(json.dumps(line), flush=True)
+
+
+def measure_dense(torch, stream, args, rank, steps=5, warmup=3):
+    """The precision form's step on the dense variant of the GEM cycle: 256 x
+    128 x 128 cells, 4 species x 134,217,728 particles (32 ppc), NiterMover 3,
+    generated on the device. The same step as the headline (new fields, push
+    and deposit of every species, applyBCids per species), CUDA graphs,
+    overflow checks every `args.resort` cycles, device-timed over `steps`
+    steps after `warmup`; frac_contract as the headline's (60 B per particle
+    plus the grid bytes over the step time)."""
+    from sputnipic_b200 import _lib
+    from sputnipic_b200.device import gen_fields, gen_particles
+    from sputnipic_b200.sim import Simulation
+    wl = R.rank_workload(W.PRESETS["dense"](), rank)
+    ns = len(wl.species)
+    fields = gen_fields(wl)
+    sim = Simulation(wl, tile=tuple(args.tile), resort_every=args.resort, graph=True)
+    sim.set_fields(fields)
+    n = 0
+    for s in range(ns):
+        p = gen_particles(wl, s)
+        n += p["x"].numel()
+        sim.load_species(s, p)
+        del p
+        torch.cuda.empty_cache()
+
+    def step():
+        sim.set_fields(fields)
+        sim.cycle(1)
+        for s in range(ns):
+            sim.apply_bc_ids(s)
+
+    for _ in range(warmup):
+        step()
+    rc = sim.check()
+    if rc:
+        raise RuntimeError(f"dense warm-up status {rc}: {_lib.last_error()}")
+    ms = device_timed(torch, None, stream, steps, step)
+    rc = sim.check()
+    sim.close()
+    torch.cuda.empty_cache()
+    if rc:
+        raise RuntimeError(f"dense status {rc}: {_lib.last_error()}")
+    peak = peaks()[0]
+    grid_bytes = wl.nodes * (6 * 4 + ns * 10 * 8)
+    contract = (60 * n + grid_bytes) / (ms / steps / 1e3) / 1e9
+    return {"workload": f"{wl.name}: {ns} species x {n // ns:,} particles, "
+                        f"{wl.species[0].ppc:g} ppc, NiterMover {wl.niter}",
+            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "warmup": warmup, "tile": list(args.tile),
+            "frac_contract": contract / peak, "peak_gbs": peak}
 
 
 def measure_batching(torch, rank):
@@ -763,6 +820,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-hat", action="store_true",
                     help="skip the calculateHatDensities measurement")
+    ap.add_argument("--no-dense", action="store_true",
+                    help="skip the dense variant (256x128x128, 4 x 134M particles)")
     ap.add_argument("--no-batching", action="store_true",
                     help="skip the batching-form measurement (uneven species, autotuned)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
