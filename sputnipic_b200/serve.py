@@ -306,13 +306,16 @@ def fifo_latencies(arrivals, service):
 
 
 def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), rates=None,
-                   extra_budget=0.0, uniform=False):
+                   extra_budget=0.0, uniform=False, reserve_fraction=0.6):
     """Poisson streams of `njobs` jobs drawn from a seeded mix of
     configurations, at `rate` jobs/s or at each of `rates`. Every
     configuration is also run alone (its single-job latency). Returns per
     rate the latency percentiles, slowdowns against running alone and the
     aggregate throughput in particle-cycles per second (the first rate's also
-    at the top level)."""
+    at the top level). The engines of the burst, the single-job runs and the
+    streams map `reserve_fraction` of their budget into the memory pool when
+    they are created (spb_serve_desc.reserve_bytes), so that admissions during
+    a stream do not wait for the pool to grow."""
     import numpy as np
     configs = job_mix(n_configs, seed, uniform=uniform)
     pool = device_jobs(configs)
@@ -325,16 +328,19 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
     # before the engine's pool grows, as its copies come from torch)
     plain_job_seconds(pool[0])
     plain = [plain_job_seconds(job) for job in pool]
+    probe = Server(tile=tile)
+    reserve = int(reserve_fraction * probe.counts()["budget"])
+    probe.close()
     # warm-up burst of a full launch's worth of jobs (every configuration,
     # repeated), so the device memory pool has grown to a saturated engine's
     # footprint before the single-job runs and the timed streams
-    srv = Server(tile=tile, extra_budget=extra_budget)
+    srv = Server(tile=tile, extra_budget=extra_budget, reserve_bytes=reserve)
     burst = [pool[i % len(pool)] for i in range(max(len(pool), 64))]
     run_stream(srv, burst, [0.0] * len(burst))
     srv.close()
     alone = []
     for job in pool:
-        srv = Server(tile=tile, extra_budget=extra_budget)
+        srv = Server(tile=tile, extra_budget=extra_budget, reserve_bytes=reserve)
         done, _ = run_stream(srv, [job], [0.0])
         srv.close()
         assert done[0].status == DONE
@@ -347,7 +353,7 @@ def measure_stream(rate=10.0, njobs=100, n_configs=12, seed=0, tile=(4, 4, 4), r
         arrivals = np.cumsum(rng.exponential(1.0 / r, size=njobs))
         arrivals -= arrivals[0]
         jobs = [pool[i] for i in pick]
-        srv = Server(tile=tile, extra_budget=extra_budget)
+        srv = Server(tile=tile, extra_budget=extra_budget, reserve_bytes=reserve)
         done, wall = run_stream(srv, jobs, list(arrivals))
         stats = srv.stats()
         stats["release_s"] = srv.release_s
