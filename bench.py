@@ -367,7 +367,9 @@ def measure_precision(args, torch, wl, fields, parts, dist, stream, world):
                      "bytes_per_step": contract_bytes, "achieved": contract_bytes / step_s / 1e9,
                      "basis": "whole device-timed step (fields, push, deposit, applyBCids)"},
         "algorithmic_bytes": d["algorithmic_bytes"], "kernel_ms_mean": d["ms_mean"],
-        "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+        "peak_source": ("measured: MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else
+                        "fallback: 6650 GB/s, an earlier copy-bandwidth measurement on B200 "
+                        "(MEASURED_PEAKS.json absent)"),
         "share_of_step": d["share_of_step"], "kernels": kernels,
         "cycle": {"kernels_ms": cyc_ms, "algorithmic_bytes": cyc_alg,
                   "achieved": cyc_alg / (cyc_ms / 1e3) / 1e9,
