@@ -564,8 +564,10 @@ struct RunSmem {
 };
 
 // half_terms from the stored node distances of particle j: the same 40
-// summands, bit for bit (each product in the reference's order; pairs of
-// independent products issued as one packed FP32x2 multiply).
+// summands, each product in the reference's order (pairs of independent
+// products issued as one packed FP32x2 multiply). With ADD, a term's last
+// multiply may be fused into the packed sum that follows it (one rounding
+// instead of two); the moments are a reordered FP32 sum either way.
 template <bool ADD>
 __device__ __forceinline__ void run_terms(const GeomDev &g, const RunSmem &S, int j,
                                           float2 (&t)[20], int lane, int a) {
