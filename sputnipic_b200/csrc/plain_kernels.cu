@@ -59,6 +59,22 @@ __device__ __forceinline__ int clamp_cell(int i, int n, int &bad) {
   return i;
 }
 
+// x * y on a pair of floats, each half rounded to nearest on its own, as a
+// scalar float multiply rounds it. The mover adds the two halves with scalar
+// adds: a packed product that feeds a packed add came out rounded once with
+// its sum, which the reference's float code does not do.
+__device__ __forceinline__ float2 mul2_rn(float2 x, float2 y) {
+  float2 d;
+  asm("{\n\t.reg .b64 a, b, c;\n\t"
+      "mov.b64 a, {%2, %3};\n\t"
+      "mov.b64 b, {%4, %5};\n\t"
+      "mul.rn.f32x2 c, a, b;\n\t"
+      "mov.b64 {%0, %1}, c;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(x.x), "f"(x.y), "f"(y.x), "f"(y.y));
+  return d;
+}
+
 // Particle boundary condition on one axis (src/Mover.cpp:103-157): an
 // "above L" test in double, then a separate "below 0" test in float.
 __device__ __forceinline__ void bc_axis(float &pos, float &vel, double L, int periodic) {
@@ -127,12 +143,17 @@ __device__ __forceinline__ void move_one(const GeomDev &g, const PushDev &p,
           const int n = base - a * sx - b * sy - c;
           const float4 f4 = __ldg(F.eb4 + n);
           const float2 f2 = __ldg(F.eb2 + n);
-          Ex += wgt * f4.x;
-          Ey += wgt * f4.y;
-          Ez += wgt * f4.z;
-          Bx += wgt * f4.w;
-          By += wgt * f2.x;
-          Bz += wgt * f2.y;
+          // the six products as three packed multiplies, summed one by one
+          const float2 w2 = make_float2(wgt, wgt);
+          const float2 pxy = mul2_rn(w2, make_float2(f4.x, f4.y));
+          const float2 pzx = mul2_rn(w2, make_float2(f4.z, f4.w));
+          const float2 pyz = mul2_rn(w2, f2);
+          Ex += pxy.x;
+          Ey += pxy.y;
+          Ez += pzx.x;
+          Bx += pzx.y;
+          By += pyz.x;
+          Bz += pyz.y;
         }
     const float omdtsq = qomdt2 * qomdt2 * (Bx * Bx + By * By + Bz * Bz);
     const float denom = (float)(1.0 / (1.0 + (double)omdtsq));
