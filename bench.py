@@ -37,6 +37,10 @@ Keys of the JSON line:
               autotuned) and calculateHatDensities on the GEM grid
   dense       the headline step on the dense variant (256x128x128 cells,
               4 species x 134,217,728 particles)
+  next_rows   the drop-in's calls beside the path on the e2e leg's resident
+              particles: the driver's moment section in one call
+              (spb_interp_all_species) and the binned particle sort
+              (spb_particle_sort)
 The particle arrays (8.4 GB) are far larger than the 126 MB L2, so no L2
 flush is needed between steps.
 
@@ -507,6 +511,7 @@ def run_ours(args, rank, world, local_rank):
                 "kernels": plain["kernels"], "speedup_of_precision_form": value / plain["value"]},
             "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "hat_densities": hat,
             "batching": batching, "dense": dense,
+            "next_rows": None if e2e is None else e2e.pop("next_rows", None),
         }
         print(json.dumps(line), flush=True)
 
@@ -729,6 +734,7 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
             td = timed(steps_d)
             for s in range(ns):
                 dropin.sync_particles_to_host(P[s])
+            out["next_rows"] = measure_next_rows(args, wl, P, ids, field, grd, param, dist)
         finally:
             dropin.set_residency(False)
         out["device_residency"] = {
@@ -741,6 +747,82 @@ def run_e2e(args, wl, host_parts, host_f, world, dist):
                     "species' fields and moments uploaded and its moments read back"}
     dropin.release_all()
     return out
+
+
+def measure_next_rows(args, wl, P, ids, field, grd, param, dist):
+    """The drop-in's calls beside the mover and the deposit, on the e2e leg's
+    reference structs in DEVICE residency (particles resident), host clock
+    around the synchronous calls, slowest rank:
+      moment_section  spb_interp_all_species, the driver's moment section in
+                      one call (src/sputniPIC_CPU.cpp:247-259: zero, interpP2G
+                      of every species, applyBCids, sumOverSpecies; the
+                      species' and net moments written to the host once)
+      particle_sort   spb_particle_sort of every species (src/Particles.cpp:
+                      72-234) with GEM_3D's sort_cps = 2: in place on the
+                      resident copy when the device holds the newest particles
+                      (after a mover_PC step), and through PCIe when the host
+                      arrays are the newest (uploaded, sorted, downloaded);
+                      algorithmic bytes of the sort: each particle's 28 bytes
+                      read and written once"""
+    import torch
+    from sputnipic_b200 import dropin
+    ns = len(P)
+    n = sum(p.nop for p in P)
+    nodes = wl.nodes
+    idn = dropin.interp_dens_net_allocate(grd)
+    keep = []
+    for name in list(idn._arrays):
+        t = torch.zeros(idn._arrays[name].size, dtype=torch.float32).pin_memory()
+        keep.append(t)
+        idn._arrays[name] = t.numpy()
+        setattr(idn, name + "_flat", t.numpy().ctypes.data)
+
+    def timed(call, reps):
+        call()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            call()
+        torch.cuda.synchronize()
+        return R.max_over_ranks(time.perf_counter() - t0, dist) / reps
+
+    def section():
+        if dropin.interp_all_species(P, ids, idn, grd, param) != 0:
+            raise RuntimeError(dropin.last_error())
+
+    param.sort_cps = 2
+
+    def sort_all():
+        for s in range(ns):
+            if dropin.particle_sort(param, P[s], grd) != 0:
+                raise RuntimeError(dropin.last_error())
+
+    reps = max(3, min(args.steps, 10))
+    t_sec = timed(section, reps)
+    t_copy = timed(sort_all, reps)          # the host arrays are the newest copy
+    for s in range(ns):                     # now the device copy is
+        if dropin.mover_PC(P[s], field, grd, param) != 0:
+            raise RuntimeError(dropin.last_error())
+    t_dev = timed(sort_all, reps)
+    peak, peak_kind = peaks()
+    sort_bytes = 56 * n
+    return {
+        "moment_section": {
+            "call": "spb_interp_all_species", "residency": "device", "species": ns,
+            "ms_per_call": 1e3 * t_sec, "particles_per_s": n / t_sec,
+            "d2h_bytes_per_call": (ns + 1) * 40 * nodes},
+        "particle_sort": {
+            "call": "spb_particle_sort", "sort_cps": 2, "species": ns,
+            "in_place": {
+                "ms_per_call_all_species": 1e3 * t_dev, "particles_per_s": n / t_dev,
+                "algorithmic_bytes": sort_bytes, "achieved_gbs": sort_bytes / t_dev / 1e9,
+                "frac": sort_bytes / t_dev / 1e9 / peak, "peak_gbs": peak,
+                "peak_source": peak_kind},
+            "through_pcie": {
+                "ms_per_call_all_species": 1e3 * t_copy, "particles_per_s": n / t_copy,
+                "h2d_bytes_per_call": 28 * n, "d2h_bytes_per_call": 28 * n}}}
 
 
 def launch_ranks(n: int) -> int:

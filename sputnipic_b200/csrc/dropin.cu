@@ -618,14 +618,12 @@ extern "C" int spb_particle_sort(struct parameters *param, struct particles *par
     sp->host_q_stale = false;
   }
   if (int rc = ensure_capacity(sp, n)) return rc;
-  // seven temporary arrays and the sort's scratch in one allocation
-  void *block = nullptr;
+  // seven temporary arrays and the sort's scratch in one block from the
+  // device's memory pool (kept there for the next sort)
   const size_t tmp_bytes = 7 * (size_t)n * sizeof(float);
   const size_t bytes = tmp_bytes + particle_sort_scratch_bytes(n) + 256;
-  if (cudaMalloc(&block, bytes) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(SPB_ERR_ALLOC, "spb_particle_sort: scratch allocation failed");
-  }
+  void *block = pool_alloc(bytes, sp->stream);
+  if (!block) return fail(SPB_ERR_ALLOC, "spb_particle_sort: scratch allocation failed");
   float *tmp[7];
   for (int a = 0; a < 7; ++a) tmp[a] = static_cast<float *>(block) + a * n;
   void *scratch = static_cast<unsigned char *>(block) + ((tmp_bytes + 255) & ~size_t(255));
@@ -633,8 +631,8 @@ extern "C" int spb_particle_sort(struct parameters *param, struct particles *par
   if (!in_place) rc = copy_particles(sp, part, 0, 7, true, n);
   if (!rc) rc = device_particle_sort(sp->d, tmp, n, B, scratch, sp->stream);
   if (!rc && !in_place) rc = copy_particles(sp, part, 0, 7, false, n);
+  pool_free(block, sp->stream);
   if (!rc) SPB_CUDA(cudaStreamSynchronize(sp->stream));
-  cudaFree(block);
   if (rc) return rc;
   // the device copy now equals the (sorted) host arrays, or is the newest copy
   sp->dev_current = true;

@@ -25,6 +25,11 @@ int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const
 // net[m*nodes + i] = sum over species s (in order) of bases[s][m*nodes + i].
 int launch_sum_species(const float *const *bases, int ns, long nodes, float *net,
                        cudaStream_t s);
+// Scratch from the device's stream-ordered pool on stream s (which keeps freed
+// memory for reuse), or nullptr when it cannot be had; pool_free returns it in
+// stream order.
+void *pool_alloc(size_t bytes, cudaStream_t s);
+void pool_free(void *p, cudaStream_t s);
 // The plain deposit's accumulator: a zeroed node-interleaved buffer (the ten
 // moments of a node side by side, 48 bytes per node) from the device's
 // stream-ordered pool on stream s, or nullptr when it cannot be had (the

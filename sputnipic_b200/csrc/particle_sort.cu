@@ -8,8 +8,9 @@
 // z + y*nbz + x*nbz*nby (src/Particles.cpp:67-69).
 //
 // Sort. A stable LSD radix sort of (bin, original index) pairs with 8-bit
-// digits: per pass, each CTA counts the digits of its chunk, one scan turns the
-// counts into digit-major offsets, and each CTA scatters its chunk in order
+// digits: per pass, each CTA counts the digits of its chunk, a scan (per tile,
+// over the tiles' totals, then the carries) turns the counts into digit-major
+// offsets, and each CTA scatters its chunk in order
 // (ranks within a warp from match_any, across warps through shared counters),
 // which keeps every pass stable. A gather then permutes the seven arrays.
 #include <algorithm>
@@ -108,6 +109,42 @@ __global__ void __launch_bounds__(RS_TPB) k_digit_scatter(const unsigned *__rest
 
 constexpr int SCAN_TPB = 1024;
 
+// Exclusive scan of one tile of SCAN_TPB elements of a, in place; the tile's
+// total goes to tot[tile].
+__global__ void __launch_bounds__(SCAN_TPB) k_scan_tiles(unsigned *a, long m, unsigned *tot) {
+  __shared__ unsigned ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long i = (long)blockIdx.x * SCAN_TPB + threadIdx.x;
+  const unsigned v = i < m ? a[i] : 0u;
+  unsigned x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(FULLM, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned t = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned u = __shfl_up_sync(FULLM, t, o);
+      if (lane >= o) t += u;
+    }
+    ws[lane] = t;
+  }
+  __syncthreads();
+  if (i < m) a[i] = (warp ? ws[warp - 1] : 0u) + x - v;
+  if (threadIdx.x == 0) tot[blockIdx.x] = ws[31];
+}
+
+// Adds each tile's carry (the exclusive scan of the tiles' totals).
+__global__ void __launch_bounds__(SCAN_TPB) k_scan_carry(unsigned *a, long m,
+                                                         const unsigned *__restrict__ tot) {
+  const long i = (long)blockIdx.x * SCAN_TPB + threadIdx.x;
+  if (i < m) a[i] += tot[blockIdx.x];
+}
+
 // Exclusive scan of a (here small) array in one CTA: block sums carried.
 __global__ void __launch_bounds__(SCAN_TPB) k_scan_one(unsigned *a, long m) {
   __shared__ unsigned ws[32];
@@ -156,7 +193,9 @@ __global__ void k_gather7(float *const *__restrict__ tab, const unsigned *__rest
 
 size_t particle_sort_scratch_bytes(long n) {
   const long nchunks = std::max<long>(1, ceil_div(n, RS_CHUNK));
-  return (size_t)n * 4 * 4 + (size_t)nchunks * 256 * 4 + 14 * sizeof(float *) + 256;
+  const long ntiles = ceil_div(nchunks * 256, SCAN_TPB);
+  return (size_t)n * 4 * 4 + (size_t)nchunks * 256 * 4 + (size_t)ntiles * 4 +
+         14 * sizeof(float *) + 256;
 }
 
 int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const SortBins &B,
@@ -172,8 +211,10 @@ int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const
   unsigned *key2 = idx + n;
   unsigned *idx2 = key2 + n;
   unsigned *hist = idx2 + n;
+  const long nh = nchunks * 256, ntiles = ceil_div(nh, SCAN_TPB);
+  unsigned *tot = hist + nh;
   float **tab = reinterpret_cast<float **>(
-      (reinterpret_cast<uintptr_t>(hist + nchunks * 256) + 15) & ~uintptr_t(15));
+      (reinterpret_cast<uintptr_t>(tot + ntiles) + 15) & ~uintptr_t(15));
   const unsigned blocks = (unsigned)std::min<long>(ceil_div(n, 256), 148L * 32);
   k_bin_keys<<<blocks, 256, 0, st>>>(arr[0], arr[1], arr[2], n, B, key, idx);
   SPB_CUDA(cudaGetLastError());
@@ -182,11 +223,14 @@ int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const
   while (bits < 32 && ((unsigned long long)(bins - 1) >> bits) != 0) bits += 8;
   for (int shift = 0; shift < bits; shift += 8) {
     k_digit_hist<<<(unsigned)nchunks, RS_TPB, 0, st>>>(key, n, shift, hist, (int)nchunks);
-    k_scan_one<<<1, SCAN_TPB, 0, st>>>(hist, nchunks * 256);
+    // digit-major offsets: tiles, the tiles' totals, the carries
+    k_scan_tiles<<<(unsigned)ntiles, SCAN_TPB, 0, st>>>(hist, nh, tot);
+    k_scan_one<<<1, SCAN_TPB, 0, st>>>(tot, ntiles);
+    k_scan_carry<<<(unsigned)ntiles, SCAN_TPB, 0, st>>>(hist, nh, tot);
     k_digit_scatter<<<(unsigned)nchunks, RS_TPB, 0, st>>>(key, idx, n, shift, hist,
                                                           (int)nchunks, key2, idx2);
     SPB_CUDA(cudaGetLastError());
-    launches += 3;
+    launches += 5;
     std::swap(key, key2);
     std::swap(idx, idx2);
   }

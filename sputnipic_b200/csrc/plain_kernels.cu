@@ -1051,6 +1051,20 @@ namespace {
 std::atomic<int> g_deposit_mode{SPB_DEPOSIT_ACCUMULATOR};
 }  // namespace
 
+void *pool_alloc(size_t bytes, cudaStream_t s) {
+  keep_pool_memory();
+  void *p = nullptr;
+  if (cudaMallocAsync(&p, std::max<size_t>(bytes, 1), s) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void pool_free(void *p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
 float *plain_acc_alloc(const GeomDev &g, cudaStream_t s) {
   if (g_deposit_mode.load() == SPB_DEPOSIT_DIRECT) return nullptr;
   keep_pool_memory();
