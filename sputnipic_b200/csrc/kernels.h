@@ -18,7 +18,8 @@ struct SortBins {
 };
 size_t particle_sort_scratch_bytes(long n);
 // Sorts arr[0..6] (x, y, z, u, v, w, q; n each) by bin, stably; tmp: seven
-// arrays of n floats; scratch: particle_sort_scratch_bytes(n). Synchronises.
+// arrays of n floats; scratch: particle_sort_scratch_bytes(n). Queued on st in
+// stream order (the caller synchronises before it frees tmp or scratch).
 int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const SortBins &B,
                          void *scratch, cudaStream_t st);
 

@@ -178,14 +178,23 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan_one(unsigned *a, long m) {
   }
 }
 
-// dst[a][j] = src[a][idx[j]] for the seven arrays; tab = src[0..6], dst[0..6].
-__global__ void k_gather7(float *const *__restrict__ tab, const unsigned *__restrict__ idx,
+// The seven source and destination arrays of the gather, passed by value.
+struct Arrays7 {
+  const float *src[7];
+  float *dst[7];
+};
+
+// dst[a][j] = src[a][idx[j]] for the seven arrays.
+__global__ void k_gather7(const __grid_constant__ Arrays7 A, const unsigned *__restrict__ idx,
                           long n) {
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n;
        j += (long)gridDim.x * blockDim.x) {
     const unsigned i = idx[j];
+    float v[7];
 #pragma unroll
-    for (int a = 0; a < 7; ++a) tab[7 + a][j] = tab[a][i];
+    for (int a = 0; a < 7; ++a) v[a] = __ldg(A.src[a] + i);
+#pragma unroll
+    for (int a = 0; a < 7; ++a) A.dst[a][j] = v[a];
   }
 }
 
@@ -194,8 +203,7 @@ __global__ void k_gather7(float *const *__restrict__ tab, const unsigned *__rest
 size_t particle_sort_scratch_bytes(long n) {
   const long nchunks = std::max<long>(1, ceil_div(n, RS_CHUNK));
   const long ntiles = ceil_div(nchunks * 256, SCAN_TPB);
-  return (size_t)n * 4 * 4 + (size_t)nchunks * 256 * 4 + (size_t)ntiles * 4 +
-         14 * sizeof(float *) + 256;
+  return (size_t)n * 4 * 4 + (size_t)nchunks * 256 * 4 + (size_t)ntiles * 4 + 256;
 }
 
 int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const SortBins &B,
@@ -213,8 +221,6 @@ int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const
   unsigned *hist = idx2 + n;
   const long nh = nchunks * 256, ntiles = ceil_div(nh, SCAN_TPB);
   unsigned *tot = hist + nh;
-  float **tab = reinterpret_cast<float **>(
-      (reinterpret_cast<uintptr_t>(tot + ntiles) + 15) & ~uintptr_t(15));
   const unsigned blocks = (unsigned)std::min<long>(ceil_div(n, 256), 148L * 32);
   k_bin_keys<<<blocks, 256, 0, st>>>(arr[0], arr[1], arr[2], n, B, key, idx);
   SPB_CUDA(cudaGetLastError());
@@ -234,19 +240,17 @@ int device_particle_sort(float *const arr[7], float *const tmp[7], long n, const
     std::swap(key, key2);
     std::swap(idx, idx2);
   }
-  // permute the seven arrays: tmp = arr[idx], then copy back
-  float *h[14];
+  // permute the seven arrays: tmp = arr[idx], then copy back (in stream order;
+  // the caller synchronises)
+  Arrays7 A;
   for (int a = 0; a < 7; ++a) {
-    h[a] = arr[a];
-    h[7 + a] = tmp[a];
+    A.src[a] = arr[a];
+    A.dst[a] = tmp[a];
   }
-  SPB_CUDA(cudaMemcpyAsync(tab, h, sizeof(h), cudaMemcpyHostToDevice, st));
-  k_gather7<<<blocks, 256, 0, st>>>(tab, idx, n);
+  k_gather7<<<blocks, 256, 0, st>>>(A, idx, n);
   SPB_CUDA(cudaGetLastError());
   for (int a = 0; a < 7; ++a)
     SPB_CUDA(cudaMemcpyAsync(arr[a], tmp[a], n * sizeof(float), cudaMemcpyDeviceToDevice, st));
-  // the pointer table is read by the gather: finish before the caller reuses `h`
-  SPB_CUDA(cudaStreamSynchronize(st));
   g_launches += launches + 1;
   return SPB_OK;
 }
