@@ -34,6 +34,12 @@
        buckets): the FP64 oracle run on the particles of the first x-slabs of
        cells gives the same moments on the node planes that only those
        particles can reach in one cycle (relative L2 1e-5).
+
+3. particle_sort on one full GEM species (65,536,000 particles) after one
+   mover_PC step, with GEM_3D's sort_cps = 2: in place on the resident copy
+   (DEVICE residency) and through PCIe (COPY residency), both bit-identical
+   to the oracle's particle_sort of the same moved particles (all seven
+   arrays, order within each bin included).
 """
 import numpy as np
 import pytest
@@ -240,3 +246,43 @@ def test_batching_workload_twenty_cycles(cuda):
         assert (err <= 1e-5).all(), (s, err)
     sim.close()
     torch.cuda.empty_cache()
+
+
+def test_particle_sort_full_gem_species(cuda):
+    torch = cuda
+    from sputnipic_b200 import dropin as D
+    from sputnipic_b200.device import gen_fields, gen_particles
+    wl = W.gem()
+    orc = oracle.CpuOracle("restated", 32)
+    fields = [f.cpu().numpy() for f in gen_fields(wl)]
+    param = D.make_parameters(wl)
+    grd = D.setGrid(param)
+    field = D.field_allocate(grd, fields)
+    param.sort_cps = 2
+    p = gen_particles(wl, 0)
+    host = {k: p[k].cpu().numpy() for k in "xyzuvwq"}
+    del p
+    torch.cuda.empty_cache()
+    a = D.particle_allocate(param, 0, arrays={k: host[k].copy() for k in "xyzuvwq"})
+    b = D.particle_allocate(param, 0, arrays=host)
+    try:
+        # a: moved and sorted where it lies (the device copy is the newest
+        # and, after a deposit, holds q too)
+        assert D.set_residency(True) == 0
+        assert D.mover_PC(a, field, grd, param) == 0, D.last_error()
+        D.interpP2G(a, D.interp_dens_species_allocate(grd, 0), grd, raise_on_error=True)
+        assert D.particle_sort(param, a, grd) == 0, D.last_error()
+        assert D.sync_particles_to_host(a) == 0
+    finally:
+        D.set_residency(False)
+    D.release_all()
+    # b: moved in COPY residency (the oracle's input), then sorted through PCIe
+    assert D.mover_PC(b, field, grd, param) == 0, D.last_error()
+    ref = {k: v.copy() for k, v in D.particle_arrays(b).items()}
+    assert D.particle_sort(param, b, grd) == 0, D.last_error()
+    D.release_all()
+    assert orc.particle_sort(oracle.setup_from(wl), 2, ref) == 0
+    got_a, got_b = D.particle_arrays(a), D.particle_arrays(b)
+    for k in "xyzuvwq":
+        assert np.array_equal(got_a[k].view(np.uint32), ref[k].view(np.uint32)), ("in place", k)
+        assert np.array_equal(got_b[k].view(np.uint32), ref[k].view(np.uint32)), ("pcie", k)
