@@ -16,7 +16,11 @@
      - the moments on the node planes x = 3 .. SLABS-1, which in one cycle only
        the slabs' particles reach, are within the reordering bound
        |gpu - ref| <= 32 eps32 sum|terms| of the reference FP32 deposit of
-       the moved slab particles.
+       the moved slab particles;
+     - the driver's moment section in one call (spb_interp_all_species) on
+       the moved particles: each species' moments within relative L2 1e-5 of
+       its own interpP2G deposit with applyBCids applied, the net moments
+       bit-identical to the float sum of the species' in species order.
 
 2. Batching workload (species of 65.5M, 65.5M, 6.55M and 6.55M particles on
    the GEM grid, background at 12.5 ppc), 20 cycles with CUDA graphs,
@@ -127,6 +131,22 @@ def test_plain_dropin_full_gem_device_residency(cuda):
         bound = 32 * EPS32 * np.stack(absm)[:, keep] + 1e-30
         diff = np.abs(mom[:, keep] - np.stack(ref_m).astype(np.float64)[:, keep])
         assert (diff <= bound).all(), (s, int((diff > bound).sum()))
+    # the driver's moment section in one call on the same moved particles:
+    # each species' moments match its own interpP2G deposit above with the
+    # oracle's applyBCids applied (two FP32 sums in different orders), and the
+    # net moments are the float sum of the species' in species order
+    ids2 = [D.interp_dens_species_allocate(grd, s) for s in range(ns)]
+    idn = D.interp_dens_net_allocate(grd)
+    assert D.interp_all_species(P, ids2, idn, grd, param) == 0, D.last_error()
+    net = np.zeros((10, wl.nodes), np.float32)
+    for s in range(ns):
+        sep = [m.copy() for m in D.moments(ids[s])]
+        orc32.apply_bc_ids(setup, sep)
+        got = np.stack(D.moments(ids2[s]))
+        err = rel_l2(got.astype(np.float64), np.stack(sep).astype(np.float64))
+        assert (err <= 1e-5).all(), (s, err)
+        net = net + got
+    assert np.array_equal(np.stack(D.moments(idn)), net)
     # species 0 again in COPY residency (chunked PCIe pipeline): bit-identical
     dev_result = {k: v.copy() for k, v in D.particle_arrays(P[0]).items()}
     D.release_all()
