@@ -92,8 +92,10 @@ struct Species6 {
 
 // Pressure-tensor rows (pxx pxy pxz / pxy pyy pyz / pxz pyz pzz): divergence
 // of each row on the inner cells, times alfa = (T)(-dt/2); species blockIdx.y.
+// Five CTAs per SM (at most 51 registers; a few bytes spill): the pass is
+// bound by the latency of its FP64 stencil loads, so residency pays.
 template <typename T>
-__global__ void k_hat_div_tensor(HatGeom g, const __grid_constant__ Species6<T> S, T alfa) {
+__global__ void __launch_bounds__(256, 5) k_hat_div_tensor(HatGeom g, const __grid_constant__ Species6<T> S, T alfa) {
   const int is = blockIdx.y;
   const int mx = g.nxc - 2, my = g.nyc - 2, mz = g.nzc - 2;
   const long inner = (long)mx * my * mz;
@@ -241,8 +243,9 @@ struct Out3 {
 // Every node: per species in order, the interpolated divergence (inner
 // nodes) plus J, rotated by the species' beta B and added into J hat, which
 // starts at 0 (the reference's per-species accumulation, in registers).
+// Four CTAs per SM (at most 64 registers), for the same reason.
 template <typename T>
-__global__ void k_hat_pidot(HatGeom g, const __grid_constant__ Species6<T> S, int ns, Vec3<T> B,
+__global__ void __launch_bounds__(256, 4) k_hat_pidot(HatGeom g, const __grid_constant__ Species6<T> S, int ns, Vec3<T> B,
                             Out3<T> JH) {
   const long nodes = (long)g.nxn * g.nyn * g.nzn;
   for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < nodes;
